@@ -1,0 +1,274 @@
+/*
+ * tmpm.h -- C ABI of the B200 (sm_100a) MLS-MPM substep library `libtmpm.so`.
+ *
+ * The library is a drop-in device backend for tessera-mpm's resident GPU path.
+ * Every entry point below replaces one method of the reference's Rust type
+ * `GpuMpmResidentSession` (crates/tessera-mpm/src/gpu.rs:206-662) or one of the
+ * `MpmWorld` GPU conveniences (gpu.rs:2168-2293); the citation sits beside each
+ * declaration.  Types are plain C: host pointers, sizes and integer status codes,
+ * so a Rust `extern "C"` block, cgo or Python ctypes can bind them directly.
+ *
+ * Threading: a session is single-owner, like the reference's session (one wgpu
+ * queue, `&mut self` methods).  Distinct sessions may be used from distinct
+ * threads.  All calls are synchronous with respect to host memory: host arrays
+ * passed in are not retained after the call returns.
+ */
+#ifndef TMPM_H
+#define TMPM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes, one per variant of GpuMpmError (gpu.rs:135-154) and MpmError
+ * (world.rs:164-181).  The Python binding maps every non-zero status onto
+ * TesseraError.Failed(reason) exactly like tessera-python3d (lib.rs:82-95). */
+typedef enum TmpmStatus {
+    TMPM_OK = 0,
+    TMPM_ERR_INVALID_INPUT = 1,        /* GpuMpmError::InvalidInput */
+    TMPM_ERR_CAPACITY = 2,             /* GpuMpmError::Capacity */
+    TMPM_ERR_PENDING_STEPS = 3,        /* GpuMpmError::PendingSteps */
+    TMPM_ERR_READBACK = 4,             /* GpuMpmError::Readback(String) */
+    TMPM_ERR_RESIDENT_UNAVAILABLE = 5, /* GpuMpmError::ResidentUnavailable */
+    TMPM_ERR_MPM_INVALID_INPUT = 6,    /* GpuMpmError::Reference(MpmError::InvalidInput) */
+    TMPM_ERR_EXCESSIVE_SUBSTEPS = 7,   /* MpmError::ExcessiveSubsteps */
+    TMPM_ERR_NON_FINITE_STATE = 8,     /* MpmError::NonFiniteState */
+    TMPM_ERR_UNKNOWN_CHUNK = 9,        /* MpmError::UnknownChunk */
+    TMPM_ERR_PARTICLE_CAPACITY = 10,   /* MpmError::ParticleCapacity */
+    TMPM_ERR_DEVICE = 11               /* CUDA runtime failure (wgpu device loss in the reference) */
+} TmpmStatus;
+
+/* Constitutive models, in the order of MaterialModel (material.rs:28-91). */
+typedef enum TmpmMaterialKind {
+    TMPM_MAT_ELASTIC = 0,          /* params: young, poisson (corotated, material.rs:440-455) */
+    TMPM_MAT_NEO_HOOKEAN = 1,      /* params: young, poisson (material.rs:457-467) */
+    TMPM_MAT_SAND = 2,             /* params: young, poisson, friction_angle, cohesion */
+    TMPM_MAT_FLUID = 3,            /* params: bulk, gamma, viscosity, tensile_stiffness (material.rs:469-486) */
+    TMPM_MAT_SNOW = 4,             /* params: young, poisson, critical_compression, critical_stretch, hardening */
+    TMPM_MAT_SAND_NEO_HOOKEAN = 5  /* params: young, poisson, friction_angle, cohesion */
+} TmpmMaterialKind;
+
+/* Obstacle shapes (obstacle.rs:10-61). */
+typedef enum TmpmObstacleShape {
+    TMPM_SHAPE_SPHERE = 0,         /* dims[0] = radius */
+    TMPM_SHAPE_BOX = 1,            /* dims = half extents */
+    TMPM_SHAPE_CAPSULE = 2,        /* dims[0] = half_height, dims[1] = radius */
+    TMPM_SHAPE_CYLINDER = 3,       /* dims[0] = half_height, dims[1] = radius */
+    TMPM_SHAPE_CONE = 4,           /* dims[0] = half_height, dims[1] = radius */
+    TMPM_SHAPE_GROUND = 5,         /* dims[0..2] = half extents x, y */
+    TMPM_SHAPE_TRIANGLE_PRISM = 6, /* dims[0] = half_thickness, vertices = a, b, c */
+    TMPM_SHAPE_CONVEX = 7          /* planes, plane_count, bound_radius */
+} TmpmObstacleShape;
+
+/* Boundary responses (obstacle.rs:63-77). */
+typedef enum TmpmBoundary {
+    TMPM_BOUNDARY_SLIP = 0,
+    TMPM_BOUNDARY_STICK = 1,
+    TMPM_BOUNDARY_SEPARATE = 2,
+    TMPM_BOUNDARY_NON_REFLECTING = 3,
+    TMPM_BOUNDARY_FREE_SLIP = 4
+} TmpmBoundary;
+
+/* Integration parameters, MpmParams (world.rs:27-49).  `wall_mode` 0 is the
+ * reference's separating frictionless walls (world.rs:561-575); 1 selects
+ * sticky walls (grid velocity zeroed within one cell of a wall), an extension
+ * the reference does not have. */
+typedef struct TmpmParams {
+    double cell_width;
+    double gravity[3];
+    double max_substep;
+    int32_t has_bounds;
+    int32_t wall_mode;
+    double bounds_min[3];
+    double bounds_max[3];
+} TmpmParams;
+
+/* Caller-owned structure-of-arrays view of particles (MpmParticle,
+ * world.rs:67-102).  Matrices are 9 doubles per particle in column-major order,
+ * as MpmParticleState exposes them (tessera-python3d/src/mpm.rs:253-256).
+ * On input, NULL optional arrays mean: force = 0, damping = 0, plastic state =
+ * (1, 0, 0) (or hardening 1 for sand materials, world.rs:132-142), enabled = 1,
+ * fixed = 0, transfer_color = 0, group_id = 0, chunk_id = 0.  On output (read)
+ * every non-NULL array is filled. */
+typedef struct TmpmParticleArrays {
+    size_t count;
+    double *position;        /* count x 3 */
+    double *velocity;        /* count x 3 */
+    double *deformation;     /* count x 9 */
+    double *affine;          /* count x 9 */
+    double *force;           /* count x 3, optional */
+    double *mass;            /* count */
+    double *rest_volume;     /* count */
+    double *radius;          /* count */
+    double *damping;         /* count, optional */
+    double *plastic;         /* count x 3: plastic_det, hardening, log_volume_gain; optional */
+    int32_t *material;       /* count, TmpmMaterialKind */
+    double *material_params; /* count x 5 */
+    uint8_t *enabled;        /* count, optional */
+    uint8_t *fixed;          /* count, optional */
+    uint16_t *transfer_color;/* count, optional */
+    uint32_t *group_id;      /* count, optional */
+    uint64_t *chunk_id;      /* count, optional (read only) */
+} TmpmParticleArrays;
+
+/* One prescribed rigid obstacle (RigidObstacle, obstacle.rs:79-98). */
+typedef struct TmpmObstacle {
+    int32_t shape;           /* TmpmObstacleShape */
+    int32_t boundary;        /* TmpmBoundary */
+    int32_t cpic_group;      /* -1 = none, else 0..31 (triangle prisms only) */
+    uint32_t plane_count;    /* convex only */
+    double center[3];
+    double orientation[4];   /* unit quaternion x, y, z, w (local to world) */
+    double linear_velocity[3];
+    double angular_velocity[3];
+    double friction;
+    double dims[3];
+    double vertices[9];      /* triangle prism local vertices a, b, c */
+    double bound_radius;     /* convex only */
+    const double *planes;    /* convex only: plane_count x (nx, ny, nz, offset), local frame */
+} TmpmObstacle;
+
+/* Optional session knobs.  Zero-initialised means defaults. */
+typedef struct TmpmSessionOptions {
+    int32_t device;          /* CUDA device ordinal; default 0 */
+    uint32_t max_blocks;     /* block pool capacity per grid; 0 = sized from the scene */
+    uint32_t resort_interval;/* substeps between particle re-sorts; 0 = once per submit */
+    uint32_t reserved;
+    uint64_t next_chunk_id;  /* MpmWorld's next chunk id (world.rs:220); 0 = max(chunk_id) + 1 */
+    uint64_t substeps;       /* MpmWorld::substeps of the uploaded world (world.rs:215) */
+} TmpmSessionOptions;
+
+typedef struct TmpmSession TmpmSession;
+
+/* ---------------- session lifecycle (GpuMpmResidentSession) ---------------- */
+
+/* GpuMpmResidentSession::new (gpu.rs:253-280): validate (gpu.rs:664-677),
+ * pack f64 -> f32, upload and keep device buffers.  `use_cpic` mirrors
+ * MpmWorld::use_cpic (world.rs:216-219).  On failure *out is NULL and
+ * tmpm_last_error() describes the reason. */
+TmpmStatus tmpm_session_create(const TmpmParams *params,
+                               const TmpmParticleArrays *particles,
+                               const TmpmObstacle *obstacles, size_t obstacle_count,
+                               int32_t use_cpic, double substep_dt,
+                               const TmpmSessionOptions *options,
+                               TmpmSession **out);
+
+/* Drop (gpu.rs:205-216 owns buffers; dropping releases them). */
+void tmpm_session_destroy(TmpmSession *session);
+
+/* GpuMpmResidentSession::submit_steps (gpu.rs:303-322): 1..64 substeps queued
+ * on the session's stream without waiting. */
+TmpmStatus tmpm_submit_steps(TmpmSession *session, uint32_t steps);
+
+/* GpuMpmResidentSession::step (gpu.rs:286-292): submit + synchronize. */
+TmpmStatus tmpm_step(TmpmSession *session, uint32_t steps);
+
+/* GpuMpmResidentSession::synchronize (gpu.rs:382-411): wait (5 s limit ->
+ * TMPM_ERR_READBACK), check device failure flags, replace the host world only
+ * on success.  Any error invalidates the session. */
+TmpmStatus tmpm_synchronize(TmpmSession *session);
+
+/* GpuMpmResidentSession::pending_substeps / has_pending_steps (gpu.rs:367-375). */
+uint64_t tmpm_pending_substeps(const TmpmSession *session);
+int32_t tmpm_has_pending_steps(const TmpmSession *session);
+
+/* MpmWorld::substeps of the last synchronized world (world.rs:215). */
+uint64_t tmpm_substeps(const TmpmSession *session);
+
+/* world().particles.len() (gpu.rs:654-656). */
+size_t tmpm_particle_count(const TmpmSession *session);
+
+/* world() (gpu.rs:654-656): copy the last synchronized particles into caller
+ * arrays.  out->count must equal tmpm_particle_count(). */
+TmpmStatus tmpm_read_particles(const TmpmSession *session, TmpmParticleArrays *out);
+
+/* MpmWorld::stable_timestep of the last synchronized world (world.rs:288-303). */
+double tmpm_stable_timestep(const TmpmSession *session);
+
+/* GpuMpmResidentSession::set_particle_force (gpu.rs:457-485). */
+TmpmStatus tmpm_set_particle_force(TmpmSession *session, size_t index, const double force[3]);
+
+/* GpuMpmResidentSession::set_obstacles (gpu.rs:491-529). */
+TmpmStatus tmpm_set_obstacles(TmpmSession *session, const TmpmObstacle *obstacles, size_t count);
+
+/* GpuMpmResidentSession::add_particles (gpu.rs:535-549). */
+TmpmStatus tmpm_add_particles(TmpmSession *session, const TmpmParticleArrays *particles,
+                              uint64_t *chunk_out);
+
+/* GpuMpmResidentSession::remove_chunk (gpu.rs:553-564). */
+TmpmStatus tmpm_remove_chunk(TmpmSession *session, uint64_t chunk, size_t *removed_out);
+
+/* Replace the synchronized world's particles by `particles` (same semantics
+ * as the private replace_particle_world, gpu.rs:566-579: validate, re-pack,
+ * re-upload; device buffers are reused when they are large enough).  Chunk ids
+ * are taken from particles->chunk_id when given. */
+TmpmStatus tmpm_write_particles(TmpmSession *session, const TmpmParticleArrays *particles);
+
+/* GpuMpmResidentSession::encode_particle_snapshot (gpu.rs:595-651): write one
+ * 32-byte record (position xyz, mass; velocity xyz, rest volume) per particle,
+ * in world order, into caller-owned DEVICE memory on the session's stream.
+ * Disabled particles get zero mass.  *written = records written. */
+TmpmStatus tmpm_encode_particle_snapshot(TmpmSession *session, void *device_out,
+                                         size_t capacity_bytes, uint32_t *written);
+
+/* The substep size this session was created with (gpu.rs:359-361). */
+double tmpm_substep_dt(const TmpmSession *session);
+
+/* Change the fixed substep of an idle session (the Python binding rebuilds the
+ * session when dt changes, mpm.rs:813-832; here buffers are kept and only the
+ * CFL validation of gpu.rs:664-677 is repeated). */
+TmpmStatus tmpm_set_substep_dt(TmpmSession *session, double substep_dt);
+
+/* ------------- MpmWorld GPU conveniences (gpu.rs:2168-2293) ------------- */
+
+/* MpmWorld::step_with_gpu_transfers (gpu.rs:2208-2240): CFL-limited substeps
+ * of total duration dt; each substep validated and synchronized. */
+TmpmStatus tmpm_step_cfl(TmpmSession *session, double dt);
+
+/* MpmWorld::step_with_gpu_obstacle_reactions (gpu.rs:2247-2293): as
+ * tmpm_step_cfl, also returning per-obstacle impulses, 6 doubles each
+ * (linear xyz, angular xyz about the obstacle centre), in obstacle order. */
+TmpmStatus tmpm_step_cfl_with_reactions(TmpmSession *session, double dt,
+                                        double *reactions_out, size_t obstacle_count);
+
+/* ------------------------------ diagnostics ------------------------------ */
+
+/* Human-readable reason for the last failed call on this session. */
+const char *tmpm_last_error_message(const TmpmSession *session);
+
+/* Reason for the last failed session-less call on this thread. */
+const char *tmpm_last_error(void);
+
+/* Library version string. */
+const char *tmpm_version(void);
+
+/* Binning view of the device state (no reference counterpart; test hook).
+ * Re-bins the current device particles exactly as a substep does and returns,
+ * in DEVICE STORAGE order: the world index of each stored particle, its f32
+ * base cell (3 ints) and its sort key.  Arrays hold tmpm_device_count() items. */
+size_t tmpm_device_count(const TmpmSession *session);
+TmpmStatus tmpm_debug_binning(TmpmSession *session, uint32_t *world_index_out,
+                              int32_t *base_cell_out, uint32_t *key_out);
+
+/* Grid view (test hook): run only P2G on the current device state with the
+ * session's substep and return every node with non-zero mass: cell (3 ints per
+ * node), mass and momentum (4 floats per node), plus the node count.  Arrays
+ * must hold `capacity` nodes; *count receives the total. */
+TmpmStatus tmpm_debug_p2g(TmpmSession *session, int32_t *cells_out, float *mass_momentum_out,
+                          size_t capacity, size_t *count);
+
+/* Kernel timing (bench hook): time `steps` substeps of the resident path on the
+ * session stream with CUDA events; returns milliseconds via *ms.  Per-kernel
+ * averages (ms per launch) go to kernel_ms[0..n) in the order p2g, grid,
+ * g2p2g, g2p, resort when kernel_ms is non-NULL. */
+TmpmStatus tmpm_bench_substeps(TmpmSession *session, uint32_t steps, double *ms,
+                               double *kernel_ms, size_t kernel_count);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TMPM_H */

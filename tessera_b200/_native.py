@@ -1,0 +1,94 @@
+"""Loads ``libtmpm.so`` (built in-tree for sm_100a) and declares its C signatures.
+
+The device path has no fallback: if the library is missing or no CUDA device is
+present, the calls that need it raise.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+from ._abi import TmpmObstacle, TmpmParams, TmpmParticleArrays, TmpmSessionOptions
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libtmpm.so")
+_lib = None
+
+
+def build() -> str:
+    """Compile libtmpm.so with nvcc (cross-compiles without a GPU)."""
+    subprocess.run(["make", "-s", "-C", os.path.join(_HERE, "csrc"), "-j4"], check=True)
+    return LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"libtmpm.so is not built ({LIB_PATH}); run tessera_b200._native.build()")
+    L = C.CDLL(LIB_PATH)
+    P = C.c_void_p
+    S = C.c_int32
+    L.tmpm_version.restype = C.c_char_p
+    L.tmpm_last_error.restype = C.c_char_p
+    L.tmpm_last_error_message.restype = C.c_char_p
+    L.tmpm_last_error_message.argtypes = [P]
+    L.tmpm_session_create.restype = S
+    L.tmpm_session_create.argtypes = [C.POINTER(TmpmParams), C.POINTER(TmpmParticleArrays), P, C.c_size_t,
+                                      C.c_int32, C.c_double, C.POINTER(TmpmSessionOptions), C.POINTER(P)]
+    L.tmpm_session_destroy.argtypes = [P]
+    L.tmpm_session_destroy.restype = None
+    for name in ("tmpm_submit_steps", "tmpm_step"):
+        getattr(L, name).argtypes = [P, C.c_uint32]
+        getattr(L, name).restype = S
+    L.tmpm_synchronize.argtypes = [P]
+    L.tmpm_synchronize.restype = S
+    L.tmpm_pending_substeps.argtypes = [P]
+    L.tmpm_pending_substeps.restype = C.c_uint64
+    L.tmpm_has_pending_steps.argtypes = [P]
+    L.tmpm_has_pending_steps.restype = C.c_int32
+    L.tmpm_substeps.argtypes = [P]
+    L.tmpm_substeps.restype = C.c_uint64
+    L.tmpm_particle_count.argtypes = [P]
+    L.tmpm_particle_count.restype = C.c_size_t
+    L.tmpm_device_count.argtypes = [P]
+    L.tmpm_device_count.restype = C.c_size_t
+    L.tmpm_read_particles.argtypes = [P, C.POINTER(TmpmParticleArrays)]
+    L.tmpm_read_particles.restype = S
+    L.tmpm_stable_timestep.argtypes = [P]
+    L.tmpm_stable_timestep.restype = C.c_double
+    L.tmpm_set_particle_force.argtypes = [P, C.c_size_t, P]
+    L.tmpm_set_particle_force.restype = S
+    L.tmpm_set_obstacles.argtypes = [P, P, C.c_size_t]
+    L.tmpm_set_obstacles.restype = S
+    L.tmpm_add_particles.argtypes = [P, C.POINTER(TmpmParticleArrays), C.POINTER(C.c_uint64)]
+    L.tmpm_add_particles.restype = S
+    L.tmpm_remove_chunk.argtypes = [P, C.c_uint64, C.POINTER(C.c_size_t)]
+    L.tmpm_remove_chunk.restype = S
+    L.tmpm_write_particles.argtypes = [P, C.POINTER(TmpmParticleArrays)]
+    L.tmpm_write_particles.restype = S
+    L.tmpm_encode_particle_snapshot.argtypes = [P, P, C.c_size_t, C.POINTER(C.c_uint32)]
+    L.tmpm_encode_particle_snapshot.restype = S
+    L.tmpm_substep_dt.argtypes = [P]
+    L.tmpm_substep_dt.restype = C.c_double
+    L.tmpm_set_substep_dt.argtypes = [P, C.c_double]
+    L.tmpm_set_substep_dt.restype = S
+    L.tmpm_step_cfl.argtypes = [P, C.c_double]
+    L.tmpm_step_cfl.restype = S
+    L.tmpm_step_cfl_with_reactions.argtypes = [P, C.c_double, P, C.c_size_t]
+    L.tmpm_step_cfl_with_reactions.restype = S
+    L.tmpm_debug_binning.argtypes = [P, P, P, P]
+    L.tmpm_debug_binning.restype = S
+    L.tmpm_debug_p2g.argtypes = [P, P, P, C.c_size_t, C.POINTER(C.c_size_t)]
+    L.tmpm_debug_p2g.restype = S
+    L.tmpm_bench_substeps.argtypes = [P, C.c_uint32, C.POINTER(C.c_double), P, C.c_size_t]
+    L.tmpm_bench_substeps.restype = S
+    _lib = L
+    return L
+
+
+def version() -> str:
+    return lib().tmpm_version().decode()

@@ -1,0 +1,132 @@
+// tmpm_internal.h -- device data layout shared by the kernels and the host session.
+//
+// HBM layout (one session, one GPU):
+//   * particles: structure of arrays in f32, component-major (x[c * cap + i]),
+//     kept in "storage order" = sorted by the Morton key of each particle's 4^3
+//     grid block, re-sorted at the start of every submitted batch;
+//   * particle classes: one 48-byte record per distinct (material, mass, volume,
+//     radius, damping, transfer colour) tuple, indexed by a u32 per particle;
+//   * two sparse grids (ping-pong, step n and n+1), each an open-addressing hash
+//     table of 4^3 blocks (64-bit key -> u32 block id) plus a block pool of
+//     64 float4 nodes (mass, momentum xyz -> velocity xyz after the grid update).
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+
+#include <cuda_runtime.h>
+
+namespace tmpm {
+
+constexpr int kBlockShift = 2;  // 4^3 cells per grid block
+constexpr int kNodesPerBlock = 64;
+constexpr unsigned long long kEmptyKey = ~0ull;
+constexpr uint32_t kPendingId = 0xFFFFFFFFu;
+constexpr uint32_t kInvalidId = 0xFFFFFFFEu;
+constexpr int kBlockBias = 32768;      // block coordinate bias inside the 64-bit key
+constexpr int kBlockCoordMin = -32767; // representable block coordinates
+constexpr int kBlockCoordMax = 32766;
+constexpr int kMaxProbe = 4096;        // hash probe limit before reporting Capacity
+constexpr int kSpinLimit = 1 << 20;    // bounded wait for a block id to be published
+
+// Device status word bits (or-ed by kernels, read by synchronize).
+constexpr uint32_t kStatusResident = 1u;  // CFL, escape, irregular F, non-finite -> ResidentUnavailable
+constexpr uint32_t kStatusCapacity = 2u;  // hash table or block pool exhausted -> Capacity
+constexpr uint32_t kStatusTimeout = 4u;   // a bounded device wait gave up -> Readback
+
+// GPU material codes (the reference shader's codes, gpu.rs:1171-1276).
+constexpr int kMatNeoHookean = 1;
+constexpr int kMatFluid = 2;
+constexpr int kMatCorotated = 3;
+
+constexpr uint32_t kFixedBit = 0x80000000u;
+constexpr uint32_t kClassMask = 0x7FFFFFFFu;
+
+struct DevClass {
+    float mass, volume, radius, damping;
+    float p0, p1, p2, p3;  // corotated/NH: lambda, mu; fluid: bulk, gamma, viscosity, tensile
+    int32_t kind;          // kMat*
+    float wave;            // CFL wave speed sqrt((lambda + 2 mu) / rho) or sqrt(K gamma / rho)
+    uint32_t color;        // transfer colour (separate grid namespace)
+    float pad;
+};
+static_assert(sizeof(DevClass) == 48, "DevClass layout");
+
+struct DevObstacle {
+    int32_t shape, boundary, cpic_group, plane_offset;
+    int32_t plane_count, pad0, pad1, pad2;
+    float center[4];    // xyz, bound (triangle prism / convex bounding radius)
+    float q[4];         // x, y, z, w
+    float lin[4];       // xyz, friction
+    float ang[4];
+    float dims[4];
+    float verts[12];    // a, b, c (xyz + pad)
+};
+
+struct GridTable {
+    unsigned long long *keys;  // [capacity]
+    uint32_t *vals;            // [capacity]
+    uint32_t *count;           // allocated blocks
+    float4 *pool;              // [max_blocks * 64]
+    int4 *coords;              // [max_blocks]: bx, by, bz, colour
+    uint32_t mask;             // capacity - 1
+    uint32_t max_blocks;
+};
+
+struct SimParams {
+    float h, inv_h, inv_d, dt;
+    float gx, gy, gz;
+    int has_bounds;
+    float bmin[3], bmax[3];
+    int first_base[3], last_base[3];  // escape window of base cells (bounded worlds)
+    int wall_mode;
+    int num_obstacles;
+    int reactions;
+    int apply_force;
+    int resident_checks;  // CFL / escape / conditioning flags (resident path only, gpu.rs:1429)
+};
+
+struct ParticleSoA {
+    float *x;       // 3 * cap
+    float *v;       // 3 * cap
+    float *C;       // 9 * cap, column-major components (col * 3 + row)
+    float *F;       // 9 * cap
+    float *force;   // 3 * force_stride, indexed by WORLD index (one-shot forces)
+    uint32_t *cls;  // class index | kFixedBit
+    uint32_t *widx; // world index of each stored particle
+    size_t cap;
+    size_t force_stride;
+};
+
+struct SortBuffers {
+    uint32_t *keys[2];
+    uint32_t *vals[2];
+    uint32_t *hist;    // 256 * tiles
+    uint32_t *totals;  // 256
+    size_t cap;
+};
+
+enum TransferMode { kModeP2G = 0, kModeG2P2G = 1, kModeG2P = 2 };
+
+// Launchers (tmpm_kernels.cu).  All run on `stream`.
+void launch_transfer(int mode, const ParticleSoA &P, int n, const DevClass *classes, const GridTable &cur,
+                     const GridTable &next, const SimParams &sp, const DevObstacle *obstacles,
+                     const float *planes, double *reactions, uint32_t *status, cudaStream_t stream);
+void launch_grid_update(const GridTable &g, const GridTable &clear, const SimParams &sp,
+                        const DevObstacle *obstacles, const float *planes, double *reactions,
+                        uint32_t *status, cudaStream_t stream);
+void launch_clear_table(const GridTable &g, cudaStream_t stream);
+void launch_resort(ParticleSoA &src, ParticleSoA &dst, int n, const SimParams &sp, SortBuffers &sb,
+                   cudaStream_t stream);
+void launch_bin_keys(const ParticleSoA &P, int n, const SimParams &sp, int32_t *cells, uint32_t *keys,
+                     cudaStream_t stream);
+void launch_dump_grid(const GridTable &g, int32_t *cells, float4 *values, uint32_t *count, uint32_t capacity,
+                      cudaStream_t stream);
+void launch_snapshot(const ParticleSoA &P, int n, const DevClass *classes, float4 *out, cudaStream_t stream);
+int device_sm_count();
+
+// Radix sort (tmpm_sort.cu): stable sort of (key, value) pairs by `bits` low key bits.
+// Result ends in sb.keys[0] / sb.vals[0].
+void radix_sort_pairs(SortBuffers &sb, int n, int bits, cudaStream_t stream);
+
+}  // namespace tmpm

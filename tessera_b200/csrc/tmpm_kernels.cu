@@ -1,0 +1,633 @@
+// tmpm_kernels.cu -- the MLS-MPM substep on sm_100a.
+//
+// One substep n of the resident path is two kernels:
+//   k_grid(n):      v = p / m + g dt, walls, obstacles, reactions
+//                   (world.rs:401-417, gpu.wgsl:772-819 / 1056-1108)
+//   k_transfer(n):  G2P of step n fused with P2G of step n+1
+//                   (world.rs:419-464 then 378-399; gpu.wgsl:821-1019, 711-770)
+// A batch opens with a P2G-only transfer and closes with a G2P-only transfer,
+// which alone writes velocity and the affine matrix back to HBM.
+//
+// Each CTA owns 256 consecutive particles in storage order (sorted by 4^3
+// block).  It stages the grid nodes its particles touch in a shared-memory
+// box ("tile"): the gather tile holds step-n velocities, the scatter tile
+// accumulates step-(n+1) mass and momentum with shared atomics and is flushed
+// to the block pool with one float4 atomic per touched node.  Chunks whose box
+// is too large (scattered particles) fall back to per-node global access.
+
+#include <climits>
+
+#include "tmpm_device.cuh"
+
+namespace tmpm {
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kTileMaxDim = 12;
+constexpr int kTileMaxNodes = 1024;
+constexpr int kMaxTileBlocks = 64;
+constexpr uint32_t kFatal = kStatusCapacity | kStatusTimeout | kStatusResident;
+
+struct Box {
+    int lo[3];
+    int dim[3];
+    int blo[3];
+    int nb[3];
+    int nodes;
+    int nbt;
+    int ok;
+    uint32_t color;
+};
+
+__device__ __forceinline__ int node_local(int cx, int cy, int cz) { return ((cx & 3) * 4 + (cy & 3)) * 4 + (cz & 3); }
+
+// Block-wide min/max of base cells and colours; thread 0 fills `box`.
+__device__ __forceinline__ void reduce_box(bool valid, const int b[3], uint32_t color, int (*red)[8], Box &box) {
+    int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int vals[8];
+    for (int a = 0; a < 3; ++a) {
+        vals[a] = valid ? b[a] : INT_MAX;
+        vals[3 + a] = valid ? b[a] : INT_MIN;
+    }
+    vals[6] = valid ? static_cast<int>(color) : INT_MAX;
+    vals[7] = valid ? static_cast<int>(color) : INT_MIN;
+    int r[8];
+    for (int a = 0; a < 3; ++a) r[a] = __reduce_min_sync(0xffffffffu, vals[a]);
+    for (int a = 3; a < 6; ++a) r[a] = __reduce_max_sync(0xffffffffu, vals[a]);
+    r[6] = __reduce_min_sync(0xffffffffu, vals[6]);
+    r[7] = __reduce_max_sync(0xffffffffu, vals[7]);
+    if (lane == 0)
+        for (int a = 0; a < 8; ++a) red[warp][a] = r[a];
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int m[8];
+        for (int a = 0; a < 8; ++a) m[a] = red[0][a];
+        for (int w = 1; w < kThreads / 32; ++w) {
+            for (int a = 0; a < 3; ++a) m[a] = min(m[a], red[w][a]);
+            for (int a = 3; a < 6; ++a) m[a] = max(m[a], red[w][a]);
+            m[6] = min(m[6], red[w][6]);
+            m[7] = max(m[7], red[w][7]);
+        }
+        bool any = m[0] <= m[3];
+        int nodes = 1, nbt = 1;
+        bool ok = any && m[6] == m[7];
+        for (int a = 0; a < 3 && ok; ++a) {
+            long long d = static_cast<long long>(m[3 + a]) - m[a] + 3;
+            if (d > kTileMaxDim) ok = false;
+        }
+        if (ok) {
+            for (int a = 0; a < 3; ++a) {
+                box.lo[a] = m[a];
+                box.dim[a] = m[3 + a] - m[a] + 3;
+                box.blo[a] = m[a] >> kBlockShift;
+                box.nb[a] = ((m[3 + a] + 2) >> kBlockShift) - box.blo[a] + 1;
+                nodes *= box.dim[a];
+                nbt *= box.nb[a];
+            }
+            ok = nodes <= kTileMaxNodes && nbt <= kMaxTileBlocks;
+        }
+        box.nodes = nodes;
+        box.nbt = nbt;
+        box.ok = ok ? 1 : 0;
+        box.color = static_cast<uint32_t>(m[6]);
+    }
+    __syncthreads();
+}
+
+__device__ __forceinline__ void quad_weights(float f, float w[3]) {
+    w[0] = 0.5f * (1.5f - f) * (1.5f - f);
+    w[1] = 0.75f - (f - 1.0f) * (f - 1.0f);
+    w[2] = 0.5f * (f - 0.5f) * (f - 0.5f);
+}
+
+__device__ __forceinline__ int tile_block_index(const Box &bx, int cx, int cy, int cz) {
+    return (((cx >> kBlockShift) - bx.blo[0]) * bx.nb[1] + ((cy >> kBlockShift) - bx.blo[1])) * bx.nb[2] +
+           ((cz >> kBlockShift) - bx.blo[2]);
+}
+
+__device__ __forceinline__ M3f load_m3(const float *base, size_t cap, int i) {
+    M3f m;
+    m.c0 = mk(base[0 * cap + i], base[1 * cap + i], base[2 * cap + i]);
+    m.c1 = mk(base[3 * cap + i], base[4 * cap + i], base[5 * cap + i]);
+    m.c2 = mk(base[6 * cap + i], base[7 * cap + i], base[8 * cap + i]);
+    return m;
+}
+__device__ __forceinline__ void store_m3(float *base, size_t cap, int i, const M3f &m) {
+    base[0 * cap + i] = m.c0.x;
+    base[1 * cap + i] = m.c0.y;
+    base[2 * cap + i] = m.c0.z;
+    base[3 * cap + i] = m.c1.x;
+    base[4 * cap + i] = m.c1.y;
+    base[5 * cap + i] = m.c1.z;
+    base[6 * cap + i] = m.c2.x;
+    base[7 * cap + i] = m.c2.y;
+    base[8 * cap + i] = m.c2.z;
+}
+
+__device__ __forceinline__ void add_reaction(double *reactions, int oi, V3f center, V3f point, V3f impulse) {
+    V3f ang = cross(point - center, impulse);
+    double *r = reactions + 6 * oi;
+    atomicAdd(r + 0, static_cast<double>(impulse.x));
+    atomicAdd(r + 1, static_cast<double>(impulse.y));
+    atomicAdd(r + 2, static_cast<double>(impulse.z));
+    atomicAdd(r + 3, static_cast<double>(ang.x));
+    atomicAdd(r + 4, static_cast<double>(ang.y));
+    atomicAdd(r + 5, static_cast<double>(ang.z));
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(kThreads, 2)
+    k_transfer(ParticleSoA P, int n, const DevClass *__restrict__ classes, GridTable cur, GridTable next,
+               SimParams sp, const DevObstacle *__restrict__ obstacles, const float *__restrict__ planes,
+               double *reactions, uint32_t *status) {
+    __shared__ float s_gv[3][kTileMaxNodes];
+    __shared__ float s_sc[4][kTileMaxNodes];
+    __shared__ int s_blk[kMaxTileBlocks];
+    __shared__ int s_used[kMaxTileBlocks];
+    __shared__ int s_red[kThreads / 32][8];
+    __shared__ Box s_box;
+    __shared__ int s_abort;
+
+    if (threadIdx.x == 0) s_abort = (*reinterpret_cast<volatile uint32_t *>(status) & kFatal) != 0;
+    __syncthreads();
+    if (s_abort) return;
+
+    const size_t cap = P.cap;
+    const int i = blockIdx.x * kThreads + threadIdx.x;
+    const bool valid = i < n;
+    const float h = sp.h, inv_h = sp.inv_h, inv_d = sp.inv_d, dt = sp.dt;
+
+    V3f x = mk(0, 0, 0);
+    M3f F = m3_identity();
+    uint32_t cw = 0;
+    DevClass k;
+    k.mass = 0.f;
+    k.color = 0;
+    if (valid) {
+        x = mk(P.x[i], P.x[cap + i], P.x[2 * cap + i]);
+        F = load_m3(P.F, cap, i);
+        cw = P.cls[i];
+        k = classes[cw & kClassMask];
+    }
+    const bool fixed = (cw & kFixedBit) != 0;
+    V3f v = mk(0, 0, 0);
+    M3f Cm = m3_zero();
+
+    if (MODE == kModeP2G) {
+        if (valid) {
+            v = mk(P.v[i], P.v[cap + i], P.v[2 * cap + i]);
+            Cm = load_m3(P.C, cap, i);
+        }
+    } else {
+        // ------------------------------------------------------------- G2P
+        int b[3] = {base_cell(x.x, inv_h), base_cell(x.y, inv_h), base_cell(x.z, inv_h)};
+        reduce_box(valid, b, k.color, s_red, s_box);
+        const Box bx = s_box;
+        V3f gp = mk(x.x * inv_h, x.y * inv_h, x.z * inv_h);
+        V3f fx = mk(gp.x - static_cast<float>(b[0]), gp.y - static_cast<float>(b[1]), gp.z - static_cast<float>(b[2]));
+        float wx[3], wy[3], wz[3];
+        quad_weights(fx.x, wx);
+        quad_weights(fx.y, wy);
+        quad_weights(fx.z, wz);
+        V3f vel = mk(0, 0, 0);
+        M3f aff = m3_zero();
+        if (bx.ok) {
+            for (int t = threadIdx.x; t < bx.nbt; t += kThreads) {
+                int tz = t % bx.nb[2], ty = (t / bx.nb[2]) % bx.nb[1], tx = t / (bx.nb[2] * bx.nb[1]);
+                s_blk[t] = lookup_block(cur, block_key(bx.blo[0] + tx, bx.blo[1] + ty, bx.blo[2] + tz, bx.color));
+            }
+            __syncthreads();
+            for (int t = threadIdx.x; t < bx.nodes; t += kThreads) {
+                int tz = t % bx.dim[2], ty = (t / bx.dim[2]) % bx.dim[1], tx = t / (bx.dim[2] * bx.dim[1]);
+                int cx = bx.lo[0] + tx, cy = bx.lo[1] + ty, cz = bx.lo[2] + tz;
+                int id = s_blk[tile_block_index(bx, cx, cy, cz)];
+                float4 val = make_float4(0.f, 0.f, 0.f, 0.f);
+                if (id >= 0) val = __ldcg(cur.pool + static_cast<size_t>(id) * kNodesPerBlock + node_local(cx, cy, cz));
+                s_gv[0][t] = val.x;
+                s_gv[1][t] = val.y;
+                s_gv[2][t] = val.z;
+            }
+            __syncthreads();
+            if (valid && !fixed) {
+                int ox = b[0] - bx.lo[0], oy = b[1] - bx.lo[1], oz = b[2] - bx.lo[2];
+#pragma unroll
+                for (int a = 0; a < 3; ++a)
+#pragma unroll
+                    for (int c = 0; c < 3; ++c)
+#pragma unroll
+                        for (int e = 0; e < 3; ++e) {
+                            float w = wx[a] * wy[c] * wz[e];
+                            int t = ((ox + a) * bx.dim[1] + (oy + c)) * bx.dim[2] + (oz + e);
+                            V3f nv = mk(s_gv[0][t], s_gv[1][t], s_gv[2][t]);
+                            V3f dpos = mk((a - fx.x) * h, (c - fx.y) * h, (e - fx.z) * h);
+                            vel = vel + nv * w;
+                            float s = w * inv_d;
+                            aff.c0 = aff.c0 + nv * (dpos.x * s);
+                            aff.c1 = aff.c1 + nv * (dpos.y * s);
+                            aff.c2 = aff.c2 + nv * (dpos.z * s);
+                        }
+            }
+        } else if (valid && !fixed) {
+            unsigned long long last_key = kEmptyKey;
+            int last_id = -1;
+            for (int a = 0; a < 3; ++a)
+                for (int c = 0; c < 3; ++c)
+                    for (int e = 0; e < 3; ++e) {
+                        int cx = b[0] + a, cy = b[1] + c, cz = b[2] + e;
+                        unsigned long long key = block_key(cx >> kBlockShift, cy >> kBlockShift, cz >> kBlockShift, k.color);
+                        if (key != last_key) {
+                            last_key = key;
+                            last_id = lookup_block(cur, key);
+                        }
+                        float4 val = make_float4(0.f, 0.f, 0.f, 0.f);
+                        if (last_id >= 0)
+                            val = __ldcg(cur.pool + static_cast<size_t>(last_id) * kNodesPerBlock + node_local(cx, cy, cz));
+                        float w = wx[a] * wy[c] * wz[e];
+                        V3f nv = mk(val.x, val.y, val.z);
+                        V3f dpos = mk((a - fx.x) * h, (c - fx.y) * h, (e - fx.z) * h);
+                        vel = vel + nv * w;
+                        float s = w * inv_d;
+                        aff.c0 = aff.c0 + nv * (dpos.x * s);
+                        aff.c1 = aff.c1 + nv * (dpos.y * s);
+                        aff.c2 = aff.c2 + nv * (dpos.z * s);
+                    }
+        }
+
+        if (valid && !fixed) {
+            // Particle update (gpu.wgsl:885-1003; world.rs:443-463).
+            if (sp.apply_force) {
+                const size_t w = P.widx[i], fs = P.force_stride;
+                V3f f = mk(P.force[w], P.force[fs + w], P.force[2 * fs + w]);
+                vel = vel + f * (dt / k.mass);
+            }
+            vel = vel * expf(-k.damping * dt);
+            V3f pos = x + vel * dt;
+            float radius = k.radius;
+            if (sp.has_bounds) {
+                for (int a = 0; a < 3; ++a) {
+                    float lower = sp.bmin[a] + radius, upper = sp.bmax[a] - radius;
+                    float pa = comp(pos, a), va = comp(vel, a);
+                    if (pa < lower) {
+                        set_comp(pos, a, lower);
+                        set_comp(vel, a, fmaxf(va, 0.0f));
+                    } else if (pa > upper) {
+                        set_comp(pos, a, upper);
+                        set_comp(vel, a, fminf(va, 0.0f));
+                    }
+                }
+            }
+            for (int oi = 0; oi < sp.num_obstacles; ++oi) {
+                const DevObstacle &o = obstacles[oi];
+                if (!obstacle_may_contact(o, pos, radius)) continue;
+                V3f nrm;
+                float d = obstacle_surface(o, planes, pos, nrm);
+                if (d < radius) {
+                    pos = pos + nrm * (radius - d);
+                    V3f before = vel;
+                    vel = contact_velocity(o, pos, vel, nrm);
+                    if (sp.reactions)
+                        add_reaction(reactions, oi, mk(o.center[0], o.center[1], o.center[2]), pos - nrm * radius,
+                                     (before - vel) * k.mass);
+                }
+            }
+            M3f Fn = mul(add(m3_identity(), scale(aff, dt)), F);
+            if (k.kind == kMatFluid) {
+                float sc = cbrtf(fmaxf(det(Fn), 1e-9f));
+                Fn = scale(m3_identity(), sc);
+            }
+            // Resident failure detection (gpu.wgsl:946-994).
+            float ncx = floorf(__fsub_rn(__fmul_rn(pos.x, inv_h), 0.5f));
+            float ncy = floorf(__fsub_rn(__fmul_rn(pos.y, inv_h), 0.5f));
+            float ncz = floorf(__fsub_rn(__fmul_rn(pos.z, inv_h), 0.5f));
+            bool failed = !finite3(pos) || !finite3(vel) || !finite_m(aff) || !finite_m(Fn);
+            bool representable = ncx >= -131000.0f && ncx <= 131000.0f && ncy >= -131000.0f && ncy <= 131000.0f &&
+                                 ncz >= -131000.0f && ncz <= 131000.0f;
+            failed = failed || !representable;
+            if (!failed && sp.has_bounds) {
+                int nb3[3] = {static_cast<int>(ncx), static_cast<int>(ncy), static_cast<int>(ncz)};
+                for (int a = 0; a < 3; ++a)
+                    failed = failed || nb3[a] < sp.first_base[a] || nb3[a] > sp.last_base[a];
+            }
+            if (sp.resident_checks) {
+                if (k.kind == kMatCorotated) failed = failed || !regular_corotated(Fn);
+                failed = failed || dt * (k.wave + len(vel)) > 0.4f * h * (1.0f + 1e-4f);
+                if (failed) atomicOr(status, kStatusResident);
+            } else if (finite3(pos) && !representable) {
+                atomicOr(status, kStatusCapacity);  // finite but beyond the block key range
+            }
+            x = pos;
+            v = vel;
+            Cm = aff;
+            F = Fn;
+        }
+        if (valid) {
+            P.x[i] = x.x;
+            P.x[cap + i] = x.y;
+            P.x[2 * cap + i] = x.z;
+            if (!fixed) store_m3(P.F, cap, i, F);
+            if (MODE == kModeG2P) {
+                P.v[i] = v.x;
+                P.v[cap + i] = v.y;
+                P.v[2 * cap + i] = v.z;
+                store_m3(P.C, cap, i, Cm);
+            }
+        }
+        if (MODE == kModeG2P) return;
+        __syncthreads();  // the gather tile and box are reused below
+    }
+
+    // ----------------------------------------------------------------- P2G
+    int b[3] = {base_cell(x.x, inv_h), base_cell(x.y, inv_h), base_cell(x.z, inv_h)};
+    bool in_range = block_representable(b[0] >> kBlockShift, b[1] >> kBlockShift, b[2] >> kBlockShift) &&
+                    block_representable((b[0] + 2) >> kBlockShift, (b[1] + 2) >> kBlockShift, (b[2] + 2) >> kBlockShift);
+    bool active = valid && in_range;
+    if (valid && !in_range) atomicOr(status, sp.resident_checks ? kStatusResident : kStatusCapacity);
+    reduce_box(active, b, k.color, s_red, s_box);
+    const Box bx = s_box;
+    V3f gp = mk(x.x * inv_h, x.y * inv_h, x.z * inv_h);
+    V3f fx = mk(gp.x - static_cast<float>(b[0]), gp.y - static_cast<float>(b[1]), gp.z - static_cast<float>(b[2]));
+    float wx[3], wy[3], wz[3];
+    quad_weights(fx.x, wx);
+    quad_weights(fx.y, wy);
+    quad_weights(fx.z, wz);
+    M3f A = m3_zero();
+    V3f mv = mk(0, 0, 0);
+    if (active) {
+        M3f S = scaled_stress(k, F, Cm, -dt * inv_d);
+        A = add(S, scale(Cm, k.mass));
+        mv = v * k.mass;
+    }
+    if (bx.ok) {
+        for (int t = threadIdx.x; t < bx.nodes; t += kThreads) {
+            s_sc[0][t] = 0.f;
+            s_sc[1][t] = 0.f;
+            s_sc[2][t] = 0.f;
+            s_sc[3][t] = 0.f;
+        }
+        for (int t = threadIdx.x; t < bx.nbt; t += kThreads) s_used[t] = 0;
+        __syncthreads();
+        if (active) {
+            int ox = b[0] - bx.lo[0], oy = b[1] - bx.lo[1], oz = b[2] - bx.lo[2];
+#pragma unroll
+            for (int a = 0; a < 3; ++a)
+#pragma unroll
+                for (int c = 0; c < 3; ++c)
+#pragma unroll
+                    for (int e = 0; e < 3; ++e) {
+                        float w = wx[a] * wy[c] * wz[e];
+                        V3f dpos = mk((a - fx.x) * h, (c - fx.y) * h, (e - fx.z) * h);
+                        V3f mom = (mv + mul(A, dpos)) * w;
+                        int t = ((ox + a) * bx.dim[1] + (oy + c)) * bx.dim[2] + (oz + e);
+                        atomicAdd(&s_sc[0][t], w * k.mass);
+                        atomicAdd(&s_sc[1][t], mom.x);
+                        atomicAdd(&s_sc[2][t], mom.y);
+                        atomicAdd(&s_sc[3][t], mom.z);
+                    }
+        }
+        __syncthreads();
+        for (int t = threadIdx.x; t < bx.nodes; t += kThreads) {
+            if (s_sc[0][t] != 0.0f) {
+                int tz = t % bx.dim[2], ty = (t / bx.dim[2]) % bx.dim[1], tx = t / (bx.dim[2] * bx.dim[1]);
+                s_used[tile_block_index(bx, bx.lo[0] + tx, bx.lo[1] + ty, bx.lo[2] + tz)] = 1;
+            }
+        }
+        __syncthreads();
+        for (int t = threadIdx.x; t < bx.nbt; t += kThreads) {
+            int id = -1;
+            if (s_used[t]) {
+                int tz = t % bx.nb[2], ty = (t / bx.nb[2]) % bx.nb[1], tx = t / (bx.nb[2] * bx.nb[1]);
+                int gx = bx.blo[0] + tx, gy = bx.blo[1] + ty, gz = bx.blo[2] + tz;
+                id = find_or_insert_block(next, block_key(gx, gy, gz, bx.color),
+                                          make_int4(gx, gy, gz, static_cast<int>(bx.color)), status);
+            }
+            s_blk[t] = id;
+        }
+        __syncthreads();
+        for (int t = threadIdx.x; t < bx.nodes; t += kThreads) {
+            float m = s_sc[0][t];
+            if (m == 0.0f) continue;
+            int tz = t % bx.dim[2], ty = (t / bx.dim[2]) % bx.dim[1], tx = t / (bx.dim[2] * bx.dim[1]);
+            int cx = bx.lo[0] + tx, cy = bx.lo[1] + ty, cz = bx.lo[2] + tz;
+            int id = s_blk[tile_block_index(bx, cx, cy, cz)];
+            if (id < 0) continue;
+            atomicAdd(next.pool + static_cast<size_t>(id) * kNodesPerBlock + node_local(cx, cy, cz),
+                      make_float4(m, s_sc[1][t], s_sc[2][t], s_sc[3][t]));
+        }
+    } else if (active) {
+        unsigned long long last_key = kEmptyKey;
+        int last_id = -1;
+        for (int a = 0; a < 3; ++a)
+            for (int c = 0; c < 3; ++c)
+                for (int e = 0; e < 3; ++e) {
+                    int cx = b[0] + a, cy = b[1] + c, cz = b[2] + e;
+                    int gx = cx >> kBlockShift, gy = cy >> kBlockShift, gz = cz >> kBlockShift;
+                    unsigned long long key = block_key(gx, gy, gz, k.color);
+                    if (key != last_key) {
+                        last_key = key;
+                        last_id = find_or_insert_block(next, key, make_int4(gx, gy, gz, static_cast<int>(k.color)), status);
+                    }
+                    if (last_id < 0) continue;
+                    float w = wx[a] * wy[c] * wz[e];
+                    V3f dpos = mk((a - fx.x) * h, (c - fx.y) * h, (e - fx.z) * h);
+                    V3f mom = (mv + mul(A, dpos)) * w;
+                    atomicAdd(next.pool + static_cast<size_t>(last_id) * kNodesPerBlock + node_local(cx, cy, cz),
+                              make_float4(w * k.mass, mom.x, mom.y, mom.z));
+                }
+    }
+}
+
+// Grid update over all allocated blocks; also clears the table of the next step.
+__global__ void __launch_bounds__(256) k_grid(GridTable g, GridTable clr, SimParams sp,
+                                               const DevObstacle *__restrict__ obstacles,
+                                               const float *__restrict__ planes, double *reactions, uint32_t *status) {
+    __shared__ int s_abort;
+    if (threadIdx.x == 0) s_abort = (*reinterpret_cast<volatile uint32_t *>(status) & kFatal) != 0;
+    __syncthreads();
+    if (s_abort) return;
+    const size_t gtid = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    const size_t stride = static_cast<size_t>(gridDim.x) * blockDim.x;
+    if (clr.keys) {
+        for (size_t s = gtid; s <= clr.mask; s += stride) {
+            clr.keys[s] = kEmptyKey;
+            clr.vals[s] = kPendingId;
+        }
+        if (gtid == 0) *clr.count = 0;
+    }
+    uint32_t nblocks = min(*g.count, g.max_blocks);
+    const size_t nodes = static_cast<size_t>(nblocks) * kNodesPerBlock;
+    const float h = sp.h;
+    for (size_t node = gtid; node < nodes; node += stride) {
+        float4 mp = g.pool[node];
+        if (mp.x <= 0.0f) {
+            g.pool[node] = make_float4(0.f, 0.f, 0.f, 0.f);
+            continue;
+        }
+        int4 c = g.coords[node >> 6];
+        int l = static_cast<int>(node & 63);
+        int cx = c.x * 4 + (l >> 4), cy = c.y * 4 + ((l >> 2) & 3), cz = c.z * 4 + (l & 3);
+        V3f vel = mk(mp.y / mp.x + sp.gx * sp.dt, mp.z / mp.x + sp.gy * sp.dt, mp.w / mp.x + sp.gz * sp.dt);
+        V3f pos = mk(static_cast<float>(cx) * h, static_cast<float>(cy) * h, static_cast<float>(cz) * h);
+        if (sp.has_bounds) {
+            if (sp.wall_mode == 1) {
+                bool near = false;
+                for (int a = 0; a < 3; ++a)
+                    near = near || comp(pos, a) <= sp.bmin[a] + h || comp(pos, a) >= sp.bmax[a] - h;
+                if (near) vel = mk(0, 0, 0);
+            } else {
+                for (int a = 0; a < 3; ++a) {
+                    float pa = comp(pos, a), va = comp(vel, a);
+                    if ((pa <= sp.bmin[a] + h && va < 0.0f) || (pa >= sp.bmax[a] - h && va > 0.0f)) set_comp(vel, a, 0.0f);
+                }
+            }
+        }
+        for (int oi = 0; oi < sp.num_obstacles; ++oi) {
+            const DevObstacle &o = obstacles[oi];
+            if (!obstacle_may_contact(o, pos, h)) continue;
+            V3f nrm;
+            float d = obstacle_surface(o, planes, pos, nrm);
+            if (d <= h * (1.0f + 1e-5f)) {
+                V3f before = vel;
+                vel = contact_velocity(o, pos, vel, nrm);
+                if (sp.reactions)
+                    add_reaction(reactions, oi, mk(o.center[0], o.center[1], o.center[2]), pos - nrm * d,
+                                 (before - vel) * mp.x);
+            }
+        }
+        g.pool[node] = make_float4(vel.x, vel.y, vel.z, mp.x);
+    }
+}
+
+__global__ void k_clear_table(GridTable g) {
+    const size_t gtid = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    const size_t stride = static_cast<size_t>(gridDim.x) * blockDim.x;
+    for (size_t s = gtid; s <= g.mask; s += stride) {
+        g.keys[s] = kEmptyKey;
+        g.vals[s] = kPendingId;
+    }
+    if (gtid == 0) *g.count = 0;
+}
+
+__global__ void k_bin_keys(const float *x, size_t cap, int n, float inv_h, int32_t *cells, uint32_t *keys,
+                           uint32_t *vals) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int b0 = base_cell(x[i], inv_h), b1 = base_cell(x[cap + i], inv_h), b2 = base_cell(x[2 * cap + i], inv_h);
+    if (cells) {
+        cells[3 * i] = b0;
+        cells[3 * i + 1] = b1;
+        cells[3 * i + 2] = b2;
+    }
+    keys[i] = morton_block(b0 >> kBlockShift, b1 >> kBlockShift, b2 >> kBlockShift);
+    if (vals) vals[i] = static_cast<uint32_t>(i);
+}
+
+// dst[j] = src[perm[j]] for every particle field.
+__global__ void k_gather(ParticleSoA src, ParticleSoA dst, const uint32_t *__restrict__ perm, int n) {
+    int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    int s = static_cast<int>(perm[j]);
+    const size_t cs = src.cap, cd = dst.cap;
+    for (int c = 0; c < 3; ++c) {
+        dst.x[c * cd + j] = src.x[c * cs + s];
+        dst.v[c * cd + j] = src.v[c * cs + s];
+    }
+    for (int c = 0; c < 9; ++c) {
+        dst.C[c * cd + j] = src.C[c * cs + s];
+        dst.F[c * cd + j] = src.F[c * cs + s];
+    }
+    dst.cls[j] = src.cls[s];
+    dst.widx[j] = src.widx[s];
+}
+
+__global__ void k_dump_grid(GridTable g, int32_t *cells, float4 *values, uint32_t *count, uint32_t capacity) {
+    uint32_t nblocks = min(*g.count, g.max_blocks);
+    size_t nodes = static_cast<size_t>(nblocks) * kNodesPerBlock;
+    for (size_t node = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x; node < nodes;
+         node += static_cast<size_t>(gridDim.x) * blockDim.x) {
+        float4 mp = g.pool[node];
+        if (mp.x == 0.0f) continue;
+        uint32_t slot = atomicAdd(count, 1u);
+        if (slot >= capacity) continue;
+        int4 c = g.coords[node >> 6];
+        int l = static_cast<int>(node & 63);
+        cells[3 * slot] = c.x * 4 + (l >> 4);
+        cells[3 * slot + 1] = c.y * 4 + ((l >> 2) & 3);
+        cells[3 * slot + 2] = c.z * 4 + (l & 3);
+        values[slot] = mp;
+    }
+}
+
+__global__ void k_snapshot(ParticleSoA P, int n, const DevClass *__restrict__ classes, float4 *out) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const size_t cap = P.cap;
+    const DevClass &k = classes[P.cls[i] & kClassMask];
+    uint32_t w = P.widx[i];
+    out[2 * w] = make_float4(P.x[i], P.x[cap + i], P.x[2 * cap + i], k.mass);
+    out[2 * w + 1] = make_float4(P.v[i], P.v[cap + i], P.v[2 * cap + i], k.volume);
+}
+
+}  // namespace
+
+int device_sm_count() {
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    return sms;
+}
+
+void launch_transfer(int mode, const ParticleSoA &P, int n, const DevClass *classes, const GridTable &cur,
+                     const GridTable &next, const SimParams &sp, const DevObstacle *obstacles, const float *planes,
+                     double *reactions, uint32_t *status, cudaStream_t stream) {
+    if (n <= 0) return;
+    dim3 grid((n + kThreads - 1) / kThreads);
+    switch (mode) {
+    case kModeP2G:
+        k_transfer<kModeP2G><<<grid, kThreads, 0, stream>>>(P, n, classes, cur, next, sp, obstacles, planes, reactions, status);
+        break;
+    case kModeG2P2G:
+        k_transfer<kModeG2P2G><<<grid, kThreads, 0, stream>>>(P, n, classes, cur, next, sp, obstacles, planes, reactions, status);
+        break;
+    default:
+        k_transfer<kModeG2P><<<grid, kThreads, 0, stream>>>(P, n, classes, cur, next, sp, obstacles, planes, reactions, status);
+        break;
+    }
+}
+
+void launch_grid_update(const GridTable &g, const GridTable &clear, const SimParams &sp, const DevObstacle *obstacles,
+                        const float *planes, double *reactions, uint32_t *status, cudaStream_t stream) {
+    int blocks = device_sm_count() * 8;
+    k_grid<<<blocks, 256, 0, stream>>>(g, clear, sp, obstacles, planes, reactions, status);
+}
+
+void launch_clear_table(const GridTable &g, cudaStream_t stream) {
+    int blocks = device_sm_count() * 4;
+    k_clear_table<<<blocks, 256, 0, stream>>>(g);
+}
+
+void launch_bin_keys(const ParticleSoA &P, int n, const SimParams &sp, int32_t *cells, uint32_t *keys,
+                     cudaStream_t stream) {
+    if (n <= 0) return;
+    k_bin_keys<<<(n + 255) / 256, 256, 0, stream>>>(P.x, P.cap, n, sp.inv_h, cells, keys, nullptr);
+}
+
+void launch_resort(ParticleSoA &src, ParticleSoA &dst, int n, const SimParams &sp, SortBuffers &sb,
+                   cudaStream_t stream) {
+    if (n <= 0) return;
+    k_bin_keys<<<(n + 255) / 256, 256, 0, stream>>>(src.x, src.cap, n, sp.inv_h, nullptr, sb.keys[0], sb.vals[0]);
+    radix_sort_pairs(sb, n, 30, stream);
+    k_gather<<<(n + 255) / 256, 256, 0, stream>>>(src, dst, sb.vals[0], n);
+}
+
+void launch_dump_grid(const GridTable &g, int32_t *cells, float4 *values, uint32_t *count, uint32_t capacity,
+                      cudaStream_t stream) {
+    k_dump_grid<<<device_sm_count() * 4, 256, 0, stream>>>(g, cells, values, count, capacity);
+}
+
+void launch_snapshot(const ParticleSoA &P, int n, const DevClass *classes, float4 *out, cudaStream_t stream) {
+    if (n <= 0) return;
+    k_snapshot<<<(n + 255) / 256, 256, 0, stream>>>(P, n, classes, out);
+}
+
+}  // namespace tmpm
