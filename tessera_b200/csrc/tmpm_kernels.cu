@@ -136,13 +136,43 @@ __device__ __forceinline__ void add_reaction(double *reactions, int oi, V3f cent
     atomicAdd(r + 5, static_cast<double>(ang.z));
 }
 
+// Block-wide sums of two floats (all threads get the totals).
+__device__ __forceinline__ void block_sum2(float &a, float &b, float (*red)[2]) {
+    int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        a += __shfl_xor_sync(0xffffffffu, a, off);
+        b += __shfl_xor_sync(0xffffffffu, b, off);
+    }
+    if (lane == 0) {
+        red[warp][0] = a;
+        red[warp][1] = b;
+    }
+    __syncthreads();
+    a = 0.f;
+    b = 0.f;
+#pragma unroll
+    for (int w = 0; w < kThreads / 32; ++w) {
+        a += red[w][0];
+        b += red[w][1];
+    }
+}
+
+// Largest power of two s with total * s <= 2^30 (exponent clamped to the normal range).
+__device__ __forceinline__ float pow2_scale(float total) {
+    float e = floorf(30.0f - log2f(fmaxf(total, 1e-30f)));
+    e = fminf(fmaxf(e, -120.0f), 120.0f);
+    return exp2f(e);
+}
+
 template <int MODE>
 __global__ void __launch_bounds__(kThreads, 2)
     k_transfer(ParticleSoA P, int n, const DevClass *__restrict__ classes, GridTable cur, GridTable next,
                SimParams sp, const DevObstacle *__restrict__ obstacles, const float *__restrict__ planes,
                double *reactions, uint32_t *status) {
     __shared__ float s_gv[3][kTileMaxNodes];
-    __shared__ float s_sc[4][kTileMaxNodes];
+    __shared__ int s_sc[4][kTileMaxNodes];
+    __shared__ float s_fred[kThreads / 32][2];
     __shared__ int s_blk[kMaxTileBlocks];
     __shared__ int s_used[kMaxTileBlocks];
     __shared__ int s_red[kThreads / 32][8];
@@ -259,7 +289,7 @@ __global__ void __launch_bounds__(kThreads, 2)
             if (sp.apply_force) {
                 const size_t w = P.widx[i], fs = P.force_stride;
                 V3f f = mk(P.force[w], P.force[fs + w], P.force[2 * fs + w]);
-                vel = vel + f * (dt / k.mass);
+                vel = vel + mk(f.x / k.mass, f.y / k.mass, f.z / k.mass) * dt;  // force / mass * dt (gpu.wgsl:885)
             }
             vel = vel * expf(-k.damping * dt);
             V3f pos = x + vel * dt;
@@ -353,41 +383,70 @@ __global__ void __launch_bounds__(kThreads, 2)
     quad_weights(fx.z, wz);
     M3f A = m3_zero();
     V3f mv = mk(0, 0, 0);
+    float bound_m = 0.f, bound_p = 0.f;
     if (active) {
         M3f S = scaled_stress(k, F, Cm, -dt * inv_d);
         A = add(S, scale(Cm, k.mass));
         mv = v * k.mass;
+        // |(m v + A dpos)_i| <= |m v_i| + 1.5 h sum_j |A_ij| and a particle's 27 weights sum to one,
+        // so the chunk's sums bound every node value it produces.
+        float r0 = fabsf(A.c0.x) + fabsf(A.c1.x) + fabsf(A.c2.x);
+        float r1 = fabsf(A.c0.y) + fabsf(A.c1.y) + fabsf(A.c2.y);
+        float r2 = fabsf(A.c0.z) + fabsf(A.c1.z) + fabsf(A.c2.z);
+        bound_m = k.mass;
+        bound_p = fmaxf(fmaxf(fabsf(mv.x) + 1.5f * h * r0, fabsf(mv.y) + 1.5f * h * r1), fabsf(mv.z) + 1.5f * h * r2);
+        if (!(bound_p < 1e30f)) bound_p = 1e30f;  // non-finite state is flagged by the G2P checks
     }
     if (bx.ok) {
+        // Shared accumulation in 32-bit fixed point: integer shared atomics are
+        // native, float ones are not.  Power-of-two scales from the chunk bounds
+        // keep every node sum below 2^30 (no overflow) with unbiased rounding.
+        float tot_m = bound_m, tot_p = bound_p;
+        block_sum2(tot_m, tot_p, s_fred);
+        const float sm = pow2_scale(tot_m), spv = pow2_scale(tot_p);
         for (int t = threadIdx.x; t < bx.nodes; t += kThreads) {
-            s_sc[0][t] = 0.f;
-            s_sc[1][t] = 0.f;
-            s_sc[2][t] = 0.f;
-            s_sc[3][t] = 0.f;
+            s_sc[0][t] = 0;
+            s_sc[1][t] = 0;
+            s_sc[2][t] = 0;
+            s_sc[3][t] = 0;
         }
         for (int t = threadIdx.x; t < bx.nbt; t += kThreads) s_used[t] = 0;
         __syncthreads();
         if (active) {
-            int ox = b[0] - bx.lo[0], oy = b[1] - bx.lo[1], oz = b[2] - bx.lo[2];
+            const int ox = b[0] - bx.lo[0], oy = b[1] - bx.lo[1], oz = b[2] - bx.lo[2];
+            const float msc = k.mass * sm;
+            float dxs[3], dys[3], dzs[3];
 #pragma unroll
-            for (int a = 0; a < 3; ++a)
+            for (int a = 0; a < 3; ++a) {
+                dxs[a] = (a - fx.x) * h;
+                dys[a] = (a - fx.y) * h;
+                dzs[a] = (a - fx.z) * h;
+            }
 #pragma unroll
-                for (int c = 0; c < 3; ++c)
+            for (int a = 0; a < 3; ++a) {
+                const V3f qa = mv + A.c0 * dxs[a];
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+                    const V3f qac = qa + A.c1 * dys[c];
+                    const float wac = wx[a] * wy[c];
+                    const int row = ((ox + a) * bx.dim[1] + (oy + c)) * bx.dim[2] + oz;
 #pragma unroll
                     for (int e = 0; e < 3; ++e) {
-                        float w = wx[a] * wy[c] * wz[e];
-                        V3f dpos = mk((a - fx.x) * h, (c - fx.y) * h, (e - fx.z) * h);
-                        V3f mom = (mv + mul(A, dpos)) * w;
-                        int t = ((ox + a) * bx.dim[1] + (oy + c)) * bx.dim[2] + (oz + e);
-                        atomicAdd(&s_sc[0][t], w * k.mass);
-                        atomicAdd(&s_sc[1][t], mom.x);
-                        atomicAdd(&s_sc[2][t], mom.y);
-                        atomicAdd(&s_sc[3][t], mom.z);
+                        const V3f q = qac + A.c2 * dzs[e];
+                        const float w = wac * wz[e];
+                        const float wp = w * spv;
+                        const int t = row + e;
+                        atomicAdd(reinterpret_cast<unsigned *>(&s_sc[0][t]), static_cast<unsigned>(__float2int_rn(w * msc)));
+                        atomicAdd(reinterpret_cast<unsigned *>(&s_sc[1][t]), static_cast<unsigned>(__float2int_rn(q.x * wp)));
+                        atomicAdd(reinterpret_cast<unsigned *>(&s_sc[2][t]), static_cast<unsigned>(__float2int_rn(q.y * wp)));
+                        atomicAdd(reinterpret_cast<unsigned *>(&s_sc[3][t]), static_cast<unsigned>(__float2int_rn(q.z * wp)));
                     }
+                }
+            }
         }
         __syncthreads();
         for (int t = threadIdx.x; t < bx.nodes; t += kThreads) {
-            if (s_sc[0][t] != 0.0f) {
+            if ((s_sc[0][t] | s_sc[1][t] | s_sc[2][t] | s_sc[3][t]) != 0) {
                 int tz = t % bx.dim[2], ty = (t / bx.dim[2]) % bx.dim[1], tx = t / (bx.dim[2] * bx.dim[1]);
                 s_used[tile_block_index(bx, bx.lo[0] + tx, bx.lo[1] + ty, bx.lo[2] + tz)] = 1;
             }
@@ -404,15 +463,17 @@ __global__ void __launch_bounds__(kThreads, 2)
             s_blk[t] = id;
         }
         __syncthreads();
+        const float inv_sm = 1.0f / sm, inv_sp = 1.0f / spv;
         for (int t = threadIdx.x; t < bx.nodes; t += kThreads) {
-            float m = s_sc[0][t];
-            if (m == 0.0f) continue;
+            const int m = s_sc[0][t], px = s_sc[1][t], py = s_sc[2][t], pz = s_sc[3][t];
+            if ((m | px | py | pz) == 0) continue;
             int tz = t % bx.dim[2], ty = (t / bx.dim[2]) % bx.dim[1], tx = t / (bx.dim[2] * bx.dim[1]);
             int cx = bx.lo[0] + tx, cy = bx.lo[1] + ty, cz = bx.lo[2] + tz;
             int id = s_blk[tile_block_index(bx, cx, cy, cz)];
             if (id < 0) continue;
             atomicAdd(next.pool + static_cast<size_t>(id) * kNodesPerBlock + node_local(cx, cy, cz),
-                      make_float4(m, s_sc[1][t], s_sc[2][t], s_sc[3][t]));
+                      make_float4(static_cast<float>(m) * inv_sm, static_cast<float>(px) * inv_sp,
+                                  static_cast<float>(py) * inv_sp, static_cast<float>(pz) * inv_sp));
         }
     } else if (active) {
         unsigned long long last_key = kEmptyKey;

@@ -272,15 +272,23 @@ def test_capacity_exhaustion_reports_capacity_and_keeps_world():  # gpu.rs:2872-
 
 
 def test_non_finite_direct_step_reports_non_finite_and_keeps_world():
-    params = make_params(0.1, bounds=REF_BOUNDS)
+    # Unbounded: with walls the clamp would turn the infinite velocity into a finite state.
+    params = make_params(0.1)
     p = density_particles([(0.5, 0.5, 0.5)], 0.04, 1000.0, MAT_NEO_HOOKEAN, (2000.0, 0.2))
     s = Session(params, p, 1e-4)
-    s.set_particle_force(0, (3.0e38, 0.0, 0.0))  # f / m overflows f32
+    s.set_particle_force(0, (3.0e38, 0.0, 0.0))  # force / mass overflows f32
     before = s.particles()
     with pytest.raises(TesseraError) as e:
         s.step_cfl(1e-4)
     assert e.value.status == TMPM_ERR_NON_FINITE_STATE
     assert np.array_equal(s.particles().position, before.position)
+    # the f64 reference path fails too (its overflow comes one step later, in x += v dt)
+    q = p.copy()
+    q.force[0, 0] = 1.0e308
+    cpu = O.OracleWorld(params, q)
+    with pytest.raises(O.OracleError) as oe:
+        cpu.step(1e-4)
+    assert oe.value.status == TMPM_ERR_NON_FINITE_STATE
 
 
 def test_pending_steps_block_edits_and_synchronize_applies():  # gpu.rs:3306-3409
