@@ -13,7 +13,7 @@ import subprocess
 from ._abi import TmpmObstacle, TmpmParams, TmpmParticleArrays, TmpmSessionOptions
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "libtmpm.so")
+LIB_PATH = os.environ.get("TMPM_LIB_PATH") or os.path.join(_HERE, "libtmpm.so")
 _lib = None
 
 

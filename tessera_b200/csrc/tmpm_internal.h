@@ -39,6 +39,9 @@ constexpr int kMatNeoHookean = 1;
 constexpr int kMatFluid = 2;
 constexpr int kMatCorotated = 3;
 
+constexpr int kTransferThreads = 256;  // particles per CTA of the transfer kernels
+constexpr int kCacheStride = 80;       // per-CTA record: 8-int box header + up to 64 block ids
+
 constexpr uint32_t kFixedBit = 0x80000000u;
 constexpr uint32_t kClassMask = 0x7FFFFFFFu;
 
@@ -109,10 +112,13 @@ struct SortBuffers {
 enum TransferMode { kModeP2G = 0, kModeG2P2G = 1, kModeG2P = 2 };
 
 // Launchers (tmpm_kernels.cu).  All run on `stream`.
+// `cur` and `next` share one hash table (block ids are stable within a batch)
+// and differ in their node pools; `cache` holds kCacheStride ints per CTA.
 void launch_transfer(int mode, const ParticleSoA &P, int n, const DevClass *classes, const GridTable &cur,
                      const GridTable &next, const SimParams &sp, const DevObstacle *obstacles,
-                     const float *planes, double *reactions, uint32_t *status, cudaStream_t stream);
-void launch_grid_update(const GridTable &g, const GridTable &clear, const SimParams &sp,
+                     const float *planes, double *reactions, uint32_t *status, int *cache, cudaStream_t stream);
+// Grid update of `g`'s pool; also zeroes the same blocks in `next`'s pool.
+void launch_grid_update(const GridTable &g, const GridTable &next, const SimParams &sp,
                         const DevObstacle *obstacles, const float *planes, double *reactions,
                         uint32_t *status, cudaStream_t stream);
 void launch_clear_table(const GridTable &g, cudaStream_t stream);

@@ -19,14 +19,19 @@
 
 #include "tmpm_device.cuh"
 
+#ifndef TMPM_TRANSFER_MIN_BLOCKS
+#define TMPM_TRANSFER_MIN_BLOCKS 3  // CTAs per SM the transfer kernels are compiled for (measured best)
+#endif
+
 namespace tmpm {
 
 namespace {
 
-constexpr int kThreads = 256;
+constexpr int kThreads = kTransferThreads;
 constexpr int kTileMaxDim = 12;
 constexpr int kTileMaxNodes = 1024;
 constexpr int kMaxTileBlocks = 64;
+constexpr int kCacheHeader = 16;
 constexpr uint32_t kFatal = kStatusCapacity | kStatusTimeout | kStatusResident;
 
 struct Box {
@@ -166,27 +171,33 @@ __device__ __forceinline__ float pow2_scale(float total) {
 }
 
 template <int MODE>
-__global__ void __launch_bounds__(kThreads, 2)
+__global__ void __launch_bounds__(kThreads, TMPM_TRANSFER_MIN_BLOCKS)
     k_transfer(ParticleSoA P, int n, const DevClass *__restrict__ classes, GridTable cur, GridTable next,
                SimParams sp, const DevObstacle *__restrict__ obstacles, const float *__restrict__ planes,
-               double *reactions, uint32_t *status) {
-    __shared__ float s_gv[3][kTileMaxNodes];
-    __shared__ int s_sc[4][kTileMaxNodes];
+               double *reactions, uint32_t *status, int *__restrict__ cache) {
+    __shared__ float4 s_gv[kTileMaxNodes];
+    __shared__ __align__(16) int s_sc[4][kTileMaxNodes];
     __shared__ float s_fred[kThreads / 32][2];
     __shared__ int s_blk[kMaxTileBlocks];
+    __shared__ int s_blk2[kMaxTileBlocks];
     __shared__ int s_used[kMaxTileBlocks];
     __shared__ int s_red[kThreads / 32][8];
     __shared__ Box s_box;
     __shared__ int s_abort;
 
-    if (threadIdx.x == 0) s_abort = (*reinterpret_cast<volatile uint32_t *>(status) & kFatal) != 0;
-    __syncthreads();
-    if (s_abort) return;
-
     const size_t cap = P.cap;
     const int i = blockIdx.x * kThreads + threadIdx.x;
     const bool valid = i < n;
     const float h = sp.h, inv_h = sp.inv_h, inv_d = sp.inv_d, dt = sp.dt;
+    int *const cc = cache + static_cast<size_t>(blockIdx.x) * kCacheStride;
+
+    if (threadIdx.x == 0) s_abort = (*reinterpret_cast<volatile uint32_t *>(status) & kFatal) != 0;
+    if (MODE != kModeG2P) {
+        // The scatter tile is zeroed up front; the first barrier of the kernel orders it.
+        int4 *z = reinterpret_cast<int4 *>(&s_sc[0][0]);
+        for (int t = threadIdx.x; t < kTileMaxNodes; t += kThreads) z[t] = make_int4(0, 0, 0, 0);
+        for (int t = threadIdx.x; t < kMaxTileBlocks; t += kThreads) s_used[t] = 0;
+    }
 
     V3f x = mk(0, 0, 0);
     M3f F = m3_identity();
@@ -203,6 +214,8 @@ __global__ void __launch_bounds__(kThreads, 2)
     const bool fixed = (cw & kFixedBit) != 0;
     V3f v = mk(0, 0, 0);
     M3f Cm = m3_zero();
+    Box gbox;
+    gbox.ok = 0;
 
     if (MODE == kModeP2G) {
         if (valid) {
@@ -211,77 +224,121 @@ __global__ void __launch_bounds__(kThreads, 2)
         }
     } else {
         // ------------------------------------------------------------- G2P
-        int b[3] = {base_cell(x.x, inv_h), base_cell(x.y, inv_h), base_cell(x.z, inv_h)};
-        reduce_box(valid, b, k.color, s_red, s_box);
-        const Box bx = s_box;
-        V3f gp = mk(x.x * inv_h, x.y * inv_h, x.z * inv_h);
-        V3f fx = mk(gp.x - static_cast<float>(b[0]), gp.y - static_cast<float>(b[1]), gp.z - static_cast<float>(b[2]));
+        const int b[3] = {base_cell(x.x, inv_h), base_cell(x.y, inv_h), base_cell(x.z, inv_h)};
+        // The previous P2G of this CTA recorded the box and block ids for these
+        // very positions (ids are stable within a batch), so normally no box
+        // reduction and no hash lookup is needed.  A record that does not
+        // cover every particle sends the CTA through the general path.
+        bool use_cache = cc[0] == 1;
+        Box bx;
+        for (int attempt = 0; attempt < 2; ++attempt) {
+            if (use_cache) {
+                bx.lo[0] = cc[8];
+                bx.lo[1] = cc[9];
+                bx.lo[2] = cc[10];
+                bx.dim[0] = cc[11];
+                bx.dim[1] = cc[12];
+                bx.dim[2] = cc[13];
+                bx.blo[0] = cc[1];
+                bx.blo[1] = cc[2];
+                bx.blo[2] = cc[3];
+                bx.nb[0] = cc[4];
+                bx.nb[1] = cc[5];
+                bx.nb[2] = cc[6];
+                bx.color = static_cast<uint32_t>(cc[7]);
+                bx.nodes = cc[14];
+                bx.nbt = cc[15];
+                bx.ok = 1;
+            } else {
+                reduce_box(valid, b, k.color, s_red, s_box);
+                bx = s_box;
+                if (bx.ok) {
+                    for (int t = threadIdx.x; t < bx.nbt; t += kThreads) {
+                        int tz = t % bx.nb[2], ty = (t / bx.nb[2]) % bx.nb[1], tx = t / (bx.nb[2] * bx.nb[1]);
+                        s_blk[t] = lookup_block(cur, block_key(bx.blo[0] + tx, bx.blo[1] + ty, bx.blo[2] + tz, bx.color));
+                    }
+                    __syncthreads();
+                }
+            }
+            bool bad = use_cache && valid &&
+                       (b[0] < bx.lo[0] || b[1] < bx.lo[1] || b[2] < bx.lo[2] || b[0] + 2 >= bx.lo[0] + bx.dim[0] ||
+                        b[1] + 2 >= bx.lo[1] + bx.dim[1] || b[2] + 2 >= bx.lo[2] + bx.dim[2] || k.color != bx.color);
+            if (bx.ok && !bad) {
+                for (int t = threadIdx.x; t < bx.nodes; t += kThreads) {
+                    int tz = t % bx.dim[2], ty = (t / bx.dim[2]) % bx.dim[1], tx = t / (bx.dim[2] * bx.dim[1]);
+                    int cx = bx.lo[0] + tx, cy = bx.lo[1] + ty, cz = bx.lo[2] + tz;
+                    int tb = tile_block_index(bx, cx, cy, cz);
+                    int id = use_cache ? cc[kCacheHeader + tb] : s_blk[tb];
+                    if (use_cache) s_blk[tb] = id;
+                    float4 val = make_float4(0.f, 0.f, 0.f, 0.f);
+                    if (id >= 0) val = __ldcg(cur.pool + static_cast<size_t>(id) * kNodesPerBlock + node_local(cx, cy, cz));
+                    s_gv[t] = val;
+                }
+            }
+            bad = __syncthreads_or(bad) != 0;
+            if (!bad) break;
+            use_cache = false;
+        }
+        if (s_abort) return;
+        const V3f gp = mk(x.x * inv_h, x.y * inv_h, x.z * inv_h);
+        const V3f fx = mk(gp.x - static_cast<float>(b[0]), gp.y - static_cast<float>(b[1]), gp.z - static_cast<float>(b[2]));
         float wx[3], wy[3], wz[3];
         quad_weights(fx.x, wx);
         quad_weights(fx.y, wy);
         quad_weights(fx.z, wz);
         V3f vel = mk(0, 0, 0);
         M3f aff = m3_zero();
-        if (bx.ok) {
-            for (int t = threadIdx.x; t < bx.nbt; t += kThreads) {
-                int tz = t % bx.nb[2], ty = (t / bx.nb[2]) % bx.nb[1], tx = t / (bx.nb[2] * bx.nb[1]);
-                s_blk[t] = lookup_block(cur, block_key(bx.blo[0] + tx, bx.blo[1] + ty, bx.blo[2] + tz, bx.color));
+        if (valid && !fixed) {
+            float dxs[3], dys[3], dzs[3];
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+                dxs[a] = (a - fx.x) * h * inv_d;
+                dys[a] = (a - fx.y) * h * inv_d;
+                dzs[a] = (a - fx.z) * h * inv_d;
             }
-            __syncthreads();
-            for (int t = threadIdx.x; t < bx.nodes; t += kThreads) {
-                int tz = t % bx.dim[2], ty = (t / bx.dim[2]) % bx.dim[1], tx = t / (bx.dim[2] * bx.dim[1]);
-                int cx = bx.lo[0] + tx, cy = bx.lo[1] + ty, cz = bx.lo[2] + tz;
-                int id = s_blk[tile_block_index(bx, cx, cy, cz)];
-                float4 val = make_float4(0.f, 0.f, 0.f, 0.f);
-                if (id >= 0) val = __ldcg(cur.pool + static_cast<size_t>(id) * kNodesPerBlock + node_local(cx, cy, cz));
-                s_gv[0][t] = val.x;
-                s_gv[1][t] = val.y;
-                s_gv[2][t] = val.z;
-            }
-            __syncthreads();
-            if (valid && !fixed) {
-                int ox = b[0] - bx.lo[0], oy = b[1] - bx.lo[1], oz = b[2] - bx.lo[2];
+            if (bx.ok) {
+                const int ox = b[0] - bx.lo[0], oy = b[1] - bx.lo[1], oz = b[2] - bx.lo[2];
 #pragma unroll
                 for (int a = 0; a < 3; ++a)
 #pragma unroll
-                    for (int c = 0; c < 3; ++c)
+                    for (int c = 0; c < 3; ++c) {
+                        const float wac = wx[a] * wy[c];
+                        const int row = ((ox + a) * bx.dim[1] + (oy + c)) * bx.dim[2] + oz;
 #pragma unroll
                         for (int e = 0; e < 3; ++e) {
-                            float w = wx[a] * wy[c] * wz[e];
-                            int t = ((ox + a) * bx.dim[1] + (oy + c)) * bx.dim[2] + (oz + e);
-                            V3f nv = mk(s_gv[0][t], s_gv[1][t], s_gv[2][t]);
-                            V3f dpos = mk((a - fx.x) * h, (c - fx.y) * h, (e - fx.z) * h);
+                            const float w = wac * wz[e];
+                            const float4 g4 = s_gv[row + e];
+                            const V3f nv = mk(g4.x, g4.y, g4.z);
                             vel = vel + nv * w;
-                            float s = w * inv_d;
-                            aff.c0 = aff.c0 + nv * (dpos.x * s);
-                            aff.c1 = aff.c1 + nv * (dpos.y * s);
-                            aff.c2 = aff.c2 + nv * (dpos.z * s);
+                            aff.c0 = aff.c0 + nv * (dxs[a] * w);
+                            aff.c1 = aff.c1 + nv * (dys[c] * w);
+                            aff.c2 = aff.c2 + nv * (dzs[e] * w);
+                        }
+                    }
+            } else {
+                unsigned long long last_key = kEmptyKey;
+                int last_id = -1;
+                for (int a = 0; a < 3; ++a)
+                    for (int c = 0; c < 3; ++c)
+                        for (int e = 0; e < 3; ++e) {
+                            int cx = b[0] + a, cy = b[1] + c, cz = b[2] + e;
+                            unsigned long long key =
+                                block_key(cx >> kBlockShift, cy >> kBlockShift, cz >> kBlockShift, k.color);
+                            if (key != last_key) {
+                                last_key = key;
+                                last_id = lookup_block(cur, key);
+                            }
+                            float4 val = make_float4(0.f, 0.f, 0.f, 0.f);
+                            if (last_id >= 0)
+                                val = __ldcg(cur.pool + static_cast<size_t>(last_id) * kNodesPerBlock + node_local(cx, cy, cz));
+                            const float w = wx[a] * wy[c] * wz[e];
+                            const V3f nv = mk(val.x, val.y, val.z);
+                            vel = vel + nv * w;
+                            aff.c0 = aff.c0 + nv * (dxs[a] * w);
+                            aff.c1 = aff.c1 + nv * (dys[c] * w);
+                            aff.c2 = aff.c2 + nv * (dzs[e] * w);
                         }
             }
-        } else if (valid && !fixed) {
-            unsigned long long last_key = kEmptyKey;
-            int last_id = -1;
-            for (int a = 0; a < 3; ++a)
-                for (int c = 0; c < 3; ++c)
-                    for (int e = 0; e < 3; ++e) {
-                        int cx = b[0] + a, cy = b[1] + c, cz = b[2] + e;
-                        unsigned long long key = block_key(cx >> kBlockShift, cy >> kBlockShift, cz >> kBlockShift, k.color);
-                        if (key != last_key) {
-                            last_key = key;
-                            last_id = lookup_block(cur, key);
-                        }
-                        float4 val = make_float4(0.f, 0.f, 0.f, 0.f);
-                        if (last_id >= 0)
-                            val = __ldcg(cur.pool + static_cast<size_t>(last_id) * kNodesPerBlock + node_local(cx, cy, cz));
-                        float w = wx[a] * wy[c] * wz[e];
-                        V3f nv = mk(val.x, val.y, val.z);
-                        V3f dpos = mk((a - fx.x) * h, (c - fx.y) * h, (e - fx.z) * h);
-                        vel = vel + nv * w;
-                        float s = w * inv_d;
-                        aff.c0 = aff.c0 + nv * (dpos.x * s);
-                        aff.c1 = aff.c1 + nv * (dpos.y * s);
-                        aff.c2 = aff.c2 + nv * (dpos.z * s);
-                    }
         }
 
         if (valid && !fixed) {
@@ -293,7 +350,7 @@ __global__ void __launch_bounds__(kThreads, 2)
             }
             vel = vel * expf(-k.damping * dt);
             V3f pos = x + vel * dt;
-            float radius = k.radius;
+            const float radius = k.radius;
             if (sp.has_bounds) {
                 for (int a = 0; a < 3; ++a) {
                     float lower = sp.bmin[a] + radius, upper = sp.bmax[a] - radius;
@@ -364,19 +421,21 @@ __global__ void __launch_bounds__(kThreads, 2)
             }
         }
         if (MODE == kModeG2P) return;
-        __syncthreads();  // the gather tile and box are reused below
+        gbox = bx;
     }
 
     // ----------------------------------------------------------------- P2G
-    int b[3] = {base_cell(x.x, inv_h), base_cell(x.y, inv_h), base_cell(x.z, inv_h)};
-    bool in_range = block_representable(b[0] >> kBlockShift, b[1] >> kBlockShift, b[2] >> kBlockShift) &&
-                    block_representable((b[0] + 2) >> kBlockShift, (b[1] + 2) >> kBlockShift, (b[2] + 2) >> kBlockShift);
-    bool active = valid && in_range;
+    const int b[3] = {base_cell(x.x, inv_h), base_cell(x.y, inv_h), base_cell(x.z, inv_h)};
+    const bool in_range =
+        block_representable(b[0] >> kBlockShift, b[1] >> kBlockShift, b[2] >> kBlockShift) &&
+        block_representable((b[0] + 2) >> kBlockShift, (b[1] + 2) >> kBlockShift, (b[2] + 2) >> kBlockShift);
+    const bool active = valid && in_range;
     if (valid && !in_range) atomicOr(status, sp.resident_checks ? kStatusResident : kStatusCapacity);
     reduce_box(active, b, k.color, s_red, s_box);
+    if (MODE == kModeP2G && s_abort) return;
     const Box bx = s_box;
-    V3f gp = mk(x.x * inv_h, x.y * inv_h, x.z * inv_h);
-    V3f fx = mk(gp.x - static_cast<float>(b[0]), gp.y - static_cast<float>(b[1]), gp.z - static_cast<float>(b[2]));
+    const V3f gp = mk(x.x * inv_h, x.y * inv_h, x.z * inv_h);
+    const V3f fx = mk(gp.x - static_cast<float>(b[0]), gp.y - static_cast<float>(b[1]), gp.z - static_cast<float>(b[2]));
     float wx[3], wy[3], wz[3];
     quad_weights(fx.x, wx);
     quad_weights(fx.y, wy);
@@ -404,14 +463,6 @@ __global__ void __launch_bounds__(kThreads, 2)
         float tot_m = bound_m, tot_p = bound_p;
         block_sum2(tot_m, tot_p, s_fred);
         const float sm = pow2_scale(tot_m), spv = pow2_scale(tot_p);
-        for (int t = threadIdx.x; t < bx.nodes; t += kThreads) {
-            s_sc[0][t] = 0;
-            s_sc[1][t] = 0;
-            s_sc[2][t] = 0;
-            s_sc[3][t] = 0;
-        }
-        for (int t = threadIdx.x; t < bx.nbt; t += kThreads) s_used[t] = 0;
-        __syncthreads();
         if (active) {
             const int ox = b[0] - bx.lo[0], oy = b[1] - bx.lo[1], oz = b[2] - bx.lo[2];
             const float msc = k.mass * sm;
@@ -443,13 +494,18 @@ __global__ void __launch_bounds__(kThreads, 2)
                     }
                 }
             }
-        }
-        __syncthreads();
-        for (int t = threadIdx.x; t < bx.nodes; t += kThreads) {
-            if ((s_sc[0][t] | s_sc[1][t] | s_sc[2][t] | s_sc[3][t]) != 0) {
-                int tz = t % bx.dim[2], ty = (t / bx.dim[2]) % bx.dim[1], tx = t / (bx.dim[2] * bx.dim[1]);
-                s_used[tile_block_index(bx, bx.lo[0] + tx, bx.lo[1] + ty, bx.lo[2] + tz)] = 1;
-            }
+            // mark the (at most 8) blocks this particle's stencil touches
+            const int bx0 = (b[0] >> kBlockShift) - bx.blo[0], bx1 = ((b[0] + 2) >> kBlockShift) - bx.blo[0];
+            const int by0 = (b[1] >> kBlockShift) - bx.blo[1], by1 = ((b[1] + 2) >> kBlockShift) - bx.blo[1];
+            const int bz0 = (b[2] >> kBlockShift) - bx.blo[2], bz1 = ((b[2] + 2) >> kBlockShift) - bx.blo[2];
+            s_used[(bx0 * bx.nb[1] + by0) * bx.nb[2] + bz0] = 1;
+            s_used[(bx0 * bx.nb[1] + by0) * bx.nb[2] + bz1] = 1;
+            s_used[(bx0 * bx.nb[1] + by1) * bx.nb[2] + bz0] = 1;
+            s_used[(bx0 * bx.nb[1] + by1) * bx.nb[2] + bz1] = 1;
+            s_used[(bx1 * bx.nb[1] + by0) * bx.nb[2] + bz0] = 1;
+            s_used[(bx1 * bx.nb[1] + by0) * bx.nb[2] + bz1] = 1;
+            s_used[(bx1 * bx.nb[1] + by1) * bx.nb[2] + bz0] = 1;
+            s_used[(bx1 * bx.nb[1] + by1) * bx.nb[2] + bz1] = 1;
         }
         __syncthreads();
         for (int t = threadIdx.x; t < bx.nbt; t += kThreads) {
@@ -457,10 +513,36 @@ __global__ void __launch_bounds__(kThreads, 2)
             if (s_used[t]) {
                 int tz = t % bx.nb[2], ty = (t / bx.nb[2]) % bx.nb[1], tx = t / (bx.nb[2] * bx.nb[1]);
                 int gx = bx.blo[0] + tx, gy = bx.blo[1] + ty, gz = bx.blo[2] + tz;
-                id = find_or_insert_block(next, block_key(gx, gy, gz, bx.color),
-                                          make_int4(gx, gy, gz, static_cast<int>(bx.color)), status);
+                // reuse the id the G2P box already holds for this block (same table)
+                if (gbox.ok && gbox.color == bx.color) {
+                    int rx = gx - gbox.blo[0], ry = gy - gbox.blo[1], rz = gz - gbox.blo[2];
+                    if (rx >= 0 && ry >= 0 && rz >= 0 && rx < gbox.nb[0] && ry < gbox.nb[1] && rz < gbox.nb[2])
+                        id = s_blk[(rx * gbox.nb[1] + ry) * gbox.nb[2] + rz];
+                }
+                if (id < 0)
+                    id = find_or_insert_block(next, block_key(gx, gy, gz, bx.color),
+                                              make_int4(gx, gy, gz, static_cast<int>(bx.color)), status);
             }
-            s_blk[t] = id;
+            s_blk2[t] = id;
+            cc[kCacheHeader + t] = id;
+        }
+        if (threadIdx.x == 0) {
+            cc[0] = 1;
+            cc[1] = bx.blo[0];
+            cc[2] = bx.blo[1];
+            cc[3] = bx.blo[2];
+            cc[4] = bx.nb[0];
+            cc[5] = bx.nb[1];
+            cc[6] = bx.nb[2];
+            cc[7] = static_cast<int>(bx.color);
+            cc[8] = bx.lo[0];
+            cc[9] = bx.lo[1];
+            cc[10] = bx.lo[2];
+            cc[11] = bx.dim[0];
+            cc[12] = bx.dim[1];
+            cc[13] = bx.dim[2];
+            cc[14] = bx.nodes;
+            cc[15] = bx.nbt;
         }
         __syncthreads();
         const float inv_sm = 1.0f / sm, inv_sp = 1.0f / spv;
@@ -469,37 +551,40 @@ __global__ void __launch_bounds__(kThreads, 2)
             if ((m | px | py | pz) == 0) continue;
             int tz = t % bx.dim[2], ty = (t / bx.dim[2]) % bx.dim[1], tx = t / (bx.dim[2] * bx.dim[1]);
             int cx = bx.lo[0] + tx, cy = bx.lo[1] + ty, cz = bx.lo[2] + tz;
-            int id = s_blk[tile_block_index(bx, cx, cy, cz)];
+            int id = s_blk2[tile_block_index(bx, cx, cy, cz)];
             if (id < 0) continue;
             atomicAdd(next.pool + static_cast<size_t>(id) * kNodesPerBlock + node_local(cx, cy, cz),
                       make_float4(static_cast<float>(m) * inv_sm, static_cast<float>(px) * inv_sp,
                                   static_cast<float>(py) * inv_sp, static_cast<float>(pz) * inv_sp));
         }
-    } else if (active) {
-        unsigned long long last_key = kEmptyKey;
-        int last_id = -1;
-        for (int a = 0; a < 3; ++a)
-            for (int c = 0; c < 3; ++c)
-                for (int e = 0; e < 3; ++e) {
-                    int cx = b[0] + a, cy = b[1] + c, cz = b[2] + e;
-                    int gx = cx >> kBlockShift, gy = cy >> kBlockShift, gz = cz >> kBlockShift;
-                    unsigned long long key = block_key(gx, gy, gz, k.color);
-                    if (key != last_key) {
-                        last_key = key;
-                        last_id = find_or_insert_block(next, key, make_int4(gx, gy, gz, static_cast<int>(k.color)), status);
+    } else {
+        if (threadIdx.x == 0) cc[0] = 0;
+        if (active) {
+            unsigned long long last_key = kEmptyKey;
+            int last_id = -1;
+            for (int a = 0; a < 3; ++a)
+                for (int c = 0; c < 3; ++c)
+                    for (int e = 0; e < 3; ++e) {
+                        int cx = b[0] + a, cy = b[1] + c, cz = b[2] + e;
+                        int gx = cx >> kBlockShift, gy = cy >> kBlockShift, gz = cz >> kBlockShift;
+                        unsigned long long key = block_key(gx, gy, gz, k.color);
+                        if (key != last_key) {
+                            last_key = key;
+                            last_id = find_or_insert_block(next, key, make_int4(gx, gy, gz, static_cast<int>(k.color)), status);
+                        }
+                        if (last_id < 0) continue;
+                        float w = wx[a] * wy[c] * wz[e];
+                        V3f dpos = mk((a - fx.x) * h, (c - fx.y) * h, (e - fx.z) * h);
+                        V3f mom = (mv + mul(A, dpos)) * w;
+                        atomicAdd(next.pool + static_cast<size_t>(last_id) * kNodesPerBlock + node_local(cx, cy, cz),
+                                  make_float4(w * k.mass, mom.x, mom.y, mom.z));
                     }
-                    if (last_id < 0) continue;
-                    float w = wx[a] * wy[c] * wz[e];
-                    V3f dpos = mk((a - fx.x) * h, (c - fx.y) * h, (e - fx.z) * h);
-                    V3f mom = (mv + mul(A, dpos)) * w;
-                    atomicAdd(next.pool + static_cast<size_t>(last_id) * kNodesPerBlock + node_local(cx, cy, cz),
-                              make_float4(w * k.mass, mom.x, mom.y, mom.z));
-                }
+        }
     }
 }
 
-// Grid update over all allocated blocks; also clears the table of the next step.
-__global__ void __launch_bounds__(256) k_grid(GridTable g, GridTable clr, SimParams sp,
+// Grid update over all allocated blocks; also zeroes those blocks in the other pool.
+__global__ void __launch_bounds__(256) k_grid(GridTable g, GridTable nxt, SimParams sp,
                                                const DevObstacle *__restrict__ obstacles,
                                                const float *__restrict__ planes, double *reactions, uint32_t *status) {
     __shared__ int s_abort;
@@ -508,18 +593,14 @@ __global__ void __launch_bounds__(256) k_grid(GridTable g, GridTable clr, SimPar
     if (s_abort) return;
     const size_t gtid = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     const size_t stride = static_cast<size_t>(gridDim.x) * blockDim.x;
-    if (clr.keys) {
-        for (size_t s = gtid; s <= clr.mask; s += stride) {
-            clr.keys[s] = kEmptyKey;
-            clr.vals[s] = kPendingId;
-        }
-        if (gtid == 0) *clr.count = 0;
-    }
     uint32_t nblocks = min(*g.count, g.max_blocks);
     const size_t nodes = static_cast<size_t>(nblocks) * kNodesPerBlock;
     const float h = sp.h;
+    float4 *next_pool = nxt.pool;
     for (size_t node = gtid; node < nodes; node += stride) {
         float4 mp = g.pool[node];
+        // the other pool receives the next P2G: zero every allocated block of it
+        if (next_pool) next_pool[node] = make_float4(0.f, 0.f, 0.f, 0.f);
         if (mp.x <= 0.0f) {
             g.pool[node] = make_float4(0.f, 0.f, 0.f, 0.f);
             continue;
@@ -640,26 +721,26 @@ int device_sm_count() {
 
 void launch_transfer(int mode, const ParticleSoA &P, int n, const DevClass *classes, const GridTable &cur,
                      const GridTable &next, const SimParams &sp, const DevObstacle *obstacles, const float *planes,
-                     double *reactions, uint32_t *status, cudaStream_t stream) {
+                     double *reactions, uint32_t *status, int *cache, cudaStream_t stream) {
     if (n <= 0) return;
     dim3 grid((n + kThreads - 1) / kThreads);
     switch (mode) {
     case kModeP2G:
-        k_transfer<kModeP2G><<<grid, kThreads, 0, stream>>>(P, n, classes, cur, next, sp, obstacles, planes, reactions, status);
+        k_transfer<kModeP2G><<<grid, kThreads, 0, stream>>>(P, n, classes, cur, next, sp, obstacles, planes, reactions, status, cache);
         break;
     case kModeG2P2G:
-        k_transfer<kModeG2P2G><<<grid, kThreads, 0, stream>>>(P, n, classes, cur, next, sp, obstacles, planes, reactions, status);
+        k_transfer<kModeG2P2G><<<grid, kThreads, 0, stream>>>(P, n, classes, cur, next, sp, obstacles, planes, reactions, status, cache);
         break;
     default:
-        k_transfer<kModeG2P><<<grid, kThreads, 0, stream>>>(P, n, classes, cur, next, sp, obstacles, planes, reactions, status);
+        k_transfer<kModeG2P><<<grid, kThreads, 0, stream>>>(P, n, classes, cur, next, sp, obstacles, planes, reactions, status, cache);
         break;
     }
 }
 
-void launch_grid_update(const GridTable &g, const GridTable &clear, const SimParams &sp, const DevObstacle *obstacles,
+void launch_grid_update(const GridTable &g, const GridTable &next, const SimParams &sp, const DevObstacle *obstacles,
                         const float *planes, double *reactions, uint32_t *status, cudaStream_t stream) {
     int blocks = device_sm_count() * 8;
-    k_grid<<<blocks, 256, 0, stream>>>(g, clear, sp, obstacles, planes, reactions, status);
+    k_grid<<<blocks, 256, 0, stream>>>(g, next, sp, obstacles, planes, reactions, status);
 }
 
 void launch_clear_table(const GridTable &g, cudaStream_t stream) {

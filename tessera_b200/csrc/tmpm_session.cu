@@ -513,6 +513,7 @@ struct TmpmSession {
     DevBuf<float> dev_planes;
     DevBuf<uint32_t> status;
     DevBuf<double> reactions;
+    DevBuf<int> cta_cache;  // kCacheStride ints per transfer CTA
     DevBuf<uint32_t> sort_keys[2], sort_vals[2], sort_hist, sort_totals;
     PinnedBuf staging;
     bool force_dirty = false;
@@ -750,6 +751,9 @@ struct TmpmSession {
         for (int b = 0; b < 2; ++b)
             if (pbuf[b].cap != cap)
                 if ((e = pbuf[b].alloc(cap))) return cuda_fail(e, "cudaMalloc particles");
+        size_t ctas = (cap + kTransferThreads - 1) / kTransferThreads;
+        if (cta_cache.count < ctas * kCacheStride)
+            if ((e = cta_cache.alloc(ctas * kCacheStride))) return cuda_fail(e, "cudaMalloc cache");
         if (force.count < 3 * std::max<size_t>(world.n, 1))
             if ((e = force.alloc(3 * std::max<size_t>(world.n, 1)))) return cuda_fail(e, "cudaMalloc forces");
         for (int g = 0; g < 2; ++g)
@@ -809,6 +813,14 @@ struct TmpmSession {
 
     ParticleSoA soa() const { return pbuf[cur].view(force.ptr, std::max<size_t>(world.n, 1)); }
 
+    // Grid views for one batch: both share grids[0]'s hash table and block
+    // metadata (ids stay stable for the whole batch); they differ in the pool.
+    void grid_views(GridTable g[2]) const {
+        g[0] = grids[0].view();
+        g[1] = g[0];
+        g[1].pool = grids[1].pool.ptr;
+    }
+
     // Queue `steps` resident substeps on the stream (encode_prepared, gpu.rs:1729-1777).
     TmpmStatus enqueue(uint32_t steps, double dt, bool resident, bool with_reactions, std::vector<float> *kernel_ms) {
         if (n_dev == 0) return TMPM_OK;
@@ -851,12 +863,13 @@ struct TmpmSession {
             since_resort = 0;
             tock(4);
         }
-        GridTable g[2] = {grids[0].view(), grids[1].view()};
+        GridTable g[2];
+        grid_views(g);
         ParticleSoA P = soa();
         tick(0);
         launch_clear_table(g[0], stream);
         launch_transfer(kModeP2G, P, n_dev, classes.ptr, g[1], g[0], sp, dev_obstacles.ptr, dev_planes.ptr,
-                        reactions.ptr, status.ptr, stream);
+                        reactions.ptr, status.ptr, cta_cache.ptr, stream);
         tock(0);
         for (uint32_t s = 0; s < steps; ++s) {
             const GridTable &gc = g[s & 1], &gn = g[(s + 1) & 1];
@@ -868,7 +881,7 @@ struct TmpmSession {
             bool last = s + 1 == steps;
             tick(0);
             launch_transfer(last ? kModeG2P : kModeG2P2G, P, n_dev, classes.ptr, gc, gn, spk, dev_obstacles.ptr,
-                            dev_planes.ptr, reactions.ptr, status.ptr, stream);
+                            dev_planes.ptr, reactions.ptr, status.ptr, cta_cache.ptr, stream);
             tock(last ? 3 : 2);
             if (s == 0 && force_dirty) {
                 cudaMemsetAsync(force.ptr, 0, sizeof(float) * force.count, stream);
@@ -1372,11 +1385,13 @@ TmpmStatus tmpm_debug_p2g(TmpmSession *s, int32_t *cells_out, float *mm_out, siz
     if (s->n_dev == 0) return TMPM_OK;
     cudaSetDevice(s->device);
     SimParams sp = s->sim_params(s->substep_dt, true);
-    GridTable g0 = s->grids[0].view(), g1 = s->grids[1].view();
+    GridTable gv[2];
+    s->grid_views(gv);
+    GridTable g0 = gv[0], g1 = gv[1];
     cudaMemsetAsync(s->status.ptr, 0, sizeof(uint32_t), s->stream);
     launch_clear_table(g0, s->stream);
     launch_transfer(kModeP2G, s->soa(), s->n_dev, s->classes.ptr, g1, g0, sp, s->dev_obstacles.ptr, s->dev_planes.ptr,
-                    s->reactions.ptr, s->status.ptr, s->stream);
+                    s->reactions.ptr, s->status.ptr, s->cta_cache.ptr, s->stream);
     DevBuf<int32_t> cells;
     DevBuf<float4> vals;
     DevBuf<uint32_t> cnt;
