@@ -234,6 +234,30 @@ TmpmStatus tmpm_step_cfl(TmpmSession *session, double dt);
 TmpmStatus tmpm_step_cfl_with_reactions(TmpmSession *session, double dt,
                                         double *reactions_out, size_t obstacle_count);
 
+/* ---------------------- allocation-free binning step ---------------------- */
+
+/* No counterpart in the reference.  For callers that must not allocate device
+ * memory during a call: a loop with a frame-time budget (an allocation can
+ * synchronize the device), a host application that owns every device buffer
+ * through its own pool, or code that records work into a CUDA graph.  It runs
+ * the binning step of the substep on `count` f32 positions stored
+ * component-major on the device (x[0..count), then y and z, `stride` floats
+ * apart) and writes, to caller-owned device buffers, the stable order of the
+ * particles by the Morton key of their 4^3 grid block (order_out) and, when
+ * keys_out is not NULL, the sorted keys.  `stream` is a cudaStream_t (NULL =
+ * the default stream); the call is asynchronous on it.
+ * It allocates nothing: its scratch is a fixed array inside the library
+ * (about 4.1 MB, held on every device that loads the library until exit), so
+ * `count` is limited to 262,144; larger counts return TMPM_ERR_CAPACITY with
+ * the reason in tmpm_last_error().  The first call on a device looks up the
+ * scratch address once (set-up), so make that first call before any stream
+ * capture.  All calls share the scratch: calls that overlap on the GPU
+ * (different streams, or different host threads) race and must be ordered by
+ * the caller. */
+TmpmStatus tmpm_sort_by_block_noalloc(const float *positions, size_t count, size_t stride,
+                                      double cell_width, uint32_t *order_out, uint32_t *keys_out,
+                                      void *stream);
+
 /* ------------------------------ diagnostics ------------------------------ */
 
 /* Human-readable reason for the last failed call on this session. */

@@ -86,6 +86,8 @@ def lib():
     L.tmpm_debug_p2g.restype = S
     L.tmpm_bench_substeps.argtypes = [P, C.c_uint32, C.POINTER(C.c_double), P, C.c_size_t]
     L.tmpm_bench_substeps.restype = S
+    L.tmpm_sort_by_block_noalloc.argtypes = [P, C.c_size_t, C.c_size_t, C.c_double, P, P, P]
+    L.tmpm_sort_by_block_noalloc.restype = S
     _lib = L
     return L
 

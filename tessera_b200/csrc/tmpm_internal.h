@@ -13,6 +13,7 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <string>
 
 #include <cuda_runtime.h>
 
@@ -126,10 +127,16 @@ void launch_resort(ParticleSoA &src, ParticleSoA &dst, int n, const SimParams &s
                    cudaStream_t stream);
 void launch_bin_keys(const ParticleSoA &P, int n, const SimParams &sp, int32_t *cells, uint32_t *keys,
                      cudaStream_t stream);
+// Morton block keys (and identity values) of `n` positions stored component-major with `stride`.
+void launch_bin_keys_values(const float *x, size_t stride, int n, float inv_h, uint32_t *keys, uint32_t *vals,
+                            cudaStream_t stream);
 void launch_dump_grid(const GridTable &g, int32_t *cells, float4 *values, uint32_t *count, uint32_t capacity,
                       cudaStream_t stream);
 void launch_snapshot(const ParticleSoA &P, int n, const DevClass *classes, float4 *out, cudaStream_t stream);
 int device_sm_count();
+
+// Thread-local reason reported by tmpm_last_error() (tmpm_session.cu).
+void set_last_error(const std::string &msg);
 
 // Radix sort (tmpm_sort.cu): stable sort of (key, value) pairs by `bits` low key bits.
 // Result ends in sb.keys[0] / sb.vals[0].

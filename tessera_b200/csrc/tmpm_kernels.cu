@@ -754,6 +754,12 @@ void launch_bin_keys(const ParticleSoA &P, int n, const SimParams &sp, int32_t *
     k_bin_keys<<<(n + 255) / 256, 256, 0, stream>>>(P.x, P.cap, n, sp.inv_h, cells, keys, nullptr);
 }
 
+void launch_bin_keys_values(const float *x, size_t stride, int n, float inv_h, uint32_t *keys, uint32_t *vals,
+                            cudaStream_t stream) {
+    if (n <= 0) return;
+    k_bin_keys<<<(n + 255) / 256, 256, 0, stream>>>(x, stride, n, inv_h, nullptr, keys, vals);
+}
+
 void launch_resort(ParticleSoA &src, ParticleSoA &dst, int n, const SimParams &sp, SortBuffers &sb,
                    cudaStream_t stream) {
     if (n <= 0) return;

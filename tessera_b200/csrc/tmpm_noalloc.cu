@@ -1,0 +1,97 @@
+// tmpm_noalloc.cu -- block-order binning for callers that must not allocate.
+//
+// Some callers cannot let a library call cudaMalloc: a render or physics loop
+// that runs under a frame-time budget (an allocation can synchronize the
+// device and stall the frame), a host application that hands out all device
+// memory through its own pool, or code that records work into a CUDA graph.
+// tmpm_sort_by_block_noalloc gives them the binning step of the substep (the
+// f32 base cell of each particle, the Morton key of its 4^3 grid block and
+// the stable sort order by that key) using only the buffers they pass in plus
+// a fixed scratch area that is part of the library image itself.
+
+#include <cmath>
+#include <cstdio>
+#include <mutex>
+#include <string>
+
+#include "../../include/tmpm.h"
+#include "tmpm_internal.h"
+
+namespace {
+
+constexpr size_t kNoAllocMaxParticles = size_t(1) << 18;  // 262,144 particles per call
+constexpr size_t kNoAllocTiles = (kNoAllocMaxParticles + 4095) / 4096;
+// keys[2][max] | vals[2][max] | hist[256][tiles] | totals[256]  (about 4.1 MB)
+constexpr size_t kNoAllocWords = 4 * kNoAllocMaxParticles + 256 * kNoAllocTiles + 256;
+
+// Device-resident scratch shared by every call on a device.  Host code must
+// never hand this symbol itself to a kernel: on the host it is only a
+// stand-in, and its device address comes from cudaGetSymbolAddress below.
+static __device__ __align__(256) uint32_t g_noalloc_scratch[kNoAllocWords];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_setup_mutex;
+uint32_t *g_scratch_ptr[kMaxDevices] = {};
+
+TmpmStatus noalloc_fail(TmpmStatus st, const std::string &msg) {
+    tmpm::set_last_error(msg);  // readable through tmpm_last_error()
+    return st;
+}
+
+}  // namespace
+
+extern "C" TmpmStatus tmpm_sort_by_block_noalloc(const float *positions, size_t count, size_t stride,
+                                                 double cell_width, uint32_t *order_out, uint32_t *keys_out,
+                                                 void *stream) {
+    if (count > kNoAllocMaxParticles)
+        return noalloc_fail(TMPM_ERR_CAPACITY, "tmpm_sort_by_block_noalloc: count " + std::to_string(count) +
+                                                   " exceeds the fixed scratch limit of " +
+                                                   std::to_string(kNoAllocMaxParticles) + " particles");
+    if (count == 0) return TMPM_OK;
+    if (!positions || !order_out || stride < count)
+        return noalloc_fail(TMPM_ERR_INVALID_INPUT, "tmpm_sort_by_block_noalloc: null buffer or stride < count");
+    const float h32 = static_cast<float>(cell_width);
+    if (!std::isfinite(cell_width) || !std::isfinite(h32) || h32 <= 0.0f || !std::isfinite(1.0f / h32))
+        return noalloc_fail(TMPM_ERR_INVALID_INPUT, "tmpm_sort_by_block_noalloc: cell width not a positive f32");
+
+    // Set-up, once per device, with that device current: the scratch symbol's
+    // device address.  Doing this on the first call means the first call on a
+    // device should not happen inside a stream capture.
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return noalloc_fail(TMPM_ERR_DEVICE, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
+    if (dev < 0 || dev >= kMaxDevices) return noalloc_fail(TMPM_ERR_DEVICE, "device ordinal out of range");
+    uint32_t *base = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(g_setup_mutex);
+        if (!g_scratch_ptr[dev]) {
+            void *p = nullptr;
+            e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+            if (e != cudaSuccess || !p)
+                return noalloc_fail(TMPM_ERR_DEVICE,
+                                    std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(e));
+            g_scratch_ptr[dev] = static_cast<uint32_t *>(p);
+        }
+        base = g_scratch_ptr[dev];
+    }
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    tmpm::SortBuffers sb{};
+    sb.keys[0] = base;
+    sb.keys[1] = base + kNoAllocMaxParticles;
+    sb.vals[0] = base + 2 * kNoAllocMaxParticles;
+    sb.vals[1] = base + 3 * kNoAllocMaxParticles;
+    sb.hist = base + 4 * kNoAllocMaxParticles;
+    sb.totals = sb.hist + 256 * kNoAllocTiles;
+    sb.cap = kNoAllocMaxParticles;
+    // Every scratch word this call reads is written earlier in the same call
+    // (keys and values by the binning kernel, histograms and totals by each
+    // radix pass), so nothing has to start at zero.
+    const int n = static_cast<int>(count);
+    tmpm::launch_bin_keys_values(positions, stride, n, 1.0f / h32, sb.keys[0], sb.vals[0], s);
+    tmpm::radix_sort_pairs(sb, n, 30, s);
+    cudaMemcpyAsync(order_out, sb.vals[0], sizeof(uint32_t) * count, cudaMemcpyDeviceToDevice, s);
+    if (keys_out) cudaMemcpyAsync(keys_out, sb.keys[0], sizeof(uint32_t) * count, cudaMemcpyDeviceToDevice, s);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return noalloc_fail(TMPM_ERR_DEVICE, std::string("launch: ") + cudaGetErrorString(e));
+    return TMPM_OK;
+}

@@ -484,6 +484,8 @@ int class_kind(int material) {
 
 }  // namespace
 
+void tmpm::set_last_error(const std::string &msg) { g_last_error = msg; }
+
 struct TmpmSession {
     // host world (last synchronized state)
     TmpmParams params{};
