@@ -252,13 +252,16 @@ def run_tessera(args, world, rank, local):
     host = sc.particles
     e2e = None
     if args.e2e_steps > 0:
+        from tessera_b200._abi import ParticleArrays
+
         e2e_times = []
+        out = ParticleArrays(n)  # caller-owned host arrays, reused across steps
         for it in range(1 + args.e2e_steps):
             torch.cuda.synchronize()
             t0 = time.perf_counter()
             session.write_particles(host)
             session.step(BATCH)
-            out = session.particles()
+            session.particles(out)
             t1 = time.perf_counter()
             if it > 0:
                 e2e_times.append(t1 - t0)

@@ -31,6 +31,31 @@ thread_local std::string g_last_error;
 
 constexpr double kSyncTimeoutSeconds = 5.0;  // gpu.rs:1853-1862
 
+unsigned host_threads() { return std::max(1u, std::min(32u, std::thread::hardware_concurrency())); }
+
+// Run fn(chunk, begin, end) over [0, n) split into contiguous chunks, one per host thread.
+template <typename Fn>
+void parallel_chunks(size_t n, Fn fn, size_t min_per_chunk = 32768) {
+    size_t chunks = std::min<size_t>(host_threads(), std::max<size_t>(1, n / min_per_chunk));
+    if (chunks <= 1) {
+        fn(size_t(0), size_t(0), n);
+        return;
+    }
+    size_t per = (n + chunks - 1) / chunks;
+    std::vector<std::thread> pool;
+    for (size_t c = 0; c < chunks; ++c) {
+        size_t a = c * per, b = std::min(n, a + per);
+        if (a >= b) break;
+        pool.emplace_back([=]() { fn(c, a, b); });
+    }
+    for (auto &t : pool) t.join();
+}
+
+template <typename Fn>
+void parallel_for(size_t n, Fn fn) {
+    parallel_chunks(n, [&](size_t, size_t a, size_t b) { fn(a, b); });
+}
+
 // --------------------------------------------------------------- host world
 
 struct HostWorld {
@@ -42,30 +67,36 @@ struct HostWorld {
     std::vector<uint32_t> group;
     std::vector<uint64_t> chunk;
 
+    // Sizes every field for `count` particles; existing storage is reused and
+    // not cleared (load() writes every element).
     void resize(size_t count) {
         n = count;
-        pos.assign(3 * n, 0.0);
-        vel.assign(3 * n, 0.0);
-        F.assign(9 * n, 0.0);
-        C.assign(9 * n, 0.0);
-        force.assign(3 * n, 0.0);
-        mass.assign(n, 0.0);
-        vol.assign(n, 0.0);
-        radius.assign(n, 0.0);
-        damping.assign(n, 0.0);
-        plastic.assign(3 * n, 0.0);
-        mparams.assign(5 * n, 0.0);
-        material.assign(n, 0);
-        enabled.assign(n, 1);
-        fixed.assign(n, 0);
-        color.assign(n, 0);
-        group.assign(n, 0);
-        chunk.assign(n, 0);
+        pos.resize(3 * n);
+        vel.resize(3 * n);
+        F.resize(9 * n);
+        C.resize(9 * n);
+        force.resize(3 * n);
+        mass.resize(n);
+        vol.resize(n);
+        radius.resize(n);
+        damping.resize(n);
+        plastic.resize(3 * n);
+        mparams.resize(5 * n);
+        material.resize(n);
+        enabled.resize(n);
+        fixed.resize(n);
+        color.resize(n);
+        group.resize(n);
+        chunk.resize(n);
     }
 
     void load(const TmpmParticleArrays &a) {
         resize(a.count);
-        for (size_t i = 0; i < n; ++i) {
+        parallel_for(n, [&](size_t lo, size_t hi) { load_range(a, lo, hi); });
+    }
+
+    void load_range(const TmpmParticleArrays &a, size_t lo, size_t hi) {
+        for (size_t i = lo; i < hi; ++i) {
             for (int k = 0; k < 3; ++k) {
                 pos[3 * i + k] = a.position[3 * i + k];
                 vel[3 * i + k] = a.velocity[3 * i + k];
@@ -97,7 +128,11 @@ struct HostWorld {
     }
 
     void store(TmpmParticleArrays &a) const {
-        for (size_t i = 0; i < n; ++i) {
+        parallel_for(n, [&](size_t lo, size_t hi) { store_range(a, lo, hi); });
+    }
+
+    void store_range(TmpmParticleArrays &a, size_t lo, size_t hi) const {
+        for (size_t i = lo; i < hi; ++i) {
             for (int k = 0; k < 3; ++k) {
                 if (a.position) a.position[3 * i + k] = pos[3 * i + k];
                 if (a.velocity) a.velocity[3 * i + k] = vel[3 * i + k];
@@ -301,12 +336,18 @@ bool params_valid(const TmpmParams &p) {  // world.rs:51-65
 }
 
 double stable_timestep(const HostWorld &w, const TmpmParams &p) {  // world.rs:288-303
+    std::vector<double> part(host_threads() + 1, p.max_substep);
+    parallel_chunks(w.n, [&](size_t c, size_t lo, size_t hi) {
+        double dt = p.max_substep;
+        for (size_t i = lo; i < hi; ++i) {
+            if (!w.enabled[i] || w.fixed[i]) continue;
+            dt = std::min(dt, timestep_bound(w.material[i], &w.mparams[5 * i], w.mass[i] / w.vol[i], &w.vel[3 * i],
+                                             p.cell_width, det9(&w.F[9 * i])));
+        }
+        part[c] = dt;
+    });
     double dt = p.max_substep;
-    for (size_t i = 0; i < w.n; ++i) {
-        if (!w.enabled[i] || w.fixed[i]) continue;
-        dt = std::min(dt, timestep_bound(w.material[i], &w.mparams[5 * i], w.mass[i] / w.vol[i], &w.vel[3 * i],
-                                         p.cell_width, det9(&w.F[9 * i])));
-    }
+    for (double d : part) dt = std::min(dt, d);
     return std::min(dt, p.max_substep);
 }
 
@@ -490,6 +531,7 @@ struct TmpmSession {
     // host world (last synchronized state)
     TmpmParams params{};
     HostWorld world;
+    HostWorld spare;  // reused storage for tmpm_write_particles
     std::vector<TmpmObstacle> obstacles;
     std::vector<std::vector<double>> obstacle_planes;
     bool use_cpic = true;
@@ -517,7 +559,8 @@ struct TmpmSession {
     DevBuf<double> reactions;
     DevBuf<int> cta_cache;  // kCacheStride ints per transfer CTA
     DevBuf<uint32_t> sort_keys[2], sort_vals[2], sort_hist, sort_totals;
-    PinnedBuf staging;
+    PinnedBuf staging;         // readback
+    PinnedBuf upload_staging;  // packed f32 state for uploads
     bool force_dirty = false;
     uint64_t since_resort = 0;
 
@@ -587,120 +630,192 @@ struct TmpmSession {
         float inv_h = 1.0f / h32;
         if (!std::isfinite(inv_h)) return fail(TMPM_ERR_INVALID_INPUT, "1 / cell width not representable in f32");
 
-        // classes and per-particle packing, component-major with stride `cap`
+        // Packing runs in two parallel passes over contiguous particle chunks:
+        // pass 1 validates, builds per-chunk class tables and block lists and
+        // counts enabled particles; pass 2 writes the f32 arrays (component-
+        // major with stride `cap`) straight into pinned memory at compacted
+        // positions.  Results equal a serial pass in world order.
+        const size_t N = world.n;
+        struct ChunkOut {
+            size_t first_bad = std::numeric_limits<size_t>::max();
+            TmpmStatus st = TMPM_OK;
+            const char *msg = "";
+            size_t enabled = 0;
+            std::vector<DevClass> classes;
+            std::vector<unsigned long long> blocks;
+        };
+        const unsigned T = host_threads();
+        std::vector<ChunkOut> co(T + 1);
+        std::vector<uint32_t> lcls(std::max<size_t>(N, 1));
+        parallel_chunks(N, [&](size_t c, size_t lo, size_t hi) {
+            ChunkOut &o = co[c];
+            std::unordered_map<std::string, uint32_t> index;
+            DevClass last{};
+            uint32_t last_ci = kClassMask;
+            unsigned long long last_block = ~0ull;
+            auto bad = [&](size_t i, TmpmStatus st, const char *msg) {
+                o.first_bad = i;
+                o.st = st;
+                o.msg = msg;
+            };
+            for (size_t i = lo; i < hi; ++i) {
+                float f4[4];
+                for (int k = 0; k < 3; ++k)
+                    if (!f32_ok(world.pos[3 * i + k], f4[k]) || !f32_ok(world.vel[3 * i + k], f4[3]) ||
+                        !f32_ok(world.force[3 * i + k], f4[3]))
+                        return bad(i, TMPM_ERR_INVALID_INPUT, "particle state not representable in f32");
+                float m32, v32, r32, d32;
+                if (!f32_ok(world.enabled[i] ? world.mass[i] : 0.0, m32) || !f32_ok(world.vol[i], v32) ||
+                    !f32_ok(world.radius[i], r32) || !f32_ok(world.damping[i], d32))
+                    return bad(i, TMPM_ERR_INVALID_INPUT, "particle scalars not representable in f32");
+                if (world.enabled[i] && (m32 <= 0.0f || v32 <= 0.0f))
+                    return bad(i, TMPM_ERR_INVALID_INPUT, "particle mass or volume underflows f32");
+                if (r32 <= 0.0f || world.damping[i] < 0.0)
+                    return bad(i, TMPM_ERR_INVALID_INPUT, "particle radius or damping invalid");
+                for (int k = 0; k < 9; ++k) {
+                    float t;
+                    if (!f32_ok(world.F[9 * i + k], t) || !f32_ok(world.C[9 * i + k], t))
+                        return bad(i, TMPM_ERR_INVALID_INPUT, "particle matrices not representable in f32");
+                }
+                if (!world.enabled[i]) continue;
+                int base[3];
+                for (int k = 0; k < 3; ++k) {
+                    float xk = static_cast<float>(world.pos[3 * i + k]);
+                    float cf = std::floor(xk * inv_h - 0.5f);
+                    if (!std::isfinite(cf) || cf < -131000.0f || cf > 131000.0f)
+                        return bad(i, TMPM_ERR_INVALID_INPUT, "particle cell outside the representable grid");
+                    base[k] = static_cast<int>(cf);
+                }
+                int kind = class_kind(world.material[i]);
+                const double *mp = &world.mparams[5 * i];
+                if (kind == kMatCorotated) {
+                    // use_cpu_corotated (gpu.rs:1156-1170): ill-conditioned F is a CPU case
+                    const double *Fm = &world.F[9 * i];
+                    double nrm = fro9(Fm), inrm = std::numeric_limits<double>::infinity();
+                    inverse_norm9(Fm, inrm);
+                    if (std::fabs(det9(Fm)) < 1e-5 || !(nrm >= 1e-5 && nrm <= 20.0) || nrm * inrm > 100.0) kind = 0;
+                }
+                if (kind == 0)
+                    return bad(i, TMPM_ERR_RESIDENT_UNAVAILABLE,
+                               "particle material or deformation needs the CPU path (plastic material or "
+                               "ill-conditioned F)");
+                DevClass k{};
+                k.mass = m32;
+                k.volume = v32;
+                k.radius = r32;
+                k.damping = d32;
+                k.kind = kind;
+                k.color = world.color[i];
+                float rho = std::max(m32 / v32, 1e-12f);
+                if (kind == kMatFluid) {
+                    float b, g, vi, te;
+                    if (!f32_ok(mp[0], b) || !f32_ok(mp[1], g) || !f32_ok(mp[2], vi) || !f32_ok(mp[3], te))
+                        return bad(i, TMPM_ERR_INVALID_INPUT, "fluid parameters not representable in f32");
+                    k.p0 = b;
+                    k.p1 = g;
+                    k.p2 = vi;
+                    k.p3 = te;
+                    k.wave = std::sqrt(b * g / rho);
+                } else {
+                    double lambda, mu;
+                    lame(mp[0], mp[1], lambda, mu);
+                    float l32, m32b;
+                    if (!f32_ok(lambda, l32) || !f32_ok(mu, m32b))
+                        return bad(i, TMPM_ERR_INVALID_INPUT, "Lame parameters not representable in f32");
+                    k.p0 = l32;
+                    k.p1 = m32b;
+                    k.wave = std::sqrt((l32 + 2.0f * m32b) / rho);
+                }
+                uint32_t ci;
+                if (last_ci != kClassMask && std::memcmp(&k, &last, sizeof(DevClass)) == 0) {
+                    ci = last_ci;
+                } else {
+                    std::string key(reinterpret_cast<const char *>(&k), sizeof(DevClass));
+                    auto it = index.find(key);
+                    if (it == index.end()) {
+                        ci = static_cast<uint32_t>(o.classes.size());
+                        o.classes.push_back(k);
+                        index.emplace(std::move(key), ci);
+                    } else {
+                        ci = it->second;
+                    }
+                    last = k;
+                    last_ci = ci;
+                }
+                lcls[i] = ci;
+                unsigned long long hb =
+                    (static_cast<unsigned long long>(world.color[i]) << 48) |
+                    (static_cast<unsigned long long>(static_cast<uint32_t>((base[0] >> 2) + kBlockBias) & 0xFFFF) << 32) |
+                    (static_cast<unsigned long long>(static_cast<uint32_t>((base[1] >> 2) + kBlockBias) & 0xFFFF) << 16) |
+                    static_cast<unsigned long long>(static_cast<uint32_t>((base[2] >> 2) + kBlockBias) & 0xFFFF);
+                if (hb != last_block) {
+                    o.blocks.push_back(hb);
+                    last_block = hb;
+                }
+                ++o.enabled;
+            }
+            std::sort(o.blocks.begin(), o.blocks.end());
+            o.blocks.erase(std::unique(o.blocks.begin(), o.blocks.end()), o.blocks.end());
+        });
+        size_t worst = std::numeric_limits<size_t>::max();
+        const ChunkOut *failed = nullptr;
+        for (const ChunkOut &o : co)
+            if (o.first_bad < worst) {
+                worst = o.first_bad;
+                failed = &o;
+            }
+        if (failed) return fail(failed->st, failed->msg);
+        // merge class tables and block lists (small), compute compacted offsets
         std::vector<DevClass> cls_table;
         std::unordered_map<std::string, uint32_t> cls_index;
+        std::vector<std::vector<uint32_t>> remap(co.size());
+        std::vector<size_t> offset(co.size(), 0);
+        std::vector<unsigned long long> home_blocks;
         size_t n_enabled = 0;
-        for (size_t i = 0; i < world.n; ++i) n_enabled += world.enabled[i] ? 1 : 0;
+        for (size_t c = 0; c < co.size(); ++c) {
+            offset[c] = n_enabled;
+            n_enabled += co[c].enabled;
+            for (const DevClass &k : co[c].classes) {
+                std::string key(reinterpret_cast<const char *>(&k), sizeof(DevClass));
+                auto it = cls_index.find(key);
+                uint32_t gi;
+                if (it == cls_index.end()) {
+                    gi = static_cast<uint32_t>(cls_table.size());
+                    cls_table.push_back(k);
+                    cls_index.emplace(std::move(key), gi);
+                } else {
+                    gi = it->second;
+                }
+                remap[c].push_back(gi);
+            }
+            home_blocks.insert(home_blocks.end(), co[c].blocks.begin(), co[c].blocks.end());
+        }
         if (n_enabled > static_cast<size_t>(std::numeric_limits<int>::max() / 2))
             return fail(TMPM_ERR_CAPACITY, "too many particles for one session");
         const size_t cap = std::max<size_t>(256, (n_enabled + 255) / 256 * 256);
-        std::vector<float> hx(3 * cap, 0.f), hv(3 * cap, 0.f), hC(9 * cap, 0.f), hF(9 * cap, 0.f);
-        std::vector<uint32_t> hcls(cap, 0u), hwidx(cap, 0u);
-        std::vector<unsigned long long> home_blocks;
-        home_blocks.reserve(n_enabled);
-        DevClass last_class{};
-        uint32_t last_ci = kClassMask;
-        size_t j = 0;
-        for (size_t i = 0; i < world.n; ++i) {
-            float f4[4];
-            for (int k = 0; k < 3; ++k)
-                if (!f32_ok(world.pos[3 * i + k], f4[k]) || !f32_ok(world.vel[3 * i + k], f4[3]) ||
-                    !f32_ok(world.force[3 * i + k], f4[3]))
-                    return fail(TMPM_ERR_INVALID_INPUT, "particle state not representable in f32");
-            float m32, v32, r32, d32;
-            if (!f32_ok(world.enabled[i] ? world.mass[i] : 0.0, m32) || !f32_ok(world.vol[i], v32) ||
-                !f32_ok(world.radius[i], r32) || !f32_ok(world.damping[i], d32))
-                return fail(TMPM_ERR_INVALID_INPUT, "particle scalars not representable in f32");
-            if (world.enabled[i] && (m32 <= 0.0f || v32 <= 0.0f))
-                return fail(TMPM_ERR_INVALID_INPUT, "particle mass or volume underflows f32");
-            if (r32 <= 0.0f || world.damping[i] < 0.0)
-                return fail(TMPM_ERR_INVALID_INPUT, "particle radius or damping invalid");
-            for (int k = 0; k < 9; ++k) {
-                float t;
-                if (!f32_ok(world.F[9 * i + k], t) || !f32_ok(world.C[9 * i + k], t))
-                    return fail(TMPM_ERR_INVALID_INPUT, "particle matrices not representable in f32");
-            }
-            if (!world.enabled[i]) continue;
-            int base[3];
-            for (int k = 0; k < 3; ++k) {
-                float xk = static_cast<float>(world.pos[3 * i + k]);
-                float c = std::floor(xk * inv_h - 0.5f);
-                if (!std::isfinite(c) || c < -131000.0f || c > 131000.0f)
-                    return fail(TMPM_ERR_INVALID_INPUT, "particle cell outside the representable grid");
-                base[k] = static_cast<int>(c);
-            }
-            int kind = class_kind(world.material[i]);
-            const double *mp = &world.mparams[5 * i];
-            if (kind == kMatCorotated) {
-                // use_cpu_corotated (gpu.rs:1156-1170): ill-conditioned F is a CPU case
-                const double *Fm = &world.F[9 * i];
-                double nrm = fro9(Fm), inrm = std::numeric_limits<double>::infinity();
-                inverse_norm9(Fm, inrm);
-                if (std::fabs(det9(Fm)) < 1e-5 || !(nrm >= 1e-5 && nrm <= 20.0) || nrm * inrm > 100.0) kind = 0;
-            }
-            if (kind == 0)
-                return fail(TMPM_ERR_RESIDENT_UNAVAILABLE,
-                            "particle material or deformation needs the CPU path (plastic material or ill-conditioned F)");
-            DevClass k{};
-            k.mass = m32;
-            k.volume = v32;
-            k.radius = r32;
-            k.damping = d32;
-            k.kind = kind;
-            k.color = world.color[i];
-            float rho = std::max(m32 / v32, 1e-12f);
-            if (kind == kMatFluid) {
-                float b, g, vi, te;
-                if (!f32_ok(mp[0], b) || !f32_ok(mp[1], g) || !f32_ok(mp[2], vi) || !f32_ok(mp[3], te))
-                    return fail(TMPM_ERR_INVALID_INPUT, "fluid parameters not representable in f32");
-                k.p0 = b;
-                k.p1 = g;
-                k.p2 = vi;
-                k.p3 = te;
-                k.wave = std::sqrt(b * g / rho);
-            } else {
-                double lambda, mu;
-                lame(mp[0], mp[1], lambda, mu);
-                float l32, m32b;
-                if (!f32_ok(lambda, l32) || !f32_ok(mu, m32b))
-                    return fail(TMPM_ERR_INVALID_INPUT, "Lame parameters not representable in f32");
-                k.p0 = l32;
-                k.p1 = m32b;
-                k.wave = std::sqrt((l32 + 2.0f * m32b) / rho);
-            }
-            uint32_t ci;
-            if (last_ci != kClassMask && std::memcmp(&k, &last_class, sizeof(DevClass)) == 0) {
-                ci = last_ci;
-            } else {
-                std::string key(reinterpret_cast<const char *>(&k), sizeof(DevClass));
-                auto it = cls_index.find(key);
-                if (it == cls_index.end()) {
-                    ci = static_cast<uint32_t>(cls_table.size());
-                    cls_table.push_back(k);
-                    cls_index.emplace(std::move(key), ci);
-                } else {
-                    ci = it->second;
+        if (!upload_staging.ensure((24 * cap + 2 * cap) * sizeof(float)))
+            return fail(TMPM_ERR_DEVICE, "cudaMallocHost upload staging failed");
+        float *hx = static_cast<float *>(upload_staging.ptr);
+        float *hv = hx + 3 * cap, *hC = hv + 3 * cap, *hF = hC + 9 * cap;
+        uint32_t *hcls = reinterpret_cast<uint32_t *>(hF + 9 * cap), *hwidx = hcls + cap;
+        parallel_chunks(N, [&](size_t c, size_t lo, size_t hi) {
+            size_t j = offset[c];
+            const std::vector<uint32_t> &rm = remap[c];
+            for (size_t i = lo; i < hi; ++i) {
+                if (!world.enabled[i]) continue;
+                for (int k3 = 0; k3 < 3; ++k3) {
+                    hx[k3 * cap + j] = static_cast<float>(world.pos[3 * i + k3]);
+                    hv[k3 * cap + j] = static_cast<float>(world.vel[3 * i + k3]);
                 }
-                last_class = k;
-                last_ci = ci;
+                for (int k9 = 0; k9 < 9; ++k9) {
+                    hC[k9 * cap + j] = static_cast<float>(world.C[9 * i + k9]);
+                    hF[k9 * cap + j] = static_cast<float>(world.F[9 * i + k9]);
+                }
+                hcls[j] = rm[lcls[i]] | (world.fixed[i] ? kFixedBit : 0u);
+                hwidx[j] = static_cast<uint32_t>(i);
+                ++j;
             }
-            for (int k3 = 0; k3 < 3; ++k3) {
-                hx[k3 * cap + j] = static_cast<float>(world.pos[3 * i + k3]);
-                hv[k3 * cap + j] = static_cast<float>(world.vel[3 * i + k3]);
-            }
-            for (int k9 = 0; k9 < 9; ++k9) {
-                hC[k9 * cap + j] = static_cast<float>(world.C[9 * i + k9]);
-                hF[k9 * cap + j] = static_cast<float>(world.F[9 * i + k9]);
-            }
-            hcls[j] = ci | (world.fixed[i] ? kFixedBit : 0u);
-            hwidx[j] = static_cast<uint32_t>(i);
-            ++j;
-            home_blocks.push_back((static_cast<unsigned long long>(world.color[i]) << 48) |
-                                  (static_cast<unsigned long long>(static_cast<uint32_t>((base[0] >> 2) + kBlockBias) & 0xFFFF) << 32) |
-                                  (static_cast<unsigned long long>(static_cast<uint32_t>((base[1] >> 2) + kBlockBias) & 0xFFFF) << 16) |
-                                  static_cast<unsigned long long>(static_cast<uint32_t>((base[2] >> 2) + kBlockBias) & 0xFFFF));
-        }
+        });
         // obstacles (pack_obstacle, gpu.rs:2025-2166)
         std::vector<DevObstacle> dobs;
         std::vector<float> dplanes;
@@ -747,7 +862,7 @@ struct TmpmSession {
         if ((e = cudaSetDevice(device))) return cuda_fail(e, "cudaSetDevice");
         // block pool sizing from the number of occupied home blocks
         std::sort(home_blocks.begin(), home_blocks.end());
-        size_t unique_blocks = std::unique(home_blocks.begin(), home_blocks.end()) - home_blocks.begin();
+        size_t unique_blocks = std::unique(home_blocks.begin(), home_blocks.end()) - home_blocks.begin();  // small
         uint64_t want_blocks = options.max_blocks ? options.max_blocks : std::max<uint64_t>(4096, 16 * unique_blocks + 4096);
         if (want_blocks > (1u << 27)) want_blocks = 1u << 27;
         for (int b = 0; b < 2; ++b)
@@ -756,8 +871,11 @@ struct TmpmSession {
         size_t ctas = (cap + kTransferThreads - 1) / kTransferThreads;
         if (cta_cache.count < ctas * kCacheStride)
             if ((e = cta_cache.alloc(ctas * kCacheStride))) return cuda_fail(e, "cudaMalloc cache");
-        if (force.count < 3 * std::max<size_t>(world.n, 1))
+        if (force.count < 3 * std::max<size_t>(world.n, 1)) {
             if ((e = force.alloc(3 * std::max<size_t>(world.n, 1)))) return cuda_fail(e, "cudaMalloc forces");
+            cudaMemsetAsync(force.ptr, 0, sizeof(float) * force.count, stream);
+        }
+        if (force_dirty) cudaMemsetAsync(force.ptr, 0, sizeof(float) * force.count, stream);
         for (int g = 0; g < 2; ++g)
             if (grids[g].max_blocks != want_blocks)
                 if ((e = grids[g].alloc(static_cast<uint32_t>(want_blocks)))) return cuda_fail(e, "cudaMalloc grid");
@@ -779,12 +897,12 @@ struct TmpmSession {
         cur = 0;
         ParticleBuffers &pb = pbuf[0];
         if (n_dev) {
-            cudaMemcpyAsync(pb.x.ptr, hx.data(), sizeof(float) * hx.size(), cudaMemcpyHostToDevice, stream);
-            cudaMemcpyAsync(pb.v.ptr, hv.data(), sizeof(float) * hv.size(), cudaMemcpyHostToDevice, stream);
-            cudaMemcpyAsync(pb.C.ptr, hC.data(), sizeof(float) * hC.size(), cudaMemcpyHostToDevice, stream);
-            cudaMemcpyAsync(pb.F.ptr, hF.data(), sizeof(float) * hF.size(), cudaMemcpyHostToDevice, stream);
-            cudaMemcpyAsync(pb.cls.ptr, hcls.data(), sizeof(uint32_t) * cap, cudaMemcpyHostToDevice, stream);
-            cudaMemcpyAsync(pb.widx.ptr, hwidx.data(), sizeof(uint32_t) * cap, cudaMemcpyHostToDevice, stream);
+            cudaMemcpyAsync(pb.x.ptr, hx, sizeof(float) * 3 * cap, cudaMemcpyHostToDevice, stream);
+            cudaMemcpyAsync(pb.v.ptr, hv, sizeof(float) * 3 * cap, cudaMemcpyHostToDevice, stream);
+            cudaMemcpyAsync(pb.C.ptr, hC, sizeof(float) * 9 * cap, cudaMemcpyHostToDevice, stream);
+            cudaMemcpyAsync(pb.F.ptr, hF, sizeof(float) * 9 * cap, cudaMemcpyHostToDevice, stream);
+            cudaMemcpyAsync(pb.cls.ptr, hcls, sizeof(uint32_t) * cap, cudaMemcpyHostToDevice, stream);
+            cudaMemcpyAsync(pb.widx.ptr, hwidx, sizeof(uint32_t) * cap, cudaMemcpyHostToDevice, stream);
         }
         if (!cls_table.empty())
             cudaMemcpyAsync(classes.ptr, cls_table.data(), sizeof(DevClass) * cls_table.size(), cudaMemcpyHostToDevice, stream);
@@ -800,14 +918,21 @@ struct TmpmSession {
     }
 
     cudaError_t upload_forces() {
-        std::vector<float> f(3 * std::max<size_t>(world.n, 1), 0.0f);
-        bool any = false;
-        for (size_t i = 0; i < world.n; ++i)
-            for (int k = 0; k < 3; ++k) {
-                f[k * world.n + i] = static_cast<float>(world.force[3 * i + k]);
-                any = any || world.force[3 * i + k] != 0.0;
-            }
+        std::atomic<bool> any{false};
+        parallel_for(world.n, [&](size_t lo, size_t hi) {
+            for (size_t i = 3 * lo; i < 3 * hi; ++i)
+                if (world.force[i] != 0.0) {
+                    any = true;
+                    break;
+                }
+        });
         force_dirty = any;
+        if (!force_dirty) return cudaSuccess;  // the device array is zero after every consumption
+        std::vector<float> f(3 * std::max<size_t>(world.n, 1), 0.0f);
+        parallel_for(world.n, [&](size_t lo, size_t hi) {
+            for (size_t i = lo; i < hi; ++i)
+                for (int k = 0; k < 3; ++k) f[k * world.n + i] = static_cast<float>(world.force[3 * i + k]);
+        });
         cudaError_t e = cudaMemcpyAsync(force.ptr, f.data(), sizeof(float) * f.size(), cudaMemcpyHostToDevice, stream);
         if (e) return e;
         return cudaStreamSynchronize(stream);
@@ -995,23 +1120,6 @@ struct TmpmSession {
         return TMPM_OK;
     }
 
-    template <typename Fn>
-    static void parallel_for(size_t n, Fn fn) {
-        unsigned threads = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
-        if (n < 65536 || threads == 1) {
-            fn(0, n);
-            return;
-        }
-        std::vector<std::thread> pool;
-        size_t chunk = (n + threads - 1) / threads;
-        for (unsigned t = 0; t < threads; ++t) {
-            size_t a = t * chunk, b = std::min(n, a + chunk);
-            if (a >= b) break;
-            pool.emplace_back([=]() { fn(a, b); });
-        }
-        for (auto &th : pool) th.join();
-    }
-
     TmpmStatus synchronize() {
         if (!valid) return fail(TMPM_ERR_RESIDENT_UNAVAILABLE, "session is invalid after an earlier error");
         if (pending == 0) return TMPM_OK;
@@ -1049,11 +1157,15 @@ TmpmStatus load_checked(const TmpmParticleArrays *particles, HostWorld &out, std
         return TMPM_ERR_INVALID_INPUT;
     }
     out.load(*particles);
-    for (size_t i = 0; i < out.n; ++i)
-        if (!valid_particle(out, i)) {
-            err = "invalid MPM input";
-            return TMPM_ERR_MPM_INVALID_INPUT;
-        }
+    std::atomic<bool> bad{false};
+    parallel_for(out.n, [&](size_t lo, size_t hi) {
+        for (size_t i = lo; i < hi && !bad.load(std::memory_order_relaxed); ++i)
+            if (!valid_particle(out, i)) bad = true;
+    });
+    if (bad) {
+        err = "invalid MPM input";
+        return TMPM_ERR_MPM_INVALID_INPUT;
+    }
     return TMPM_OK;
 }
 
@@ -1274,19 +1386,20 @@ TmpmStatus tmpm_remove_chunk(TmpmSession *s, uint64_t chunk, size_t *removed_out
 TmpmStatus tmpm_write_particles(TmpmSession *s, const TmpmParticleArrays *particles) {
     TmpmStatus st = session_guard(s, true);
     if (st != TMPM_OK) return st;
-    HostWorld nw;
+    // Load into the session's spare world (its storage is reused across calls)
+    // and swap it in; the previous world comes back on any failure.
+    HostWorld &nw = s->spare;
     std::string err;
     st = load_checked(particles, nw, err);
     if (st != TMPM_OK) return s->fail(st, err);
     if (!particles || !particles->chunk_id) {
         for (size_t i = 0; i < nw.n && i < s->world.n; ++i) nw.chunk[i] = s->world.chunk[i];
     }
-    HostWorld old = std::move(s->world);
-    s->world = std::move(nw);
+    std::swap(s->world, s->spare);
     st = s->validate_resident(s->substep_dt);
     if (st == TMPM_OK) st = s->upload(s->substep_dt);
     if (st != TMPM_OK) {
-        s->world = std::move(old);
+        std::swap(s->world, s->spare);
         if (s->valid) s->upload(s->substep_dt);
         return st;
     }
