@@ -90,12 +90,29 @@ __device__ __forceinline__ bool regular_corotated(const M3f &F) {
     return nrm * inorm <= 100.0f;
 }
 
-// Kirchhoff stress times -dt V0 4/h^2 (material.rs:233-284 for the three GPU
-// materials; the scaling is world.rs:391 / gpu.wgsl:700).
-__device__ __forceinline__ M3f scaled_stress(const DevClass &k, const M3f &F, const M3f &Cm, float neg_dt_inv_d) {
+// Corotated Kirchhoff stress 2 mu (F - R) F^T + lambda (J - 1) J I, scaled by
+// snow's hardening factor (material.rs:272-283, 440-455).  Out of line: its
+// polar iteration would otherwise raise register pressure for every particle.
+__device__ __noinline__ M3f corotated_stress(const DevClass &k, const M3f &F, float J, float plastic_det) {
+    float factor = 1.0f;
+    if (k.kind == kMatSnow) factor = fminf(fmaxf(expf(k.p2 * (1.0f - plastic_det)), 0.01f), 100.0f);
+    float lambda = k.p0 * factor, mu = k.p1 * factor;
+    M3f R = polar_rotation(F);
+    float iso = lambda * (J - 1.0f) * J;
+    M3f s = scale(mul_bt(sub(F, R), F), 2.0f * mu);
+    s.c0.x += iso;
+    s.c1.y += iso;
+    s.c2.z += iso;
+    return s;
+}
+
+// Kirchhoff stress times -dt V0 4/h^2 (material.rs:233-284; the scaling is
+// world.rs:391 / gpu.wgsl:700).  `plastic_det` feeds snow's hardening factor.
+__device__ __forceinline__ M3f scaled_stress(const DevClass &k, const M3f &F, const M3f &Cm, float neg_dt_inv_d,
+                                             float plastic_det) {
     float J = det(F);
     M3f s;
-    if (k.kind == kMatNeoHookean) {
+    if (k.kind == kMatNeoHookean || k.kind == kMatSandNeoHookean) {
         float lambda = k.p0, mu = k.p1;
         float sj = fmaxf(J, 1e-10f);
         float iso = lambda * logf(sj) - mu;
@@ -114,16 +131,136 @@ __device__ __forceinline__ M3f scaled_stress(const DevClass &k, const M3f &F, co
         s.c0.x += diag;
         s.c1.y += diag;
         s.c2.z += diag;
-    } else {  // corotated
-        float lambda = k.p0, mu = k.p1;
-        M3f R = polar_rotation(F);
-        float iso = lambda * (J - 1.0f) * J;
-        s = scale(mul_bt(sub(F, R), F), 2.0f * mu);
-        s.c0.x += iso;
-        s.c1.y += iso;
-        s.c2.z += iso;
+    } else {  // corotated: elastic, sand, snow (with its hardening factor)
+        s = corotated_stress(k, F, J, plastic_det);
     }
     return scale(s, neg_dt_inv_d * k.volume);
+}
+
+// ------------------------------------------------------ plastic return maps
+
+// Eigen-decomposition of the symmetric S = F^T F by cyclic Jacobi rotations
+// (Golub & Van Loan, Matrix Computations, sec. 8.5): S = V diag(w) V^T.
+__device__ inline void sym_eigen3(const M3f &F, V3f &w, M3f &V) {
+    float a00 = dot(F.c0, F.c0), a11 = dot(F.c1, F.c1), a22 = dot(F.c2, F.c2);
+    float a01 = dot(F.c0, F.c1), a02 = dot(F.c0, F.c2), a12 = dot(F.c1, F.c2);
+    V = m3_identity();
+#pragma unroll 1
+    for (int sweep = 0; sweep < 8; ++sweep) {
+        float off = a01 * a01 + a02 * a02 + a12 * a12;
+        if (off <= 1e-24f * (a00 * a00 + a11 * a11 + a22 * a22)) break;
+#pragma unroll
+        for (int pair = 0; pair < 3; ++pair) {
+            // (p, q) = (0, 1), (0, 2), (1, 2)
+            float app = pair == 2 ? a11 : a00;
+            float aqq = pair == 0 ? a11 : a22;
+            float apq = pair == 0 ? a01 : (pair == 1 ? a02 : a12);
+            if (fabsf(apq) < 1e-30f) continue;
+            float theta = (aqq - app) / (2.0f * apq);
+            float t = copysignf(1.0f, theta) / (fabsf(theta) + sqrtf(theta * theta + 1.0f));
+            float c = rsqrtf(t * t + 1.0f), sn = t * c;
+            float napp = app - t * apq, naqq = aqq + t * apq;
+            if (pair == 0) {  // rotate rows/cols 0 and 1; r = 2
+                float a2p = a02, a2q = a12;
+                a02 = c * a2p - sn * a2q;
+                a12 = sn * a2p + c * a2q;
+                a00 = napp;
+                a11 = naqq;
+                a01 = 0.f;
+                V3f vp = V.c0, vq = V.c1;
+                V.c0 = vp * c - vq * sn;
+                V.c1 = vp * sn + vq * c;
+            } else if (pair == 1) {  // 0 and 2; r = 1
+                float a1p = a01, a1q = a12;
+                a01 = c * a1p - sn * a1q;
+                a12 = sn * a1p + c * a1q;
+                a00 = napp;
+                a22 = naqq;
+                a02 = 0.f;
+                V3f vp = V.c0, vq = V.c2;
+                V.c0 = vp * c - vq * sn;
+                V.c2 = vp * sn + vq * c;
+            } else {  // 1 and 2; r = 0
+                float a0p = a01, a0q = a02;
+                a01 = c * a0p - sn * a0q;
+                a02 = sn * a0p + c * a0q;
+                a11 = napp;
+                a22 = naqq;
+                a12 = 0.f;
+                V3f vp = V.c1, vq = V.c2;
+                V.c1 = vp * c - vq * sn;
+                V.c2 = vp * sn + vq * c;
+            }
+        }
+    }
+    w = mk(a00, a11, a22);
+}
+
+// F V diag(target / sigma) V^T = U diag(target) V^T without forming U.
+__device__ __forceinline__ M3f replace_stretches(const M3f &F, const M3f &V, V3f sigma, V3f target) {
+    M3f FV = mul(F, V);
+    FV.c0 = FV.c0 * (target.x / sigma.x);
+    FV.c1 = FV.c1 * (target.y / sigma.y);
+    FV.c2 = FV.c2 * (target.z / sigma.z);
+    return mul_bt(FV, V);
+}
+
+// Return mapping of the plastic materials (material.rs:297-368, 488-532) in
+// f32; `pl` = (plastic_det, hardening, log_volume_gain).  Returns false when
+// F is too ill-conditioned to project on the device (the reference's GPU
+// marks those particles for its CPU path, gpu.wgsl:569-573).
+__device__ __noinline__ bool project_plastic(const DevClass &k, M3f &F, float pl[3]) {
+    if ((k.kind == kMatSand || k.kind == kMatSandNeoHookean) && k.p0 == 0.0f) return true;  // lambda == 0
+    V3f w;
+    M3f V;
+    sym_eigen3(F, w, V);
+    V3f sg = mk(sqrtf(fmaxf(w.x, 0.f)), sqrtf(fmaxf(w.y, 0.f)), sqrtf(fmaxf(w.z, 0.f)));
+    float smin = fminf(fminf(sg.x, sg.y), sg.z), smax = fmaxf(fmaxf(sg.x, sg.y), sg.z);
+    if (!(smin >= 1e-6f) || smax / smin > 100.0f) return false;
+    if (k.kind == kMatSnow) {
+        float lo = 1.0f - k.p3, hi = 1.0f + k.p4;
+        V3f cl = mk(fminf(fmaxf(sg.x, lo), hi), fminf(fmaxf(sg.y, lo), hi), fminf(fmaxf(sg.z, lo), hi));
+        float old_det = sg.x * sg.y * sg.z;
+        float new_det = fmaxf(cl.x * cl.y * cl.z, 1e-12f);
+        pl[0] = fminf(fmaxf(pl[0] * old_det / new_det, 0.1f), 4.0f);
+        F = replace_stretches(F, V, sg, cl);
+        return true;
+    }
+    const float lambda = k.p0, mu = k.p1, friction = k.p2, cohesion = k.p3;
+    const float g3 = pl[2] * (1.0f / 3.0f);
+    V3f strain = mk(logf(fmaxf(sg.x, 1e-12f)) + g3, logf(fmaxf(sg.y, 1e-12f)) + g3, logf(fmaxf(sg.z, 1e-12f)) + g3);
+    float tr = strain.x + strain.y + strain.z;
+    V3f dev = strain - mk(tr, tr, tr) * (1.0f / 3.0f);
+    float nrm = len(dev);
+    float shifted = tr - cohesion;
+    float q = pl[1];
+    float angle = friction + (0.15707963267948966f * q - 0.17453292519943295f) * expf(-0.2f * q);
+    float sine = sinf(angle);
+    float alpha = 0.81649658092772603f * (2.0f * sine) / (3.0f - sine);
+    V3f plog;
+    float inc;
+    if (shifted > 0.0f || nrm <= 4.76837158203125e-7f) {  // apex (4 f32::EPSILON)
+        plog = mk(cohesion, cohesion, cohesion) * (1.0f / 3.0f);
+        inc = len(strain);
+    } else {
+        float gamma = nrm + (3.0f * lambda + 2.0f * mu) / (2.0f * mu) * shifted * alpha;
+        if (gamma <= 0.0f) return true;  // elastic region: unchanged
+        plog = strain - dev * (gamma / nrm);
+        inc = gamma;
+    }
+    V3f pr = mk(expf(plog.x), expf(plog.y), expf(plog.z));
+    float old_det = sg.x * sg.y * sg.z, new_det = pr.x * pr.y * pr.z;
+    if (k.kind == kMatSand) {
+        old_det = fmaxf(old_det, 1e-12f);
+        new_det = fmaxf(new_det, 1e-12f);
+    }
+    float pd = pl[0] * old_det / new_det;
+    if (k.kind == kMatSand) pd = fminf(fmaxf(pd, 0.01f), 100.0f);
+    pl[0] = pd;
+    pl[1] = q + inc;
+    pl[2] = pl[2] + (logf(old_det) - logf(new_det));
+    F = replace_stretches(F, V, sg, pr);
+    return true;
 }
 
 // ---------------------------------------------------------------- obstacles
@@ -161,7 +298,7 @@ __device__ inline V3f closest_point_triangle(V3f p, V3f a, V3f b, V3f c) {
 __device__ __forceinline__ V3f normalize(V3f v) { return v * (1.0f / len(v)); }
 
 // Signed distance and outward world normal (obstacle.rs:372-472).
-__device__ inline float obstacle_surface(const DevObstacle &o, const float *planes, V3f point, V3f &normal) {
+__device__ __noinline__ float obstacle_surface(const DevObstacle &o, const float *planes, V3f point, V3f &normal) {
     V3f rel = point - mk(o.center[0], o.center[1], o.center[2]);
     if (o.shape == 0) {  // sphere
         float n = len(rel);

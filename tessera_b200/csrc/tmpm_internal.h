@@ -39,6 +39,9 @@ constexpr uint32_t kStatusTimeout = 4u;   // a bounded device wait gave up -> Re
 constexpr int kMatNeoHookean = 1;
 constexpr int kMatFluid = 2;
 constexpr int kMatCorotated = 3;
+constexpr int kMatSnow = 4;
+constexpr int kMatSand = 5;
+constexpr int kMatSandNeoHookean = 6;
 
 constexpr int kTransferThreads = 256;  // particles per CTA of the transfer kernels
 constexpr int kCacheStride = 80;       // per-CTA record: 8-int box header + up to 64 block ids
@@ -48,11 +51,14 @@ constexpr uint32_t kClassMask = 0x7FFFFFFFu;
 
 struct DevClass {
     float mass, volume, radius, damping;
-    float p0, p1, p2, p3;  // corotated/NH: lambda, mu; fluid: bulk, gamma, viscosity, tensile
+    // corotated / NH: lambda, mu; fluid: bulk, gamma, viscosity, tensile;
+    // sand / NH sand: lambda, mu, friction angle, cohesion;
+    // snow: lambda, mu, hardening, critical compression, critical stretch (p4)
+    float p0, p1, p2, p3;
     int32_t kind;          // kMat*
     float wave;            // CFL wave speed sqrt((lambda + 2 mu) / rho) or sqrt(K gamma / rho)
     uint32_t color;        // transfer colour (separate grid namespace)
-    float pad;
+    float p4;
 };
 static_assert(sizeof(DevClass) == 48, "DevClass layout");
 
@@ -88,6 +94,7 @@ struct SimParams {
     int reactions;
     int apply_force;
     int resident_checks;  // CFL / escape / conditioning flags (resident path only, gpu.rs:1429)
+    int has_plastic;      // some particle class is snow, sand or NH sand
 };
 
 struct ParticleSoA {
@@ -95,6 +102,7 @@ struct ParticleSoA {
     float *v;       // 3 * cap
     float *C;       // 9 * cap, column-major components (col * 3 + row)
     float *F;       // 9 * cap
+    float *pl;      // 3 * cap: plastic_det, hardening, log_volume_gain (plastic materials only)
     float *force;   // 3 * force_stride, indexed by WORLD index (one-shot forces)
     uint32_t *cls;  // class index | kFixedBit
     uint32_t *widx; // world index of each stored particle

@@ -170,7 +170,9 @@ __device__ __forceinline__ float pow2_scale(float total) {
     return exp2f(e);
 }
 
-template <int MODE>
+// PLASTIC selects the variant that carries plastic state (snow, sand, NH sand);
+// scenes without plastic materials run the leaner variant.
+template <int MODE, bool PLASTIC>
 __global__ void __launch_bounds__(kThreads, TMPM_TRANSFER_MIN_BLOCKS)
     k_transfer(ParticleSoA P, int n, const DevClass *__restrict__ classes, GridTable cur, GridTable next,
                SimParams sp, const DevObstacle *__restrict__ obstacles, const float *__restrict__ planes,
@@ -212,6 +214,13 @@ __global__ void __launch_bounds__(kThreads, TMPM_TRANSFER_MIN_BLOCKS)
         k = classes[cw & kClassMask];
     }
     const bool fixed = (cw & kFixedBit) != 0;
+    const bool plastic = PLASTIC && valid && k.kind >= kMatSnow;
+    float pl[3] = {1.0f, 0.0f, 0.0f};
+    if (plastic) {
+        pl[0] = P.pl[i];
+        pl[1] = P.pl[cap + i];
+        pl[2] = P.pl[2 * cap + i];
+    }
     V3f v = mk(0, 0, 0);
     M3f Cm = m3_zero();
     Box gbox;
@@ -379,9 +388,12 @@ __global__ void __launch_bounds__(kThreads, TMPM_TRANSFER_MIN_BLOCKS)
                 }
             }
             M3f Fn = mul(add(m3_identity(), scale(aff, dt)), F);
+            bool plastic_ok = true;
             if (k.kind == kMatFluid) {
                 float sc = cbrtf(fmaxf(det(Fn), 1e-9f));
                 Fn = scale(m3_identity(), sc);
+            } else if (PLASTIC && k.kind >= kMatSnow) {
+                plastic_ok = project_plastic(k, Fn, pl);
             }
             // Resident failure detection (gpu.wgsl:946-994).
             float ncx = floorf(__fsub_rn(__fmul_rn(pos.x, inv_h), 0.5f));
@@ -397,11 +409,20 @@ __global__ void __launch_bounds__(kThreads, TMPM_TRANSFER_MIN_BLOCKS)
                     failed = failed || nb3[a] < sp.first_base[a] || nb3[a] > sp.last_base[a];
             }
             if (sp.resident_checks) {
-                if (k.kind == kMatCorotated) failed = failed || !regular_corotated(Fn);
-                failed = failed || dt * (k.wave + len(vel)) > 0.4f * h * (1.0f + 1e-4f);
+                if (k.kind == kMatCorotated || k.kind == kMatSnow || k.kind == kMatSand)
+                    failed = failed || !regular_corotated(Fn);
+                if (k.kind == kMatSandNeoHookean) {  // CFL with the elastic volume (gpu.wgsl:983-987)
+                    float wave = k.wave * sqrtf(fmaxf(det(Fn), 1e-6f));
+                    failed = failed || dt * fmaxf(wave, len(vel)) > 0.5f * h * (1.0f + 1e-4f);
+                } else {
+                    failed = failed || dt * (k.wave + len(vel)) > 0.4f * h * (1.0f + 1e-4f);
+                }
+                failed = failed || !plastic_ok;
                 if (failed) atomicOr(status, kStatusResident);
-            } else if (finite3(pos) && !representable) {
-                atomicOr(status, kStatusCapacity);  // finite but beyond the block key range
+            } else {
+                if (finite3(pos) && !representable) atomicOr(status, kStatusCapacity);  // beyond the key range
+                // no CPU fallback on this path: an unprojectable plastic state is unavailable here
+                if (!plastic_ok) atomicOr(status, kStatusResident);
             }
             x = pos;
             v = vel;
@@ -413,6 +434,11 @@ __global__ void __launch_bounds__(kThreads, TMPM_TRANSFER_MIN_BLOCKS)
             P.x[cap + i] = x.y;
             P.x[2 * cap + i] = x.z;
             if (!fixed) store_m3(P.F, cap, i, F);
+            if (plastic && !fixed) {
+                P.pl[i] = pl[0];
+                P.pl[cap + i] = pl[1];
+                P.pl[2 * cap + i] = pl[2];
+            }
             if (MODE == kModeG2P) {
                 P.v[i] = v.x;
                 P.v[cap + i] = v.y;
@@ -444,7 +470,7 @@ __global__ void __launch_bounds__(kThreads, TMPM_TRANSFER_MIN_BLOCKS)
     V3f mv = mk(0, 0, 0);
     float bound_m = 0.f, bound_p = 0.f;
     if (active) {
-        M3f S = scaled_stress(k, F, Cm, -dt * inv_d);
+        M3f S = scaled_stress(k, F, Cm, -dt * inv_d, pl[0]);
         A = add(S, scale(Cm, k.mass));
         mv = v * k.mass;
         // |(m v + A dpos)_i| <= |m v_i| + 1.5 h sum_j |A_ij| and a particle's 27 weights sum to one,
@@ -673,6 +699,7 @@ __global__ void k_gather(ParticleSoA src, ParticleSoA dst, const uint32_t *__res
     for (int c = 0; c < 3; ++c) {
         dst.x[c * cd + j] = src.x[c * cs + s];
         dst.v[c * cd + j] = src.v[c * cs + s];
+        dst.pl[c * cd + j] = src.pl[c * cs + s];
     }
     for (int c = 0; c < 9; ++c) {
         dst.C[c * cd + j] = src.C[c * cs + s];
@@ -724,17 +751,21 @@ void launch_transfer(int mode, const ParticleSoA &P, int n, const DevClass *clas
                      double *reactions, uint32_t *status, int *cache, cudaStream_t stream) {
     if (n <= 0) return;
     dim3 grid((n + kThreads - 1) / kThreads);
+#define TMPM_LAUNCH(M, PL) \
+    k_transfer<M, PL><<<grid, kThreads, 0, stream>>>(P, n, classes, cur, next, sp, obstacles, planes, reactions, status, cache)
+    const bool pl = sp.has_plastic != 0;
     switch (mode) {
     case kModeP2G:
-        k_transfer<kModeP2G><<<grid, kThreads, 0, stream>>>(P, n, classes, cur, next, sp, obstacles, planes, reactions, status, cache);
+        if (pl) TMPM_LAUNCH(kModeP2G, true); else TMPM_LAUNCH(kModeP2G, false);
         break;
     case kModeG2P2G:
-        k_transfer<kModeG2P2G><<<grid, kThreads, 0, stream>>>(P, n, classes, cur, next, sp, obstacles, planes, reactions, status, cache);
+        if (pl) TMPM_LAUNCH(kModeG2P2G, true); else TMPM_LAUNCH(kModeG2P2G, false);
         break;
     default:
-        k_transfer<kModeG2P><<<grid, kThreads, 0, stream>>>(P, n, classes, cur, next, sp, obstacles, planes, reactions, status, cache);
+        if (pl) TMPM_LAUNCH(kModeG2P, true); else TMPM_LAUNCH(kModeG2P, false);
         break;
     }
+#undef TMPM_LAUNCH
 }
 
 void launch_grid_update(const GridTable &g, const GridTable &next, const SimParams &sp, const DevObstacle *obstacles,

@@ -454,13 +454,13 @@ struct PinnedBuf {
 };
 
 struct ParticleBuffers {
-    DevBuf<float> x, v, C, F;
+    DevBuf<float> x, v, C, F, pl;
     DevBuf<uint32_t> cls, widx;
     size_t cap = 0;
     cudaError_t alloc(size_t c) {
         cudaError_t e;
         if ((e = x.alloc(3 * c)) || (e = v.alloc(3 * c)) || (e = C.alloc(9 * c)) || (e = F.alloc(9 * c)) ||
-            (e = cls.alloc(c)) || (e = widx.alloc(c)))
+            (e = pl.alloc(3 * c)) || (e = cls.alloc(c)) || (e = widx.alloc(c)))
             return e;
         cap = c;
         return cudaSuccess;
@@ -471,6 +471,7 @@ struct ParticleBuffers {
         p.v = v.ptr;
         p.C = C.ptr;
         p.F = F.ptr;
+        p.pl = pl.ptr;
         p.force = force;
         p.cls = cls.ptr;
         p.widx = widx.ptr;
@@ -510,6 +511,7 @@ struct GridBuffers {
     }
 };
 
+// Device material codes, as the reference packs them (gpu.rs:1171-1276).
 int class_kind(int material) {
     switch (material) {
     case TMPM_MAT_NEO_HOOKEAN:
@@ -518,8 +520,14 @@ int class_kind(int material) {
         return kMatFluid;
     case TMPM_MAT_ELASTIC:
         return kMatCorotated;
+    case TMPM_MAT_SNOW:
+        return kMatSnow;
+    case TMPM_MAT_SAND:
+        return kMatSand;
+    case TMPM_MAT_SAND_NEO_HOOKEAN:
+        return kMatSandNeoHookean;
     default:
-        return 0;  // plastic materials: not on this device path
+        return 0;
     }
 }
 
@@ -562,6 +570,7 @@ struct TmpmSession {
     PinnedBuf staging;         // readback
     PinnedBuf upload_staging;  // packed f32 state for uploads
     bool force_dirty = false;
+    bool has_plastic = false;  // class table holds a snow, sand or NH sand class
     uint64_t since_resort = 0;
 
     ~TmpmSession() {
@@ -607,6 +616,7 @@ struct TmpmSession {
         sp.reactions = 0;
         sp.apply_force = 0;
         sp.resident_checks = resident ? 1 : 0;
+        sp.has_plastic = has_plastic ? 1 : 0;
         return sp;
     }
 
@@ -688,7 +698,7 @@ struct TmpmSession {
                 }
                 int kind = class_kind(world.material[i]);
                 const double *mp = &world.mparams[5 * i];
-                if (kind == kMatCorotated) {
+                if (kind == kMatCorotated || kind == kMatSand || kind == kMatSnow) {
                     // use_cpu_corotated (gpu.rs:1156-1170): ill-conditioned F is a CPU case
                     const double *Fm = &world.F[9 * i];
                     double nrm = fro9(Fm), inrm = std::numeric_limits<double>::infinity();
@@ -725,6 +735,17 @@ struct TmpmSession {
                     k.p0 = l32;
                     k.p1 = m32b;
                     k.wave = std::sqrt((l32 + 2.0f * m32b) / rho);
+                    // sand / NH sand: friction angle, cohesion; snow: hardening, critical compression, stretch
+                    bool ok = true;
+                    if (kind == kMatSand || kind == kMatSandNeoHookean) {
+                        ok = f32_ok(mp[2], k.p2) && f32_ok(mp[3], k.p3);
+                    } else if (kind == kMatSnow) {
+                        ok = f32_ok(mp[4], k.p2) && f32_ok(mp[2], k.p3) && f32_ok(mp[3], k.p4);
+                    }
+                    float t3;
+                    if (kind >= kMatSnow)
+                        for (int q = 0; q < 3; ++q) ok = ok && f32_ok(world.plastic[3 * i + q], t3);
+                    if (!ok) return bad(i, TMPM_ERR_INVALID_INPUT, "plastic parameters not representable in f32");
                 }
                 uint32_t ci;
                 if (last_ci != kClassMask && std::memcmp(&k, &last, sizeof(DevClass)) == 0) {
@@ -792,12 +813,14 @@ struct TmpmSession {
         }
         if (n_enabled > static_cast<size_t>(std::numeric_limits<int>::max() / 2))
             return fail(TMPM_ERR_CAPACITY, "too many particles for one session");
+        bool plastic_classes = false;
+        for (const DevClass &k : cls_table) plastic_classes = plastic_classes || k.kind >= kMatSnow;
         const size_t cap = std::max<size_t>(256, (n_enabled + 255) / 256 * 256);
-        if (!upload_staging.ensure((24 * cap + 2 * cap) * sizeof(float)))
+        if (!upload_staging.ensure((27 * cap + 2 * cap) * sizeof(float)))
             return fail(TMPM_ERR_DEVICE, "cudaMallocHost upload staging failed");
         float *hx = static_cast<float *>(upload_staging.ptr);
-        float *hv = hx + 3 * cap, *hC = hv + 3 * cap, *hF = hC + 9 * cap;
-        uint32_t *hcls = reinterpret_cast<uint32_t *>(hF + 9 * cap), *hwidx = hcls + cap;
+        float *hv = hx + 3 * cap, *hC = hv + 3 * cap, *hF = hC + 9 * cap, *hpl = hF + 9 * cap;
+        uint32_t *hcls = reinterpret_cast<uint32_t *>(hpl + 3 * cap), *hwidx = hcls + cap;
         parallel_chunks(N, [&](size_t c, size_t lo, size_t hi) {
             size_t j = offset[c];
             const std::vector<uint32_t> &rm = remap[c];
@@ -811,6 +834,7 @@ struct TmpmSession {
                     hC[k9 * cap + j] = static_cast<float>(world.C[9 * i + k9]);
                     hF[k9 * cap + j] = static_cast<float>(world.F[9 * i + k9]);
                 }
+                for (int k3 = 0; k3 < 3; ++k3) hpl[k3 * cap + j] = static_cast<float>(world.plastic[3 * i + k3]);
                 hcls[j] = rm[lcls[i]] | (world.fixed[i] ? kFixedBit : 0u);
                 hwidx[j] = static_cast<uint32_t>(i);
                 ++j;
@@ -894,6 +918,7 @@ struct TmpmSession {
         if ((e = reactions.alloc(6 * std::max<size_t>(obstacles.size(), 1)))) return cuda_fail(e, "cudaMalloc reactions");
 
         n_dev = static_cast<int>(n_enabled);
+        has_plastic = plastic_classes;
         cur = 0;
         ParticleBuffers &pb = pbuf[0];
         if (n_dev) {
@@ -901,6 +926,7 @@ struct TmpmSession {
             cudaMemcpyAsync(pb.v.ptr, hv, sizeof(float) * 3 * cap, cudaMemcpyHostToDevice, stream);
             cudaMemcpyAsync(pb.C.ptr, hC, sizeof(float) * 9 * cap, cudaMemcpyHostToDevice, stream);
             cudaMemcpyAsync(pb.F.ptr, hF, sizeof(float) * 9 * cap, cudaMemcpyHostToDevice, stream);
+            cudaMemcpyAsync(pb.pl.ptr, hpl, sizeof(float) * 3 * cap, cudaMemcpyHostToDevice, stream);
             cudaMemcpyAsync(pb.cls.ptr, hcls, sizeof(uint32_t) * cap, cudaMemcpyHostToDevice, stream);
             cudaMemcpyAsync(pb.widx.ptr, hwidx, sizeof(uint32_t) * cap, cudaMemcpyHostToDevice, stream);
         }
@@ -1067,7 +1093,7 @@ struct TmpmSession {
         const int n = n_dev;
         if (n > 0) {
             const size_t pc = pbuf[cur].cap;
-            size_t floats = 24 * static_cast<size_t>(n);
+            size_t floats = 27 * static_cast<size_t>(n);
             if (!staging.ensure(floats * sizeof(float) + sizeof(uint32_t) * n))
                 return fail(TMPM_ERR_DEVICE, "cudaMallocHost staging failed");
             float *h = static_cast<float *>(staging.ptr);
@@ -1080,13 +1106,15 @@ struct TmpmSession {
                 cudaMemcpyAsync(h + (6 + k) * n, pb.C.ptr + k * pc, sizeof(float) * n, cudaMemcpyDeviceToHost, stream);
                 cudaMemcpyAsync(h + (15 + k) * n, pb.F.ptr + k * pc, sizeof(float) * n, cudaMemcpyDeviceToHost, stream);
             }
+            for (int k = 0; k < 3; ++k)
+                cudaMemcpyAsync(h + (24 + k) * n, pb.pl.ptr + k * pc, sizeof(float) * n, cudaMemcpyDeviceToHost, stream);
             uint32_t *widx = reinterpret_cast<uint32_t *>(h + floats);
             cudaMemcpyAsync(widx, pb.widx.ptr, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost, stream);
             if ((e = cudaStreamSynchronize(stream))) return cuda_fail(e, "readback");
             // collect_prepared: non-finite transfers are an error before anything is applied
             std::atomic<bool> bad{false};
             parallel_for(static_cast<size_t>(n), [&](size_t a, size_t b) {
-                for (size_t c = 0; c < 24 && !bad.load(std::memory_order_relaxed); ++c)
+                for (size_t c = 0; c < 27 && !bad.load(std::memory_order_relaxed); ++c)
                     for (size_t j = a; j < b; ++j)
                         if (!std::isfinite(h[c * n + j])) {
                             bad = true;
@@ -1113,6 +1141,9 @@ struct TmpmSession {
                         world.C[9 * w + k] = h[(6 + k) * n + j];
                         world.F[9 * w + k] = h[(15 + k) * n + j];
                     }
+                    const int mat = world.material[w];
+                    if (mat == TMPM_MAT_SAND || mat == TMPM_MAT_SNOW || mat == TMPM_MAT_SAND_NEO_HOOKEAN)
+                        for (int k = 0; k < 3; ++k) world.plastic[3 * w + k] = h[(24 + k) * n + j];
                 }
             });
         }
