@@ -243,7 +243,8 @@ TmpmStatus tmpm_step_cfl_with_reactions(TmpmSession *session, double dt,
  * the binning step of the substep on `count` f32 positions stored
  * component-major on the device (x[0..count), then y and z, `stride` floats
  * apart) and writes, to caller-owned device buffers, the stable order of the
- * particles by the Morton key of their 4^3 grid block (order_out) and, when
+ * particles by the 21-bit Morton key of their 4^3 grid block (block
+ * coordinates taken modulo 128) (order_out) and, when
  * keys_out is not NULL, the sorted keys.  `stream` is a cudaStream_t (NULL =
  * the default stream); the call is asynchronous on it.
  * It allocates nothing: its scratch is a fixed array inside the library
@@ -257,6 +258,96 @@ TmpmStatus tmpm_step_cfl_with_reactions(TmpmSession *session, double dt,
 TmpmStatus tmpm_sort_by_block_noalloc(const float *positions, size_t count, size_t stride,
                                       double cell_width, uint32_t *order_out, uint32_t *keys_out,
                                       void *stream);
+
+/* --------------------------- multi-scene batches --------------------------- */
+
+/* No single counterpart in the reference, which runs one MpmWorld per
+ * GpuMpmResidentSession (gpu.rs:206-662).  A batch keeps many independent
+ * scenes resident on one device and advances them together: every kernel of a
+ * substep is one launch over the particles of all scenes, each scene with its
+ * own MpmParams (cell width, gravity, bounds), substep dt and substep count.
+ * Per scene the result is the same as a TmpmSession over that scene alone
+ * (tmpm_session_create + tmpm_step), within f32 round-off: the transfer
+ * arithmetic is the same, only the partition of particles into thread blocks
+ * differs.  Limits: 256 live scenes, transfer colours below 256, no obstacles
+ * and no per-particle forces.  Each scene is validated like
+ * validate_resident_world (gpu.rs:664-677) when it is added. */
+typedef struct TmpmBatch TmpmBatch;
+
+typedef struct TmpmBatchOptions {
+    int32_t device;            /* CUDA device ordinal */
+    uint32_t max_blocks;       /* 0 = size the block pool from the scenes' occupied blocks */
+    uint32_t use_graphs;       /* 1 = replay each batch as a CUDA graph (captured once per shape) */
+    uint32_t reserved;
+    uint64_t particle_capacity; /* initial device rows (0 = grow on demand) */
+} TmpmBatchOptions;
+
+TmpmStatus tmpm_batch_create(const TmpmBatchOptions *options, TmpmBatch **out);
+void tmpm_batch_destroy(TmpmBatch *batch);
+
+/* A scene validated like validate_resident_world (gpu.rs:664-677) and packed
+ * into pinned host memory, not yet attached to a batch.  Preparing does no
+ * device work and touches no batch, so scenes may be prepared on any thread,
+ * also while a batch is in flight. */
+typedef struct TmpmPreparedScene TmpmPreparedScene;
+TmpmStatus tmpm_scene_prepare(const TmpmParams *params, const TmpmParticleArrays *particles,
+                              double substep_dt, TmpmPreparedScene **out);
+void tmpm_scene_prepared_destroy(TmpmPreparedScene *prepared);
+size_t tmpm_scene_prepared_particle_count(const TmpmPreparedScene *prepared);
+/* Device bytes the scene will hold in a batch (admission by footprint). */
+size_t tmpm_scene_prepared_bytes(const TmpmPreparedScene *prepared);
+
+/* Attach a prepared scene (the batch takes ownership, also on failure);
+ * *scene_out receives its id (0..255).  Allowed while a batch is in flight:
+ * the rows are copied to the device at the next submit. */
+TmpmStatus tmpm_batch_admit(TmpmBatch *batch, TmpmPreparedScene *prepared, uint32_t *scene_out);
+
+/* tmpm_scene_prepare + tmpm_batch_admit (GpuMpmResidentSession::new for one
+ * scene, gpu.rs:253-280). */
+TmpmStatus tmpm_batch_add_scene(TmpmBatch *batch, const TmpmParams *params,
+                                const TmpmParticleArrays *particles, double substep_dt,
+                                uint32_t *scene_out);
+
+/* Retire a scene (allowed while a batch is in flight).  Its device rows are
+ * dropped by the next batch's re-sort and its id becomes free then. */
+TmpmStatus tmpm_batch_remove_scene(TmpmBatch *batch, uint32_t scene);
+
+/* Queue one batch: scene ids[k] advances steps[k] substeps (1..4096); scenes
+ * not listed stay put.  When collect is not NULL and collect[k] != 0, the
+ * scene's rows are copied to pinned host memory right after the batch, so
+ * tmpm_batch_read_scene needs no device work for it (and may run while the
+ * next batch is in flight).  Asynchronous, like submit_steps
+ * (gpu.rs:303-322); one batch may be in flight. */
+TmpmStatus tmpm_batch_submit(TmpmBatch *batch, const uint32_t *ids, const uint32_t *steps,
+                             const uint8_t *collect, size_t count);
+
+/* Wait for the batch in flight (bounded, as gpu.rs:1853-1862) and record each
+ * scene's outcome.  A scene whose resident checks failed (CFL, escape,
+ * ill-conditioned F, unprojectable plastic state) is marked failed with
+ * TMPM_ERR_RESIDENT_UNAVAILABLE and keeps its last read state; the other
+ * scenes are unaffected.  Block-pool or hash-table overflow fails the batch. */
+TmpmStatus tmpm_batch_synchronize(TmpmBatch *batch);
+int32_t tmpm_batch_pending(const TmpmBatch *batch);
+
+/* Per-scene state: outcome (TMPM_OK or the failure), completed substeps,
+ * particle count, and the particles themselves (like world() after
+ * synchronize, gpu.rs:654-661): from the collected rows, else read back from
+ * the device, which needs no batch in flight. */
+TmpmStatus tmpm_batch_scene_status(const TmpmBatch *batch, uint32_t scene);
+uint64_t tmpm_batch_scene_substeps(const TmpmBatch *batch, uint32_t scene);
+size_t tmpm_batch_scene_particle_count(const TmpmBatch *batch, uint32_t scene);
+TmpmStatus tmpm_batch_read_scene(TmpmBatch *batch, uint32_t scene, TmpmParticleArrays *out);
+
+/* Device milliseconds of the last synchronized batch (CUDA events on the
+ * batch stream around its kernels). */
+double tmpm_batch_last_ms(const TmpmBatch *batch);
+
+/* Device bytes held by the batch, and the bytes a scene of `particles`
+ * particles over `home_blocks` occupied 4^3 blocks adds (admission control). */
+size_t tmpm_batch_device_bytes(const TmpmBatch *batch);
+size_t tmpm_batch_scene_bytes(size_t particles, size_t home_blocks);
+
+const char *tmpm_batch_last_error_message(const TmpmBatch *batch);
 
 /* ------------------------------ diagnostics ------------------------------ */
 

@@ -279,11 +279,13 @@ def _spread10(v: np.ndarray) -> np.ndarray:
     return v
 
 
-def block_morton_keys(base_cells: np.ndarray) -> np.ndarray:
-    """30-bit Morton key of the 4^3 block holding each base cell (block coords mod 1024)."""
+def block_morton_keys(base_cells: np.ndarray, scene: int = 0) -> np.ndarray:
+    """Sort key of the 4^3 block holding each base cell: scene << 21 | 21-bit Morton
+    code of the block coordinates taken modulo 128."""
     b = np.right_shift(np.asarray(base_cells, dtype=np.int32), BLOCK_SHIFT)
-    bu = b.astype(np.uint32)
-    return (_spread10(bu[:, 0]) << np.uint32(2)) | (_spread10(bu[:, 1]) << np.uint32(1)) | _spread10(bu[:, 2])
+    bu = b.astype(np.uint32) & np.uint32(0x7F)
+    m = (_spread10(bu[:, 0]) << np.uint32(2)) | (_spread10(bu[:, 1]) << np.uint32(1)) | _spread10(bu[:, 2])
+    return (np.uint32(scene & 0xFF) << np.uint32(21)) | m
 
 
 def binning_reference(position_f32: np.ndarray, cell_width: float):

@@ -130,6 +130,16 @@ class TmpmSessionOptions(C.Structure):
     ]
 
 
+class TmpmBatchOptions(C.Structure):
+    _fields_ = [
+        ("device", C.c_int32),
+        ("max_blocks", C.c_uint32),
+        ("use_graphs", C.c_uint32),
+        ("reserved", C.c_uint32),
+        ("particle_capacity", C.c_uint64),
+    ]
+
+
 def make_params(cell_width, gravity=(0.0, 0.0, -9.81), max_substep=1e-3,
                 bounds=None, wall_mode=0) -> TmpmParams:
     p = TmpmParams()

@@ -10,7 +10,7 @@ import ctypes as C
 import os
 import subprocess
 
-from ._abi import TmpmObstacle, TmpmParams, TmpmParticleArrays, TmpmSessionOptions
+from ._abi import TmpmBatchOptions, TmpmObstacle, TmpmParams, TmpmParticleArrays, TmpmSessionOptions
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.environ.get("TMPM_LIB_PATH") or os.path.join(_HERE, "libtmpm.so")
@@ -88,6 +88,48 @@ def lib():
     L.tmpm_bench_substeps.restype = S
     L.tmpm_sort_by_block_noalloc.argtypes = [P, C.c_size_t, C.c_size_t, C.c_double, P, P, P]
     L.tmpm_sort_by_block_noalloc.restype = S
+    U32 = C.c_uint32
+    L.tmpm_batch_create.argtypes = [C.POINTER(TmpmBatchOptions), C.POINTER(P)]
+    L.tmpm_batch_create.restype = S
+    L.tmpm_batch_destroy.argtypes = [P]
+    L.tmpm_batch_destroy.restype = None
+    L.tmpm_batch_add_scene.argtypes = [P, C.POINTER(TmpmParams), C.POINTER(TmpmParticleArrays), C.c_double,
+                                       C.POINTER(U32)]
+    L.tmpm_batch_add_scene.restype = S
+    L.tmpm_batch_remove_scene.argtypes = [P, U32]
+    L.tmpm_batch_remove_scene.restype = S
+    L.tmpm_batch_submit.argtypes = [P, P, P, P, C.c_size_t]
+    L.tmpm_batch_submit.restype = S
+    L.tmpm_batch_synchronize.argtypes = [P]
+    L.tmpm_batch_synchronize.restype = S
+    L.tmpm_batch_pending.argtypes = [P]
+    L.tmpm_batch_pending.restype = C.c_int32
+    L.tmpm_batch_scene_status.argtypes = [P, U32]
+    L.tmpm_batch_scene_status.restype = S
+    L.tmpm_batch_scene_substeps.argtypes = [P, U32]
+    L.tmpm_batch_scene_substeps.restype = C.c_uint64
+    L.tmpm_batch_scene_particle_count.argtypes = [P, U32]
+    L.tmpm_batch_scene_particle_count.restype = C.c_size_t
+    L.tmpm_batch_read_scene.argtypes = [P, U32, C.POINTER(TmpmParticleArrays)]
+    L.tmpm_batch_read_scene.restype = S
+    L.tmpm_batch_last_ms.argtypes = [P]
+    L.tmpm_batch_last_ms.restype = C.c_double
+    L.tmpm_batch_device_bytes.argtypes = [P]
+    L.tmpm_batch_device_bytes.restype = C.c_size_t
+    L.tmpm_batch_scene_bytes.argtypes = [C.c_size_t, C.c_size_t]
+    L.tmpm_batch_scene_bytes.restype = C.c_size_t
+    L.tmpm_scene_prepare.argtypes = [C.POINTER(TmpmParams), C.POINTER(TmpmParticleArrays), C.c_double, C.POINTER(P)]
+    L.tmpm_scene_prepare.restype = S
+    L.tmpm_scene_prepared_destroy.argtypes = [P]
+    L.tmpm_scene_prepared_destroy.restype = None
+    L.tmpm_scene_prepared_particle_count.argtypes = [P]
+    L.tmpm_scene_prepared_particle_count.restype = C.c_size_t
+    L.tmpm_scene_prepared_bytes.argtypes = [P]
+    L.tmpm_scene_prepared_bytes.restype = C.c_size_t
+    L.tmpm_batch_admit.argtypes = [P, P, C.POINTER(U32)]
+    L.tmpm_batch_admit.restype = S
+    L.tmpm_batch_last_error_message.argtypes = [P]
+    L.tmpm_batch_last_error_message.restype = C.c_char_p
     _lib = L
     return L
 

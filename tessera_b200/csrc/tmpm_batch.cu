@@ -1,0 +1,990 @@
+// tmpm_batch.cu -- multi-scene batches (include/tmpm.h, "multi-scene batches").
+//
+// Many independent scenes share one set of device particle rows, one class
+// table, one sparse grid (each scene in its own namespace of the block key:
+// scene << 8 | transfer colour) and one stream.  A batch is one re-sort, one
+// opening P2G and S x (grid update, fused G2P+P2G) launches over the rows of
+// every scene, S being the largest substep count asked for; each scene takes
+// part in its own first `steps` substeps only (the transfer kernel gates on
+// the scene table) and writes its velocity and affine matrix back at its last
+// substep.  The per-scene constants live in a device scene table that is
+// copied once per batch.
+//
+// Device rows stay sorted by (scene, block) after every batch's re-sort, so a
+// scene occupies one contiguous range and is read back with a few strided
+// copies.  Admission is split for overlap with device work: a scene is
+// validated and packed into pinned memory by tmpm_scene_prepare (any thread,
+// no device work), attached to the batch by tmpm_batch_admit (allowed while a
+// batch is in flight) and copied to the device at the next submit, appended
+// after the resident rows.  A retired scene is marked removed: the next
+// re-sort moves its rows past the live ones and drops them.  Finished scenes
+// can be collected: their rows are copied to pinned memory right after the
+// batch that finishes them, so reading them needs no device work.
+
+#include <chrono>
+#include <cstdio>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <tuple>
+
+#include "tmpm_host.h"
+
+using namespace tmpm;
+
+namespace {
+
+// Pinned host buffers are expensive to create (page locking), so released ones
+// are kept for reuse, up to kPoolKeepBytes in total.
+constexpr size_t kPoolKeepBytes = size_t(8) << 30;
+
+struct PinnedPool {
+    std::mutex mu;
+    std::vector<std::pair<void *, size_t>> free_list;
+    size_t free_bytes = 0;
+
+    void *acquire(size_t bytes, size_t &got) {
+        {
+            std::lock_guard<std::mutex> lock(mu);
+            size_t best = free_list.size();
+            for (size_t k = 0; k < free_list.size(); ++k) {
+                size_t b = free_list[k].second;
+                if (b >= bytes && b <= 2 * bytes + (size_t(64) << 20) &&
+                    (best == free_list.size() || b < free_list[best].second))
+                    best = k;
+            }
+            if (best != free_list.size()) {
+                void *p = free_list[best].first;
+                got = free_list[best].second;
+                free_bytes -= got;
+                free_list.erase(free_list.begin() + best);
+                return p;
+            }
+        }
+        void *p = nullptr;
+        if (cudaMallocHost(&p, bytes) != cudaSuccess) return nullptr;
+        got = bytes;
+        return p;
+    }
+
+    void release(void *p, size_t bytes) {
+        if (!p) return;
+        std::vector<void *> drop;
+        {
+            std::lock_guard<std::mutex> lock(mu);
+            free_list.emplace_back(p, bytes);
+            free_bytes += bytes;
+            while (free_bytes > kPoolKeepBytes && !free_list.empty()) {
+                drop.push_back(free_list.front().first);
+                free_bytes -= free_list.front().second;
+                free_list.erase(free_list.begin());
+            }
+        }
+        for (void *q : drop) cudaFreeHost(q);
+    }
+};
+
+PinnedPool &pinned_pool() {
+    static PinnedPool *pool = new PinnedPool();  // outlives every batch (never destroyed at exit)
+    return *pool;
+}
+
+// A pinned buffer borrowed from the pool.
+struct PinnedLease {
+    void *ptr = nullptr;
+    size_t bytes = 0;
+    bool ensure(size_t b) {
+        if (b <= bytes) return true;
+        release();
+        ptr = pinned_pool().acquire(b, bytes);
+        if (!ptr) bytes = 0;
+        return ptr != nullptr;
+    }
+    void release() {
+        pinned_pool().release(ptr, bytes);
+        ptr = nullptr;
+        bytes = 0;
+    }
+    PinnedLease() = default;
+    PinnedLease(const PinnedLease &) = delete;
+    PinnedLease &operator=(const PinnedLease &) = delete;
+    PinnedLease(PinnedLease &&o) noexcept { *this = std::move(o); }
+    PinnedLease &operator=(PinnedLease &&o) noexcept {
+        if (this != &o) {
+            release();
+            std::swap(ptr, o.ptr);
+            std::swap(bytes, o.bytes);
+        }
+        return *this;
+    }
+    ~PinnedLease() { release(); }
+};
+
+// Per-particle device bytes: two row sets of 27 floats + class + index, sort
+// keys and values (double-buffered); per home block the pool sizing rule
+// (16 blocks per occupied block) x two pools of 64 float4 nodes + coords +
+// two hash slots.
+constexpr size_t kBytesPerRow = 2 * (27 * 4 + 2 * 4) + 4 * 4;
+constexpr size_t kBytesPerPoolBlock = 2 * kNodesPerBlock * 16 + 16 + 2 * (8 + 4);
+
+// Rows of one scene in pinned memory: 27 f32 component rows of `stride`, then
+// class and world-index rows.
+float *row_base(PinnedLease &l) { return static_cast<float *>(l.ptr); }
+uint32_t *row_cls(PinnedLease &l, size_t stride) { return reinterpret_cast<uint32_t *>(row_base(l) + 27 * stride); }
+uint32_t *row_widx(PinnedLease &l, size_t stride) { return row_cls(l, stride) + stride; }
+
+}  // namespace
+
+// A validated, packed scene waiting for admission (no device state).
+struct TmpmPreparedScene {
+    TmpmParams params{};
+    double dt = 0.0;
+    HostWorld world;
+    ClassTable classes;     // local classes (namespace 0)
+    PinnedLease rows;       // packed rows, class ids local
+    size_t m = 0;           // enabled particles (device rows)
+    size_t blocks = 0;      // occupied home blocks
+};
+
+namespace {
+
+TmpmStatus prepare_scene(const TmpmParams &params, const TmpmParticleArrays *particles, double dt,
+                         TmpmPreparedScene &p) {
+    if (!params_valid(params)) {
+        g_last_error = "invalid MPM input";
+        return TMPM_ERR_MPM_INVALID_INPUT;
+    }
+    std::string err;
+    TmpmStatus st = load_checked(particles, p.world, err);
+    if (st != TMPM_OK) {
+        g_last_error = err;
+        return st;
+    }
+    if (p.world.n >= (1u << 31)) {
+        g_last_error = "too many particles in one scene";
+        return TMPM_ERR_CAPACITY;
+    }
+    for (size_t i = 0; i < p.world.n; ++i)
+        if (p.world.color[i] >= kMaxBatchColors) {
+            g_last_error = "transfer colours in a batch must be below 256";
+            return TMPM_ERR_INVALID_INPUT;
+        }
+    // validate_resident_world (gpu.rs:664-677)
+    if (!std::isfinite(dt) || dt <= 0.0 || dt > stable_timestep(p.world, params)) {
+        g_last_error = "substep dt is not finite, not positive or above the CFL bound";
+        return TMPM_ERR_INVALID_INPUT;
+    }
+    float h32, dt32, inv_d32;
+    if (!f32_ok(params.cell_width, h32) || !f32_ok(dt, dt32) ||
+        !f32_ok(4.0 / (params.cell_width * params.cell_width), inv_d32) || h32 <= 0.0f || dt32 <= 0.0f ||
+        !std::isfinite(1.0f / h32)) {
+        g_last_error = "cell width or substep not representable in f32";
+        return TMPM_ERR_INVALID_INPUT;
+    }
+    size_t stride = 0;
+    PackResult pr = pack_world(p.world, 1.0f / h32, 0u, p.classes, [&](size_t n_enabled) {
+        PackTarget tg;
+        stride = std::max<size_t>(n_enabled, 1);
+        if (!p.rows.ensure(29 * stride * sizeof(float))) return tg;
+        tg.base = row_base(p.rows);
+        tg.cls = row_cls(p.rows, stride);
+        tg.widx = row_widx(p.rows, stride);
+        tg.stride = stride;
+        return tg;
+    });
+    if (pr.st != TMPM_OK) {
+        g_last_error = pr.msg;
+        return pr.st;
+    }
+    p.params = params;
+    p.dt = dt;
+    p.m = pr.enabled;
+    p.blocks = pr.blocks.size();
+    return TMPM_OK;
+}
+
+struct BatchScene {
+    bool live = false;
+    bool draining = false;   // removed; its rows go at the next re-sort
+    TmpmParams params{};
+    double dt = 0.0;
+    HostWorld world;         // admitted state, or the last state read back
+    bool stale = false;      // the device holds substeps `world` lacks
+    uint64_t substeps = 0;   // substeps completed on the device
+    size_t dev_offset = 0;   // first device row
+    size_t dev_count = 0;    // enabled particles (device rows)
+    size_t blocks = 0;       // occupied home blocks at admission (pool sizing)
+    uint32_t queued = 0;     // substeps in the batch in flight
+    std::unique_ptr<TmpmPreparedScene> staged;  // admitted, rows not yet on the device
+    PinnedLease result;      // rows collected at the end of a batch
+    bool collect = false;    // the batch in flight copies this scene's rows back
+    bool collected = false;  // `result` holds the scene's latest rows
+    TmpmStatus status = TMPM_OK;
+    std::string error;
+};
+
+}  // namespace
+
+struct TmpmBatch {
+    TmpmBatchOptions options{};
+    int device = 0;
+    bool valid = true;
+    std::string last_error;
+    std::vector<BatchScene> scenes;  // indexed by scene id
+    ClassTable classes;
+    size_t classes_uploaded = 0;
+
+    cudaStream_t stream = nullptr;
+    cudaEvent_t done = nullptr, t_begin = nullptr, t_end = nullptr;
+    ParticleBuffers pbuf[2];
+    int cur = 0;
+    size_t n_phys = 0;  // device rows in use (live + draining)
+    size_t n_live = 0;  // rows of live scenes, staged ones included
+    DevBuf<DevClass> dclasses;
+    GridBuffers grids[2];
+    DevBuf<uint32_t> status, scene_status;
+    DevBuf<SceneParams> dscenes;
+    DevBuf<int> cta_cache;
+    DevBuf<uint32_t> sort_keys[2], sort_vals[2], sort_hist, sort_totals;
+    PinnedBuf staging, table_staging;
+    std::vector<std::unique_ptr<TmpmPreparedScene>> in_flight_uploads;  // kept until the copies complete
+    std::vector<std::unique_ptr<PinnedLease>> in_flight_results;        // results of scenes removed mid-flight
+    uint64_t epoch = 1;  // bumps whenever a device pointer a graph holds changes
+    bool pending = false;
+    double last_ms = 0.0;
+
+    struct GraphKey {
+        uint32_t steps;
+        size_t n_phys, n_live;
+        int cur;
+        uint64_t epoch;
+        bool operator<(const GraphKey &o) const {
+            return std::tie(steps, n_phys, n_live, cur, epoch) < std::tie(o.steps, o.n_phys, o.n_live, o.cur, o.epoch);
+        }
+    };
+    std::map<GraphKey, cudaGraphExec_t> graphs;
+
+    ~TmpmBatch() {
+        if (stream) cudaStreamSynchronize(stream);
+        drop_graphs();
+        if (done) cudaEventDestroy(done);
+        if (t_begin) cudaEventDestroy(t_begin);
+        if (t_end) cudaEventDestroy(t_end);
+        if (stream) cudaStreamDestroy(stream);
+    }
+
+    void drop_graphs() {
+        for (auto &kv : graphs) cudaGraphExecDestroy(kv.second);
+        graphs.clear();
+    }
+
+    TmpmStatus fail(TmpmStatus st, const std::string &msg) {
+        last_error = msg;
+        g_last_error = msg;
+        return st;
+    }
+    TmpmStatus cuda_fail(cudaError_t e, const char *what) {
+        valid = false;
+        return fail(TMPM_ERR_DEVICE, std::string(what) + ": " + cudaGetErrorString(e));
+    }
+
+    TmpmStatus guard(bool idle) {
+        if (!valid) return fail(TMPM_ERR_RESIDENT_UNAVAILABLE, "batch is invalid after an earlier error");
+        if (idle && pending) return fail(TMPM_ERR_PENDING_STEPS, "a batch is in flight; synchronize first");
+        return TMPM_OK;
+    }
+
+    BatchScene *scene_at(uint32_t id) {
+        if (id >= scenes.size() || !scenes[id].live) return nullptr;
+        return &scenes[id];
+    }
+
+    SimParams sim_params() const {
+        SimParams sp{};
+        sp.scenes = dscenes.ptr;
+        sp.scene_status = scene_status.ptr;
+        sp.multi = 1;
+        sp.step_index = 0;
+        sp.num_obstacles = 0;
+        sp.reactions = 0;
+        sp.apply_force = 0;
+        sp.resident_checks = 1;
+        sp.has_plastic = classes.plastic() ? 1 : 0;
+        return sp;
+    }
+
+    size_t total_blocks() const {
+        size_t b = 0;
+        for (const BatchScene &s : scenes)
+            if (s.live || s.draining) b += s.blocks;
+        return b;
+    }
+
+    SortBuffers sort_buffers() {
+        SortBuffers sb{};
+        sb.keys[0] = sort_keys[0].ptr;
+        sb.keys[1] = sort_keys[1].ptr;
+        sb.vals[0] = sort_vals[0].ptr;
+        sb.vals[1] = sort_vals[1].ptr;
+        sb.hist = sort_hist.ptr;
+        sb.totals = sort_totals.ptr;
+        sb.cap = sort_keys[0].count;
+        return sb;
+    }
+
+    // Grow the device rows to hold `need` rows, keeping rows [0, n_phys).  Idle only.
+    TmpmStatus ensure_rows(size_t need) {
+        cudaError_t e;
+        if (need > pbuf[cur].cap) {
+            size_t cap = std::max<size_t>(need, pbuf[cur].cap + pbuf[cur].cap / 2);
+            cap = std::max<size_t>(256, (cap + 255) / 256 * 256);
+            ParticleBuffers nb;
+            if ((e = nb.alloc(cap))) return cuda_fail(e, "cudaMalloc particles");
+            const ParticleBuffers &ob = pbuf[cur];
+            if (n_phys) {
+                auto copy_rows = [&](void *dst, const void *src, size_t elem, int rows) {
+                    return cudaMemcpy2DAsync(dst, cap * elem, src, ob.cap * elem, n_phys * elem, rows,
+                                             cudaMemcpyDeviceToDevice, stream);
+                };
+                if ((e = copy_rows(nb.x.ptr, ob.x.ptr, 4, 3)) || (e = copy_rows(nb.v.ptr, ob.v.ptr, 4, 3)) ||
+                    (e = copy_rows(nb.C.ptr, ob.C.ptr, 4, 9)) || (e = copy_rows(nb.F.ptr, ob.F.ptr, 4, 9)) ||
+                    (e = copy_rows(nb.pl.ptr, ob.pl.ptr, 4, 3)) || (e = copy_rows(nb.cls.ptr, ob.cls.ptr, 4, 1)) ||
+                    (e = copy_rows(nb.widx.ptr, ob.widx.ptr, 4, 1)))
+                    return cuda_fail(e, "grow particle rows");
+            }
+            if ((e = cudaStreamSynchronize(stream))) return cuda_fail(e, "grow particle rows");
+            pbuf[cur].swap(nb);
+            if ((e = pbuf[cur ^ 1].alloc(cap))) return cuda_fail(e, "cudaMalloc particles");
+            ++epoch;
+        }
+        const size_t cap = pbuf[cur].cap;
+        const size_t ctas = (cap + kTransferThreads - 1) / kTransferThreads;
+        if (cta_cache.count < ctas * kCacheStride) {
+            if ((e = cta_cache.alloc(ctas * kCacheStride))) return cuda_fail(e, "cudaMalloc cache");
+            ++epoch;
+        }
+        if (sort_keys[0].count < cap) {
+            const size_t tiles = (cap + 4095) / 4096;
+            for (int b = 0; b < 2; ++b)
+                if ((e = sort_keys[b].alloc(cap)) || (e = sort_vals[b].alloc(cap))) return cuda_fail(e, "cudaMalloc sort");
+            if ((e = sort_hist.alloc(256 * tiles)) || (e = sort_totals.alloc(256))) return cuda_fail(e, "cudaMalloc sort");
+            ++epoch;
+        }
+        return TMPM_OK;
+    }
+
+    TmpmStatus ensure_grid() {
+        uint64_t want = options.max_blocks ? options.max_blocks : 16 * total_blocks() + 4096;
+        if (want > (1u << 27)) want = 1u << 27;
+        if (grids[0].max_blocks >= want) return TMPM_OK;
+        if (!options.max_blocks) want = want + want / 4;  // grow with slack: admissions come one by one
+        if (want > (1u << 27)) want = 1u << 27;
+        cudaError_t e;
+        for (int g = 0; g < 2; ++g)
+            if ((e = grids[g].alloc(static_cast<uint32_t>(want)))) return cuda_fail(e, "cudaMalloc grid");
+        ++epoch;
+        return TMPM_OK;
+    }
+
+    // Idle only (synchronous copy from the host table).
+    TmpmStatus upload_classes() {
+        if (classes.table.size() == classes_uploaded) return TMPM_OK;
+        cudaError_t e;
+        if (dclasses.count < classes.table.size()) {
+            if ((e = dclasses.alloc(std::max<size_t>(2 * classes.table.size(), 64)))) return cuda_fail(e, "cudaMalloc classes");
+            ++epoch;
+        }
+        if ((e = cudaMemcpy(dclasses.ptr, classes.table.data(), sizeof(DevClass) * classes.table.size(),
+                            cudaMemcpyHostToDevice)))
+            return cuda_fail(e, "upload classes");
+        classes_uploaded = classes.table.size();
+        ++epoch;  // the transfer variant (plastic or not) captured in a graph follows the class table
+        return TMPM_OK;
+    }
+
+    // Copy the scene table (with this batch's step counts) to the device.
+    cudaError_t upload_table() {
+        SceneParams *t = static_cast<SceneParams *>(table_staging.ptr);
+        for (size_t id = 0; id < static_cast<size_t>(kMaxScenes); ++id) {
+            if (id < scenes.size() && scenes[id].live) {
+                const BatchScene &s = scenes[id];
+                t[id] = scene_params(s.params, s.dt);
+                t[id].steps = static_cast<int>(s.queued);
+            } else {
+                t[id] = SceneParams{};
+                t[id].h = 1.0f;
+                t[id].inv_h = 1.0f;
+                t[id].live = 0;
+            }
+        }
+        return cudaMemcpyAsync(dscenes.ptr, t, sizeof(SceneParams) * kMaxScenes, cudaMemcpyHostToDevice, stream);
+    }
+
+    // Device ranges after a re-sort: live scenes in id order, each contiguous.
+    void assign_offsets() {
+        size_t off = 0;
+        for (BatchScene &s : scenes) {
+            if (s.draining) s.draining = false;  // rows dropped by this re-sort: id free again
+            if (!s.live) continue;
+            s.dev_offset = off;
+            off += s.dev_count;
+        }
+        n_phys = n_live;
+    }
+
+    // Copy the rows of admitted scenes to the device (appended after the
+    // resident rows).  Idle only; the packed rows stay alive until the batch
+    // that follows completes.
+    TmpmStatus commit_staged() {
+        size_t add = 0;
+        for (BatchScene &s : scenes)
+            if (s.live && s.staged) add += s.staged->m;
+        bool any = false;
+        for (BatchScene &s : scenes) any = any || (s.live && s.staged);
+        if (!any) return TMPM_OK;
+        TmpmStatus st;
+        if ((st = ensure_rows(n_phys + add)) != TMPM_OK) return st;
+        if ((st = upload_classes()) != TMPM_OK) return st;
+        if ((st = ensure_grid()) != TMPM_OK) return st;
+        const size_t pc = pbuf[cur].cap;
+        const ParticleBuffers &pb = pbuf[cur];
+        cudaError_t e;
+        for (size_t id = 0; id < scenes.size(); ++id) {
+            BatchScene &s = scenes[id];
+            if (!s.live || !s.staged) continue;
+            TmpmPreparedScene &p = *s.staged;
+            const size_t m = p.m, stride = std::max<size_t>(m, 1);
+            if (m) {
+                const float *hb = row_base(p.rows);
+                const uint32_t *hcls = row_cls(p.rows, stride), *hw = row_widx(p.rows, stride);
+                auto rows = [&](float *dst, const float *src, int r) {
+                    return cudaMemcpy2DAsync(dst + n_phys, pc * 4, src, stride * 4, m * 4, r, cudaMemcpyHostToDevice,
+                                             stream);
+                };
+                if ((e = rows(pb.x.ptr, hb, 3)) || (e = rows(pb.v.ptr, hb + 3 * stride, 3)) ||
+                    (e = rows(pb.C.ptr, hb + 6 * stride, 9)) || (e = rows(pb.F.ptr, hb + 15 * stride, 9)) ||
+                    (e = rows(pb.pl.ptr, hb + 24 * stride, 3)) ||
+                    (e = cudaMemcpyAsync(pb.cls.ptr + n_phys, hcls, m * 4, cudaMemcpyHostToDevice, stream)) ||
+                    (e = cudaMemcpyAsync(pb.widx.ptr + n_phys, hw, m * 4, cudaMemcpyHostToDevice, stream)))
+                    return cuda_fail(e, "scene upload");
+            }
+            if ((e = cudaMemsetAsync(scene_status.ptr + id, 0, sizeof(uint32_t), stream)))
+                return cuda_fail(e, "scene status");
+            s.dev_offset = n_phys;
+            n_phys += m;
+            in_flight_uploads.push_back(std::move(s.staged));
+        }
+        return TMPM_OK;
+    }
+
+    // The kernels of one batch of `steps` substeps (captured into a graph or launched directly).
+    void launch_batch(uint32_t steps) {
+        SimParams sp = sim_params();
+        ParticleSoA src = pbuf[cur].view(nullptr, 1), dst = pbuf[cur ^ 1].view(nullptr, 1);
+        SortBuffers sb = sort_buffers();
+        launch_resort(src, dst, static_cast<int>(n_phys), static_cast<int>(n_live), dclasses.ptr, sp, sb, stream);
+        GridTable g[2];
+        g[0] = grids[0].view();
+        g[1] = g[0];
+        g[1].pool = grids[1].pool.ptr;
+        const int n = static_cast<int>(n_live);
+        launch_clear_table(g[0], stream);
+        SimParams sp0 = sp;
+        sp0.step_index = -1;
+        launch_transfer(kModeP2G, dst, n, dclasses.ptr, g[1], g[0], sp0, nullptr, nullptr, nullptr, status.ptr,
+                        cta_cache.ptr, stream);
+        for (uint32_t s = 0; s < steps; ++s) {
+            const GridTable &gc = g[s & 1], &gn = g[(s + 1) & 1];
+            SimParams spk = sp;
+            spk.step_index = static_cast<int>(s);
+            launch_grid_update(gc, gn, spk, nullptr, nullptr, nullptr, status.ptr, stream);
+            launch_transfer(s + 1 == steps ? kModeG2P : kModeG2P2G, dst, n, dclasses.ptr, gc, gn, spk, nullptr,
+                            nullptr, nullptr, status.ptr, cta_cache.ptr, stream);
+        }
+    }
+
+    TmpmStatus enqueue(uint32_t steps) {
+        cudaError_t e;
+        TmpmStatus st;
+        if ((st = commit_staged()) != TMPM_OK) return st;
+        if ((e = upload_table())) return cuda_fail(e, "scene table upload");
+        if ((e = cudaEventRecord(t_begin, stream))) return cuda_fail(e, "cudaEventRecord");
+        if (n_phys > 0) {
+            if (options.use_graphs) {
+                GraphKey key{steps, n_phys, n_live, cur, epoch};
+                auto it = graphs.find(key);
+                if (it == graphs.end()) {
+                    if (graphs.size() > 16) drop_graphs();
+                    cudaGraph_t graph = nullptr;
+                    if ((e = cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal)))
+                        return cuda_fail(e, "cudaStreamBeginCapture");
+                    launch_batch(steps);
+                    if ((e = cudaStreamEndCapture(stream, &graph))) return cuda_fail(e, "cudaStreamEndCapture");
+                    cudaGraphExec_t exec = nullptr;
+                    e = cudaGraphInstantiate(&exec, graph, 0);
+                    cudaGraphDestroy(graph);
+                    if (e) return cuda_fail(e, "cudaGraphInstantiate");
+                    it = graphs.emplace(key, exec).first;
+                }
+                if ((e = cudaGraphLaunch(it->second, stream))) return cuda_fail(e, "cudaGraphLaunch");
+            } else {
+                launch_batch(steps);
+            }
+            cur ^= 1;
+        }
+        assign_offsets();
+        if ((e = cudaEventRecord(t_end, stream))) return cuda_fail(e, "cudaEventRecord");
+        // collected scenes: rows back to pinned memory right after the batch
+        for (BatchScene &s : scenes) {
+            if (!s.live || !s.collect) continue;
+            if ((st = queue_readback(s, s.result)) != TMPM_OK) return st;
+        }
+        if ((e = cudaGetLastError())) return cuda_fail(e, "kernel launch");
+        return TMPM_OK;
+    }
+
+    // Queue the copy of a scene's rows into `dst` (27 rows + widx, stride m).
+    TmpmStatus queue_readback(BatchScene &s, PinnedLease &dst) {
+        const size_t m = s.dev_count, stride = std::max<size_t>(m, 1);
+        if (!dst.ensure(28 * stride * sizeof(float))) return fail(TMPM_ERR_DEVICE, "cudaMallocHost readback failed");
+        if (!m) return TMPM_OK;
+        const size_t pc = pbuf[cur].cap, off = s.dev_offset;
+        float *h = row_base(dst);
+        const ParticleBuffers &pb = pbuf[cur];
+        auto rows = [&](float *d, const float *src, int r) {
+            return cudaMemcpy2DAsync(d, stride * 4, src + off, pc * 4, m * 4, r, cudaMemcpyDeviceToHost, stream);
+        };
+        cudaError_t e;
+        if ((e = rows(h, pb.x.ptr, 3)) || (e = rows(h + 3 * stride, pb.v.ptr, 3)) ||
+            (e = rows(h + 6 * stride, pb.C.ptr, 9)) || (e = rows(h + 15 * stride, pb.F.ptr, 9)) ||
+            (e = rows(h + 24 * stride, pb.pl.ptr, 3)) ||
+            (e = cudaMemcpyAsync(reinterpret_cast<uint32_t *>(h + 27 * stride), pb.widx.ptr + off, m * 4,
+                                 cudaMemcpyDeviceToHost, stream)))
+            return cuda_fail(e, "scene readback");
+        return TMPM_OK;
+    }
+
+    TmpmStatus wait_done() {
+        cudaError_t e = cudaEventRecord(done, stream);
+        if (e) return cuda_fail(e, "cudaEventRecord");
+        auto t0 = std::chrono::steady_clock::now();
+        double limit = kSyncTimeoutSeconds;
+        if (const char *env = std::getenv("TMPM_SYNC_TIMEOUT_S")) limit = std::max(0.1, std::atof(env));
+        for (;;) {
+            e = cudaEventQuery(done);
+            if (e == cudaSuccess) return TMPM_OK;
+            if (e != cudaErrorNotReady) return cuda_fail(e, "device work failed");
+            double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+            if (el > limit) {
+                valid = false;
+                return fail(TMPM_ERR_READBACK, "timed out waiting for the batch");
+            }
+            std::this_thread::sleep_for(std::chrono::microseconds(el < 0.01 ? 20 : 200));
+        }
+    }
+
+    TmpmStatus synchronize() {
+        if (!valid) return fail(TMPM_ERR_RESIDENT_UNAVAILABLE, "batch is invalid after an earlier error");
+        if (!pending) return TMPM_OK;
+        pending = false;
+        TmpmStatus st = wait_done();
+        if (st != TMPM_OK) return st;
+        in_flight_uploads.clear();
+        in_flight_results.clear();
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, t_begin, t_end);
+        last_ms = ms;
+        std::vector<uint32_t> flags(kMaxScenes + 1, 0);
+        cudaError_t e;
+        if ((e = cudaMemcpy(flags.data(), status.ptr, sizeof(uint32_t), cudaMemcpyDeviceToHost)) ||
+            (e = cudaMemcpy(flags.data() + 1, scene_status.ptr, sizeof(uint32_t) * kMaxScenes, cudaMemcpyDeviceToHost)))
+            return cuda_fail(e, "status readback");
+        if (flags[0] & kStatusCapacity) {
+            valid = false;
+            return fail(TMPM_ERR_CAPACITY, "GPU MPM batch exceeds the device capacity (grid block pool or hash table)");
+        }
+        if (flags[0] & kStatusTimeout) {
+            valid = false;
+            return fail(TMPM_ERR_READBACK, "a bounded device wait gave up");
+        }
+        for (size_t id = 0; id < scenes.size(); ++id) {
+            BatchScene &s = scenes[id];
+            if (!s.live || s.queued == 0) continue;
+            if (flags[1 + id] & kStatusResident) {
+                if (s.status == TMPM_OK) {
+                    s.status = TMPM_ERR_RESIDENT_UNAVAILABLE;
+                    s.error = "GPU MPM resident substeps require a CPU fallback; scene state is the last one read";
+                }
+                s.result.release();
+            } else if (s.status == TMPM_OK) {
+                s.substeps += s.queued;
+                s.stale = true;
+                if (s.collect) s.collected = true;
+            }
+            s.queued = 0;
+            s.collect = false;
+        }
+        return TMPM_OK;
+    }
+
+    // Apply rows (27 f32 rows + widx, stride m) to a scene's host world
+    // (collect_prepared + apply_gpu_transfers, gpu.rs:1821-1989, 2295-2329).
+    TmpmStatus apply_rows(BatchScene &s, PinnedLease &src) {
+        const size_t m = s.dev_count, stride = std::max<size_t>(m, 1);
+        const float *h = row_base(src);
+        const uint32_t *widx = reinterpret_cast<const uint32_t *>(h + 27 * stride);
+        std::atomic<bool> bad{false};
+        parallel_for(m, [&](size_t a, size_t b) {
+            for (size_t c = 0; c < 27 && !bad.load(std::memory_order_relaxed); ++c)
+                for (size_t j = a; j < b; ++j)
+                    if (!std::isfinite(h[c * stride + j])) {
+                        bad = true;
+                        break;
+                    }
+        });
+        if (bad) {
+            s.status = TMPM_ERR_NON_FINITE_STATE;
+            s.error = "MPM integration produced a non-finite state";
+            return s.status;
+        }
+        HostWorld &w = s.world;
+        parallel_for(m, [&](size_t a, size_t b) {
+            for (size_t j = a; j < b; ++j) {
+                size_t i = widx[j];
+                if (w.fixed[i]) {
+                    for (int k = 0; k < 3; ++k) w.vel[3 * i + k] = 0.0;
+                    for (int k = 0; k < 9; ++k) w.C[9 * i + k] = 0.0;
+                    continue;
+                }
+                for (int k = 0; k < 3; ++k) {
+                    w.pos[3 * i + k] = h[(0 + k) * stride + j];
+                    w.vel[3 * i + k] = h[(3 + k) * stride + j];
+                }
+                for (int k = 0; k < 9; ++k) {
+                    w.C[9 * i + k] = h[(6 + k) * stride + j];
+                    w.F[9 * i + k] = h[(15 + k) * stride + j];
+                }
+                const int mat = w.material[i];
+                if (mat == TMPM_MAT_SAND || mat == TMPM_MAT_SNOW || mat == TMPM_MAT_SAND_NEO_HOOKEAN)
+                    for (int k = 0; k < 3; ++k) w.plastic[3 * i + k] = h[(24 + k) * stride + j];
+            }
+        });
+        return TMPM_OK;
+    }
+
+    // Bring a scene's host world up to date: from collected rows (no device
+    // work), else from the device (idle only).
+    TmpmStatus refresh(BatchScene &s) {
+        if (s.collected) {
+            TmpmStatus st = apply_rows(s, s.result);
+            s.result.release();
+            s.collected = false;
+            s.stale = false;
+            return st;
+        }
+        if (!s.stale) return TMPM_OK;
+        if (pending) return fail(TMPM_ERR_PENDING_STEPS, "a batch is in flight; synchronize first");
+        if (!staging_lease.ensure(28 * std::max<size_t>(s.dev_count, 1) * sizeof(float)))
+            return fail(TMPM_ERR_DEVICE, "cudaMallocHost staging failed");
+        TmpmStatus st = queue_readback(s, staging_lease);
+        if (st != TMPM_OK) return st;
+        cudaError_t e = cudaStreamSynchronize(stream);
+        if (e) return cuda_fail(e, "scene readback");
+        st = apply_rows(s, staging_lease);
+        s.stale = false;
+        return st;
+    }
+    PinnedLease staging_lease;
+
+    int free_id() const {
+        for (size_t id = 0; id < scenes.size(); ++id)
+            if (!scenes[id].live && !scenes[id].draining) return static_cast<int>(id);
+        return scenes.size() < static_cast<size_t>(kMaxScenes) ? static_cast<int>(scenes.size()) : -1;
+    }
+
+    // Attach a prepared scene (allowed while a batch is in flight: host work only).
+    TmpmStatus admit(std::unique_ptr<TmpmPreparedScene> p, uint32_t *id_out) {
+        int id = free_id();
+        if (id < 0 && !pending && n_phys != n_live) {
+            TmpmStatus st = compact();
+            if (st != TMPM_OK) return st;
+            id = free_id();
+        }
+        if (id < 0) return fail(TMPM_ERR_CAPACITY, "a batch holds at most 256 live scenes");
+        if (n_live + p->m > static_cast<size_t>(std::numeric_limits<int>::max() / 2))
+            return fail(TMPM_ERR_CAPACITY, "too many particles for one batch");
+        // classes into the batch table, in this scene's grid namespace
+        std::vector<uint32_t> remap(p->classes.table.size());
+        const size_t before = classes.table.size();
+        for (size_t k = 0; k < remap.size(); ++k) {
+            DevClass c = p->classes.table[k];
+            c.color |= static_cast<uint32_t>(id) << kSceneShift;
+            remap[k] = classes.intern(c);
+        }
+        if (classes.table.size() > kClassMask) {
+            classes.table.resize(before);  // (index entries past `before` are harmless: re-interned on use)
+            return fail(TMPM_ERR_CAPACITY, "too many distinct particle classes");
+        }
+        const size_t stride = std::max<size_t>(p->m, 1);
+        uint32_t *cls = row_cls(p->rows, stride);
+        parallel_for(p->m, [&](size_t a, size_t b) {
+            for (size_t j = a; j < b; ++j) cls[j] = remap[cls[j] & kClassMask] | (cls[j] & kFixedBit);
+        });
+        BatchScene sc;
+        sc.live = true;
+        sc.params = p->params;
+        sc.dt = p->dt;
+        sc.dev_count = p->m;
+        sc.blocks = p->blocks;
+        sc.world = std::move(p->world);
+        sc.staged = std::move(p);
+        if (static_cast<size_t>(id) == scenes.size()) scenes.emplace_back();
+        scenes[id] = std::move(sc);
+        n_live += scenes[id].dev_count;
+        if (id_out) *id_out = static_cast<uint32_t>(id);
+        return TMPM_OK;
+    }
+
+    TmpmStatus remove(uint32_t id) {
+        BatchScene *s = scene_at(id);
+        if (!s) return fail(TMPM_ERR_INVALID_INPUT, "unknown scene id");
+        n_live -= s->dev_count;
+        if (pending && s->queued) {
+            // the batch in flight may still write this scene's collected rows
+            in_flight_results.push_back(std::make_unique<PinnedLease>(std::move(s->result)));
+        }
+        const bool had_rows = !s->staged;
+        scenes[id] = BatchScene();
+        scenes[id].draining = had_rows;  // rows on the device go at the next re-sort
+        return TMPM_OK;
+    }
+
+    // Drop the rows of removed scenes now (a re-sort without substeps).  Idle only.
+    TmpmStatus compact() {
+        for (BatchScene &s : scenes) s.queued = 0;
+        cudaError_t e;
+        if ((e = upload_table())) return cuda_fail(e, "scene table upload");
+        if (n_phys) {
+            SimParams sp = sim_params();
+            ParticleSoA src = pbuf[cur].view(nullptr, 1), dst = pbuf[cur ^ 1].view(nullptr, 1);
+            SortBuffers sb = sort_buffers();
+            launch_resort(src, dst, static_cast<int>(n_phys), static_cast<int>(n_live_committed()), dclasses.ptr, sp, sb,
+                          stream);
+            cur ^= 1;
+        }
+        // rows of live committed scenes now lead, in id order; staged scenes follow at commit
+        size_t off = 0;
+        for (BatchScene &s : scenes) {
+            if (s.draining) s.draining = false;
+            if (!s.live || s.staged) continue;
+            s.dev_offset = off;
+            off += s.dev_count;
+        }
+        n_phys = off;
+        if ((e = cudaStreamSynchronize(stream))) return cuda_fail(e, "compact");
+        return TMPM_OK;
+    }
+
+    size_t n_live_committed() const {
+        size_t n = 0;
+        for (const BatchScene &s : scenes)
+            if (s.live && !s.staged) n += s.dev_count;
+        return n;
+    }
+
+    size_t device_bytes() const {
+        size_t b = 0;
+        for (int k = 0; k < 2; ++k) b += pbuf[k].cap * (27 * 4 + 2 * 4);
+        b += (sort_keys[0].count + sort_keys[1].count + sort_vals[0].count + sort_vals[1].count + sort_hist.count) * 4;
+        for (int g = 0; g < 2; ++g)
+            b += static_cast<size_t>(grids[g].max_blocks) * (kNodesPerBlock * 16 + 16) +
+                 static_cast<size_t>(grids[g].capacity) * 12;
+        b += cta_cache.count * 4 + dclasses.count * sizeof(DevClass) + kMaxScenes * (sizeof(SceneParams) + 4);
+        return b;
+    }
+};
+
+extern "C" {
+
+TmpmStatus tmpm_scene_prepare(const TmpmParams *params, const TmpmParticleArrays *particles, double substep_dt,
+                              TmpmPreparedScene **out) {
+    if (!out || !params) {
+        g_last_error = "null argument";
+        return TMPM_ERR_INVALID_INPUT;
+    }
+    *out = nullptr;
+    auto p = std::make_unique<TmpmPreparedScene>();
+    TmpmStatus st = prepare_scene(*params, particles, substep_dt, *p);
+    if (st != TMPM_OK) return st;
+    *out = p.release();
+    return TMPM_OK;
+}
+
+void tmpm_scene_prepared_destroy(TmpmPreparedScene *p) { delete p; }
+
+size_t tmpm_scene_prepared_particle_count(const TmpmPreparedScene *p) { return p ? p->world.n : 0; }
+
+size_t tmpm_scene_prepared_bytes(const TmpmPreparedScene *p) {
+    return p ? p->m * kBytesPerRow + 16 * p->blocks * kBytesPerPoolBlock : 0;
+}
+
+TmpmStatus tmpm_batch_create(const TmpmBatchOptions *options, TmpmBatch **out) {
+    if (!out) {
+        g_last_error = "null argument";
+        return TMPM_ERR_INVALID_INPUT;
+    }
+    *out = nullptr;
+    auto b = std::make_unique<TmpmBatch>();
+    if (options) b->options = *options;
+    else b->options.use_graphs = 1;
+    b->device = b->options.device;
+    cudaError_t e;
+    if ((e = cudaSetDevice(b->device)) || (e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking)) ||
+        (e = cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming)) || (e = cudaEventCreate(&b->t_begin)) ||
+        (e = cudaEventCreate(&b->t_end)) || (e = b->status.alloc(1)) || (e = b->scene_status.alloc(kMaxScenes)) ||
+        (e = b->dscenes.alloc(kMaxScenes))) {
+        g_last_error = std::string("batch setup: ") + cudaGetErrorString(e);
+        return TMPM_ERR_DEVICE;
+    }
+    if (!b->table_staging.ensure(sizeof(SceneParams) * kMaxScenes)) {
+        g_last_error = "cudaMallocHost scene table failed";
+        return TMPM_ERR_DEVICE;
+    }
+    cudaMemsetAsync(b->status.ptr, 0, sizeof(uint32_t), b->stream);
+    cudaMemsetAsync(b->scene_status.ptr, 0, sizeof(uint32_t) * kMaxScenes, b->stream);
+    if (b->options.particle_capacity) {
+        TmpmStatus st = b->ensure_rows(b->options.particle_capacity);
+        if (st != TMPM_OK) return st;
+    }
+    if (b->options.max_blocks) {
+        TmpmStatus st = b->ensure_grid();
+        if (st != TMPM_OK) return st;
+    }
+    if ((e = cudaStreamSynchronize(b->stream))) {
+        g_last_error = std::string("batch setup: ") + cudaGetErrorString(e);
+        return TMPM_ERR_DEVICE;
+    }
+    *out = b.release();
+    return TMPM_OK;
+}
+
+void tmpm_batch_destroy(TmpmBatch *batch) { delete batch; }
+
+TmpmStatus tmpm_batch_admit(TmpmBatch *b, TmpmPreparedScene *prepared, uint32_t *scene_out) {
+    if (!b || !prepared) {
+        g_last_error = "null argument";
+        if (prepared) delete prepared;
+        return TMPM_ERR_INVALID_INPUT;
+    }
+    std::unique_ptr<TmpmPreparedScene> p(prepared);
+    TmpmStatus st = b->guard(false);
+    if (st != TMPM_OK) return st;
+    return b->admit(std::move(p), scene_out);
+}
+
+TmpmStatus tmpm_batch_add_scene(TmpmBatch *b, const TmpmParams *params, const TmpmParticleArrays *particles,
+                                double substep_dt, uint32_t *scene_out) {
+    if (!b || !params) {
+        g_last_error = "null argument";
+        return TMPM_ERR_INVALID_INPUT;
+    }
+    TmpmStatus st = b->guard(false);
+    if (st != TMPM_OK) return st;
+    auto p = std::make_unique<TmpmPreparedScene>();
+    st = prepare_scene(*params, particles, substep_dt, *p);
+    if (st != TMPM_OK) return b->fail(st, g_last_error);
+    cudaSetDevice(b->device);
+    return b->admit(std::move(p), scene_out);
+}
+
+TmpmStatus tmpm_batch_remove_scene(TmpmBatch *b, uint32_t scene) {
+    if (!b) return TMPM_ERR_INVALID_INPUT;
+    TmpmStatus st = b->guard(false);
+    if (st != TMPM_OK) return st;
+    return b->remove(scene);
+}
+
+TmpmStatus tmpm_batch_submit(TmpmBatch *b, const uint32_t *ids, const uint32_t *steps, const uint8_t *collect,
+                             size_t count) {
+    if (!b) return TMPM_ERR_INVALID_INPUT;
+    TmpmStatus st = b->guard(true);
+    if (st != TMPM_OK) return st;
+    if (count && (!ids || !steps)) return b->fail(TMPM_ERR_INVALID_INPUT, "null scene or step array");
+    for (BatchScene &s : b->scenes) {
+        s.queued = 0;
+        s.collect = false;
+    }
+    uint32_t S = 0;
+    for (size_t k = 0; k < count; ++k) {
+        BatchScene *s = b->scene_at(ids[k]);
+        if (!s) return b->fail(TMPM_ERR_INVALID_INPUT, "unknown scene id");
+        if (s->status != TMPM_OK) return b->fail(s->status, "scene failed earlier: " + s->error);
+        if (steps[k] == 0 || steps[k] > 4096) return b->fail(TMPM_ERR_INVALID_INPUT, "substeps per scene must be 1..4096");
+        if (s->queued) return b->fail(TMPM_ERR_INVALID_INPUT, "scene listed twice");
+        if (s->collected && s->stale) {
+            // rows collected earlier are superseded by this batch: apply them first
+            st = b->refresh(*s);
+            if (st != TMPM_OK) return b->fail(st, s->error);
+        }
+        s->queued = steps[k];
+        s->collect = collect && collect[k];
+        S = std::max(S, steps[k]);
+    }
+    if (S == 0) return TMPM_OK;
+    cudaSetDevice(b->device);
+    st = b->enqueue(S);
+    if (st != TMPM_OK) return st;
+    b->pending = true;
+    return TMPM_OK;
+}
+
+TmpmStatus tmpm_batch_synchronize(TmpmBatch *b) {
+    if (!b) return TMPM_ERR_INVALID_INPUT;
+    cudaSetDevice(b->device);
+    return b->synchronize();
+}
+
+int32_t tmpm_batch_pending(const TmpmBatch *b) { return b && b->pending ? 1 : 0; }
+
+TmpmStatus tmpm_batch_scene_status(const TmpmBatch *b, uint32_t scene) {
+    if (!b || scene >= b->scenes.size() || !b->scenes[scene].live) return TMPM_ERR_INVALID_INPUT;
+    return b->scenes[scene].status;
+}
+
+uint64_t tmpm_batch_scene_substeps(const TmpmBatch *b, uint32_t scene) {
+    if (!b || scene >= b->scenes.size() || !b->scenes[scene].live) return 0;
+    return b->scenes[scene].substeps;
+}
+
+size_t tmpm_batch_scene_particle_count(const TmpmBatch *b, uint32_t scene) {
+    if (!b || scene >= b->scenes.size() || !b->scenes[scene].live) return 0;
+    return b->scenes[scene].world.n;
+}
+
+TmpmStatus tmpm_batch_read_scene(TmpmBatch *b, uint32_t scene, TmpmParticleArrays *out) {
+    if (!b || !out) return TMPM_ERR_INVALID_INPUT;
+    TmpmStatus st = b->guard(false);
+    if (st != TMPM_OK) return st;
+    BatchScene *s = b->scene_at(scene);
+    if (!s) return b->fail(TMPM_ERR_INVALID_INPUT, "unknown scene id");
+    if (s->status != TMPM_OK) return b->fail(s->status, s->error);
+    if (b->pending && s->queued) return b->fail(TMPM_ERR_PENDING_STEPS, "the scene is in the batch in flight");
+    if (out->count != s->world.n) return b->fail(TMPM_ERR_INVALID_INPUT, "output array count does not match the scene");
+    cudaSetDevice(b->device);
+    st = b->refresh(*s);
+    if (st != TMPM_OK) return b->fail(st, s->error.empty() ? b->last_error : s->error);
+    s->world.store(*out);
+    return TMPM_OK;
+}
+
+double tmpm_batch_last_ms(const TmpmBatch *b) { return b ? b->last_ms : 0.0; }
+
+size_t tmpm_batch_device_bytes(const TmpmBatch *b) { return b ? b->device_bytes() : 0; }
+
+size_t tmpm_batch_scene_bytes(size_t particles, size_t home_blocks) {
+    return particles * kBytesPerRow + 16 * home_blocks * kBytesPerPoolBlock;
+}
+
+const char *tmpm_batch_last_error_message(const TmpmBatch *b) { return b ? b->last_error.c_str() : g_last_error.c_str(); }
+
+}  // extern "C"

@@ -542,9 +542,18 @@ __device__ __forceinline__ unsigned long long block_key(int bx, int by, int bz, 
            static_cast<unsigned long long>(static_cast<uint32_t>(bz + kBlockBias) & 0xFFFFu);
 }
 
+// Slot of a block key: a full 64-bit avalanche (the fmix64 finalizer of
+// MurmurHash3, public domain), so the namespace bits (scene, colour) in the top
+// 16 bits of the key spread over every slot bit.  A multiply alone would leave
+// the low slot bits independent of the high key bits, and scenes or colours
+// with the same block coordinates would pile onto the same probe chain.
 __device__ __forceinline__ uint32_t hash_slot(unsigned long long key, uint32_t mask) {
-    unsigned long long h = key * 0x9E3779B97F4A7C15ull;
-    h ^= h >> 29;
+    unsigned long long h = key;
+    h ^= h >> 33;
+    h *= 0xff51afd7ed558ccdull;
+    h ^= h >> 33;
+    h *= 0xc4ceb9fe1a85ec53ull;
+    h ^= h >> 33;
     return static_cast<uint32_t>(h) & mask;
 }
 
@@ -557,10 +566,12 @@ __device__ __forceinline__ uint32_t spread10(uint32_t v) {
     return v;
 }
 
-// 30-bit Morton key of a block (coordinates taken modulo 1024).
-__device__ __forceinline__ uint32_t morton_block(int bx, int by, int bz) {
-    return (spread10(static_cast<uint32_t>(bx)) << 2) | (spread10(static_cast<uint32_t>(by)) << 1) |
-           spread10(static_cast<uint32_t>(bz));
+// Sort key of a block: scene index (8 bits) above the 21-bit Morton code of the
+// block coordinates taken modulo 128 (512 cells per axis); bit 29 marks
+// particles of removed scenes (kDeadKey).
+__device__ __forceinline__ uint32_t morton_block(int bx, int by, int bz, uint32_t scene) {
+    return ((scene & 0xFFu) << 21) | (spread10(static_cast<uint32_t>(bx) & 0x7Fu) << 2) |
+           (spread10(static_cast<uint32_t>(by) & 0x7Fu) << 1) | spread10(static_cast<uint32_t>(bz) & 0x7Fu);
 }
 
 // Find the block id of `key`, allocating (and zero-filling) the block if absent.

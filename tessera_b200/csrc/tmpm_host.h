@@ -1,0 +1,827 @@
+// tmpm_host.h -- host-side pieces shared by the single-scene session
+// (tmpm_session.cu) and the multi-scene batch (tmpm_batch.cu): the f64 host
+// world, validation that mirrors the reference's MpmWorld checks, device and
+// pinned buffers, and the f32 packing of a world for upload.
+#pragma once
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstring>
+#include <limits>
+#include <string>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include "../../include/tmpm.h"
+#include "tmpm_internal.h"
+
+namespace tmpm {
+
+inline thread_local std::string g_last_error;  // reason reported by tmpm_last_error()
+
+inline constexpr double kSyncTimeoutSeconds = 5.0;  // gpu.rs:1853-1862
+
+inline unsigned host_threads() { return std::max(1u, std::min(32u, std::thread::hardware_concurrency())); }
+
+// Run fn(chunk, begin, end) over [0, n) split into contiguous chunks, one per host thread.
+template <typename Fn>
+inline void parallel_chunks(size_t n, Fn fn, size_t min_per_chunk = 32768) {
+    size_t chunks = std::min<size_t>(host_threads(), std::max<size_t>(1, n / min_per_chunk));
+    if (chunks <= 1) {
+        fn(size_t(0), size_t(0), n);
+        return;
+    }
+    size_t per = (n + chunks - 1) / chunks;
+    std::vector<std::thread> pool;
+    for (size_t c = 0; c < chunks; ++c) {
+        size_t a = c * per, b = std::min(n, a + per);
+        if (a >= b) break;
+        pool.emplace_back([=]() { fn(c, a, b); });
+    }
+    for (auto &t : pool) t.join();
+}
+
+template <typename Fn>
+inline void parallel_for(size_t n, Fn fn) {
+    parallel_chunks(n, [&](size_t, size_t a, size_t b) { fn(a, b); });
+}
+
+// --------------------------------------------------------------- host world
+
+struct HostWorld {
+    size_t n = 0;
+    std::vector<double> pos, vel, F, C, force, mass, vol, radius, damping, plastic, mparams;
+    std::vector<int32_t> material;
+    std::vector<uint8_t> enabled, fixed;
+    std::vector<uint16_t> color;
+    std::vector<uint32_t> group;
+    std::vector<uint64_t> chunk;
+
+    // Sizes every field for `count` particles; existing storage is reused and
+    // not cleared (load() writes every element).
+    void resize(size_t count) {
+        n = count;
+        pos.resize(3 * n);
+        vel.resize(3 * n);
+        F.resize(9 * n);
+        C.resize(9 * n);
+        force.resize(3 * n);
+        mass.resize(n);
+        vol.resize(n);
+        radius.resize(n);
+        damping.resize(n);
+        plastic.resize(3 * n);
+        mparams.resize(5 * n);
+        material.resize(n);
+        enabled.resize(n);
+        fixed.resize(n);
+        color.resize(n);
+        group.resize(n);
+        chunk.resize(n);
+    }
+
+    void load(const TmpmParticleArrays &a) {
+        resize(a.count);
+        parallel_for(n, [&](size_t lo, size_t hi) { load_range(a, lo, hi); });
+    }
+
+    void load_range(const TmpmParticleArrays &a, size_t lo, size_t hi) {
+        for (size_t i = lo; i < hi; ++i) {
+            for (int k = 0; k < 3; ++k) {
+                pos[3 * i + k] = a.position[3 * i + k];
+                vel[3 * i + k] = a.velocity[3 * i + k];
+                force[3 * i + k] = a.force ? a.force[3 * i + k] : 0.0;
+            }
+            for (int k = 0; k < 9; ++k) {
+                F[9 * i + k] = a.deformation ? a.deformation[9 * i + k] : ((k % 4 == 0) ? 1.0 : 0.0);
+                C[9 * i + k] = a.affine ? a.affine[9 * i + k] : 0.0;
+            }
+            mass[i] = a.mass[i];
+            vol[i] = a.rest_volume[i];
+            radius[i] = a.radius[i];
+            damping[i] = a.damping ? a.damping[i] : 0.0;
+            material[i] = a.material[i];
+            for (int k = 0; k < 5; ++k) mparams[5 * i + k] = a.material_params[5 * i + k];
+            if (a.plastic) {
+                for (int k = 0; k < 3; ++k) plastic[3 * i + k] = a.plastic[3 * i + k];
+            } else {
+                plastic[3 * i] = 1.0;
+                plastic[3 * i + 1] = (material[i] == TMPM_MAT_SAND || material[i] == TMPM_MAT_SAND_NEO_HOOKEAN) ? 1.0 : 0.0;
+                plastic[3 * i + 2] = 0.0;
+            }
+            enabled[i] = a.enabled ? (a.enabled[i] != 0) : 1;
+            fixed[i] = a.fixed ? (a.fixed[i] != 0) : 0;
+            color[i] = a.transfer_color ? a.transfer_color[i] : 0;
+            group[i] = a.group_id ? a.group_id[i] : 0;
+            chunk[i] = a.chunk_id ? a.chunk_id[i] : 0;
+        }
+    }
+
+    void store(TmpmParticleArrays &a) const {
+        parallel_for(n, [&](size_t lo, size_t hi) { store_range(a, lo, hi); });
+    }
+
+    void store_range(TmpmParticleArrays &a, size_t lo, size_t hi) const {
+        for (size_t i = lo; i < hi; ++i) {
+            for (int k = 0; k < 3; ++k) {
+                if (a.position) a.position[3 * i + k] = pos[3 * i + k];
+                if (a.velocity) a.velocity[3 * i + k] = vel[3 * i + k];
+                if (a.force) a.force[3 * i + k] = force[3 * i + k];
+                if (a.plastic) a.plastic[3 * i + k] = plastic[3 * i + k];
+            }
+            for (int k = 0; k < 9; ++k) {
+                if (a.deformation) a.deformation[9 * i + k] = F[9 * i + k];
+                if (a.affine) a.affine[9 * i + k] = C[9 * i + k];
+            }
+            if (a.mass) a.mass[i] = mass[i];
+            if (a.rest_volume) a.rest_volume[i] = vol[i];
+            if (a.radius) a.radius[i] = radius[i];
+            if (a.damping) a.damping[i] = damping[i];
+            if (a.material) a.material[i] = material[i];
+            if (a.material_params)
+                for (int k = 0; k < 5; ++k) a.material_params[5 * i + k] = mparams[5 * i + k];
+            if (a.enabled) a.enabled[i] = enabled[i];
+            if (a.fixed) a.fixed[i] = fixed[i];
+            if (a.transfer_color) a.transfer_color[i] = color[i];
+            if (a.group_id) a.group_id[i] = group[i];
+            if (a.chunk_id) a.chunk_id[i] = chunk[i];
+        }
+    }
+
+    void append(const HostWorld &o) {
+        auto cat = [](auto &dst, const auto &src) { dst.insert(dst.end(), src.begin(), src.end()); };
+        cat(pos, o.pos);
+        cat(vel, o.vel);
+        cat(F, o.F);
+        cat(C, o.C);
+        cat(force, o.force);
+        cat(mass, o.mass);
+        cat(vol, o.vol);
+        cat(radius, o.radius);
+        cat(damping, o.damping);
+        cat(plastic, o.plastic);
+        cat(mparams, o.mparams);
+        cat(material, o.material);
+        cat(enabled, o.enabled);
+        cat(fixed, o.fixed);
+        cat(color, o.color);
+        cat(group, o.group);
+        cat(chunk, o.chunk);
+        n += o.n;
+    }
+
+    // Keep particles whose chunk differs (world.rs:267-277).
+    size_t remove_chunk(uint64_t c) {
+        size_t w = 0;
+        for (size_t i = 0; i < n; ++i) {
+            if (chunk[i] == c) continue;
+            if (w != i) {
+                for (int k = 0; k < 3; ++k) {
+                    pos[3 * w + k] = pos[3 * i + k];
+                    vel[3 * w + k] = vel[3 * i + k];
+                    force[3 * w + k] = force[3 * i + k];
+                    plastic[3 * w + k] = plastic[3 * i + k];
+                }
+                for (int k = 0; k < 9; ++k) {
+                    F[9 * w + k] = F[9 * i + k];
+                    C[9 * w + k] = C[9 * i + k];
+                }
+                for (int k = 0; k < 5; ++k) mparams[5 * w + k] = mparams[5 * i + k];
+                mass[w] = mass[i];
+                vol[w] = vol[i];
+                radius[w] = radius[i];
+                damping[w] = damping[i];
+                material[w] = material[i];
+                enabled[w] = enabled[i];
+                fixed[w] = fixed[i];
+                color[w] = color[i];
+                group[w] = group[i];
+                chunk[w] = chunk[i];
+            }
+            ++w;
+        }
+        size_t removed = n - w;
+        n = w;
+        pos.resize(3 * n);
+        vel.resize(3 * n);
+        force.resize(3 * n);
+        plastic.resize(3 * n);
+        F.resize(9 * n);
+        C.resize(9 * n);
+        mparams.resize(5 * n);
+        mass.resize(n);
+        vol.resize(n);
+        radius.resize(n);
+        damping.resize(n);
+        material.resize(n);
+        enabled.resize(n);
+        fixed.resize(n);
+        color.resize(n);
+        group.resize(n);
+        chunk.resize(n);
+        return removed;
+    }
+};
+
+// ------------------------------------------------------------- host math
+
+inline double det9(const double *m) {  // column-major
+    return m[0] * (m[4] * m[8] - m[7] * m[5]) - m[3] * (m[1] * m[8] - m[7] * m[2]) + m[6] * (m[1] * m[5] - m[4] * m[2]);
+}
+inline double fro9(const double *m) {
+    double s = 0;
+    for (int k = 0; k < 9; ++k) s += m[k] * m[k];
+    return std::sqrt(s);
+}
+inline bool inverse_norm9(const double *m, double &out) {
+    double d = det9(m);
+    if (d == 0.0 || !std::isfinite(d)) return false;
+    // cofactors: the inverse's Frobenius norm equals that of the cofactor matrix / |det|
+    const double *a = m, *b = m + 3, *c = m + 6;
+    double bc[3] = {b[1] * c[2] - b[2] * c[1], b[2] * c[0] - b[0] * c[2], b[0] * c[1] - b[1] * c[0]};
+    double ca[3] = {c[1] * a[2] - c[2] * a[1], c[2] * a[0] - c[0] * a[2], c[0] * a[1] - c[1] * a[0]};
+    double ab[3] = {a[1] * b[2] - a[2] * b[1], a[2] * b[0] - a[0] * b[2], a[0] * b[1] - a[1] * b[0]};
+    double s = 0;
+    for (int k = 0; k < 3; ++k) s += bc[k] * bc[k] + ca[k] * ca[k] + ab[k] * ab[k];
+    out = std::sqrt(s) / std::fabs(d);
+    return std::isfinite(out);
+}
+
+inline void lame(double young, double poisson, double &lambda, double &mu) {  // material.rs:433-438
+    lambda = young * poisson / ((1.0 + poisson) * (1.0 - 2.0 * poisson));
+    mu = young / (2.0 * (1.0 + poisson));
+}
+
+inline bool valid_elasticity(double young, double poisson) {  // material.rs:429-431
+    return std::isfinite(young) && young > 0.0 && std::isfinite(poisson) && poisson >= -1.0 && poisson < 0.5;
+}
+
+inline bool material_valid(int kind, const double *p) {  // material.rs:171-231
+    switch (kind) {
+    case TMPM_MAT_ELASTIC:
+    case TMPM_MAT_NEO_HOOKEAN:
+        return valid_elasticity(p[0], p[1]);
+    case TMPM_MAT_SAND:
+    case TMPM_MAT_SAND_NEO_HOOKEAN:
+        return valid_elasticity(p[0], p[1]) && std::isfinite(p[2]) && p[2] >= 0.0 && p[2] < M_PI / 2.0 &&
+               std::isfinite(p[3]) && p[3] >= 0.0;
+    case TMPM_MAT_FLUID:
+        return std::isfinite(p[0]) && p[0] > 0.0 && std::isfinite(p[1]) && p[1] > 0.0 && std::isfinite(p[2]) &&
+               p[2] >= 0.0 && std::isfinite(p[3]) && p[3] >= 0.0;
+    case TMPM_MAT_SNOW:
+        return valid_elasticity(p[0], p[1]) && std::isfinite(p[2]) && p[2] >= 0.0 && p[2] < 1.0 &&
+               std::isfinite(p[3]) && p[3] >= 0.0 && std::isfinite(p[4]) && p[4] >= 0.0;
+    default:
+        return false;
+    }
+}
+
+// MaterialModel::timestep_bound_with_deformation (material.rs:378-426)
+inline double timestep_bound(int kind, const double *p, double density, const double *v, double h, double det_f) {
+    double speed = std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+    double lambda, mu, wave;
+    if (kind == TMPM_MAT_SAND_NEO_HOOKEAN) {
+        lame(p[0], p[1], lambda, mu);
+        double rho = density / std::max(det_f, 1e-6);
+        double ws = std::sqrt((lambda + 2.0 * mu) / rho);
+        return 0.5 * h / std::max(ws, speed);
+    }
+    if (kind == TMPM_MAT_FLUID) {
+        wave = std::sqrt(p[0] * p[1] / std::max(density, 1e-12));
+    } else {
+        lame(p[0], p[1], lambda, mu);
+        wave = std::sqrt((lambda + 2.0 * mu) / std::max(density, 1e-12));
+    }
+    return 0.4 * h / std::max(wave + speed, 1e-12);
+}
+
+inline bool finite_particle(const HostWorld &w, size_t i) {  // world.rs:505-515
+    for (int k = 0; k < 3; ++k)
+        if (!std::isfinite(w.pos[3 * i + k]) || !std::isfinite(w.vel[3 * i + k]) || !std::isfinite(w.force[3 * i + k]))
+            return false;
+    for (int k = 0; k < 9; ++k)
+        if (!std::isfinite(w.F[9 * i + k]) || !std::isfinite(w.C[9 * i + k])) return false;
+    return std::isfinite(w.mass[i]) && std::isfinite(w.vol[i]) && std::isfinite(w.radius[i]) &&
+           std::isfinite(w.damping[i]);
+}
+
+inline bool valid_particle(const HostWorld &w, size_t i) {  // world.rs:492-503
+    const double *pl = &w.plastic[3 * i];
+    return finite_particle(w, i) && w.mass[i] > 0.0 && w.vol[i] > 0.0 && w.radius[i] > 0.0 &&
+           material_valid(w.material[i], &w.mparams[5 * i]) && w.damping[i] >= 0.0 && std::isfinite(pl[0]) &&
+           pl[0] > 0.0 && std::isfinite(pl[1]) && std::isfinite(pl[2]);
+}
+
+inline bool params_valid(const TmpmParams &p) {  // world.rs:51-65
+    if (!std::isfinite(p.cell_width) || p.cell_width <= 0.0 || !std::isfinite(p.max_substep) || p.max_substep <= 0.0)
+        return false;
+    for (int k = 0; k < 3; ++k)
+        if (!std::isfinite(p.gravity[k])) return false;
+    if (p.has_bounds) {
+        for (int k = 0; k < 3; ++k)
+            if (!std::isfinite(p.bounds_min[k]) || !std::isfinite(p.bounds_max[k]) || !(p.bounds_max[k] - p.bounds_min[k] > 0.0))
+                return false;
+    }
+    return p.wall_mode == 0 || p.wall_mode == 1;
+}
+
+inline double stable_timestep(const HostWorld &w, const TmpmParams &p) {  // world.rs:288-303
+    std::vector<double> part(host_threads() + 1, p.max_substep);
+    parallel_chunks(w.n, [&](size_t c, size_t lo, size_t hi) {
+        double dt = p.max_substep;
+        for (size_t i = lo; i < hi; ++i) {
+            if (!w.enabled[i] || w.fixed[i]) continue;
+            dt = std::min(dt, timestep_bound(w.material[i], &w.mparams[5 * i], w.mass[i] / w.vol[i], &w.vel[3 * i],
+                                             p.cell_width, det9(&w.F[9 * i])));
+        }
+        part[c] = dt;
+    });
+    double dt = p.max_substep;
+    for (double d : part) dt = std::min(dt, d);
+    return std::min(dt, p.max_substep);
+}
+
+// RigidObstacle::is_valid (obstacle.rs:264-341)
+inline bool obstacle_valid(const TmpmObstacle &o) {
+    auto fin = [](double v) { return std::isfinite(v); };
+    const double *d = o.dims;
+    bool shape_ok = false;
+    switch (o.shape) {
+    case TMPM_SHAPE_SPHERE:
+        shape_ok = fin(d[0]) && d[0] > 0.0;
+        break;
+    case TMPM_SHAPE_BOX:
+        shape_ok = fin(d[0]) && d[0] > 0 && fin(d[1]) && d[1] > 0 && fin(d[2]) && d[2] > 0;
+        break;
+    case TMPM_SHAPE_CAPSULE:
+        shape_ok = fin(d[0]) && d[0] >= 0.0 && fin(d[1]) && d[1] >= 0.0 && (d[0] > 0.0 || d[1] > 0.0);
+        break;
+    case TMPM_SHAPE_CYLINDER:
+    case TMPM_SHAPE_CONE:
+    case TMPM_SHAPE_GROUND:
+        shape_ok = fin(d[0]) && d[0] > 0.0 && fin(d[1]) && d[1] > 0.0;
+        break;
+    case TMPM_SHAPE_TRIANGLE_PRISM: {
+        const double *v = o.vertices;
+        double e1[3] = {v[3] - v[0], v[4] - v[1], v[5] - v[2]}, e2[3] = {v[6] - v[0], v[7] - v[1], v[8] - v[2]};
+        double c[3] = {e1[1] * e2[2] - e1[2] * e2[1], e1[2] * e2[0] - e1[0] * e2[2], e1[0] * e2[1] - e1[1] * e2[0]};
+        double area_sq = c[0] * c[0] + c[1] * c[1] + c[2] * c[2];
+        bool verts_ok = true;
+        for (int k = 0; k < 9; ++k) verts_ok = verts_ok && fin(v[k]);
+        shape_ok = fin(d[0]) && d[0] > 0.0 && verts_ok && fin(area_sq) && area_sq > 1e-24;
+        break;
+    }
+    case TMPM_SHAPE_CONVEX: {
+        shape_ok = o.plane_count >= 4 && o.planes != nullptr && fin(o.bound_radius) && o.bound_radius > 0.0;
+        for (uint32_t i = 0; shape_ok && i < o.plane_count; ++i) {
+            const double *pl = o.planes + 4 * i;
+            bool f = fin(pl[0]) && fin(pl[1]) && fin(pl[2]) && fin(pl[3]);
+            double n2 = std::fma(pl[0], pl[0], std::fma(pl[1], pl[1], pl[2] * pl[2]));
+            shape_ok = f && std::fabs(n2 - 1.0) <= 1e-4;
+        }
+        break;
+    }
+    default:
+        shape_ok = false;
+    }
+    bool cpic_ok = o.cpic_group < 0 || (o.cpic_group < 32 && o.shape == TMPM_SHAPE_TRIANGLE_PRISM);
+    bool rest = o.boundary >= 0 && o.boundary <= 4 && fin(o.friction) && o.friction >= 0.0;
+    for (int k = 0; k < 3; ++k)
+        rest = rest && fin(o.center[k]) && fin(o.linear_velocity[k]) && fin(o.angular_velocity[k]);
+    for (int k = 0; k < 4; ++k) rest = rest && fin(o.orientation[k]);
+    return shape_ok && cpic_ok && rest;
+}
+
+inline bool f32_ok(double v, float &out) {  // finite_f32 (gpu.rs:1992-1999)
+    out = static_cast<float>(v);
+    return std::isfinite(out);
+}
+
+// ------------------------------------------------------------ device memory
+
+template <typename T>
+struct DevBuf {
+    T *ptr = nullptr;
+    size_t count = 0;
+    cudaError_t alloc(size_t n) {
+        release();
+        if (n == 0) n = 1;
+        cudaError_t e = cudaMalloc(reinterpret_cast<void **>(&ptr), n * sizeof(T));
+        if (e == cudaSuccess) count = n;
+        else ptr = nullptr;
+        return e;
+    }
+    void release() {
+        if (ptr) cudaFree(ptr);
+        ptr = nullptr;
+        count = 0;
+    }
+    void swap(DevBuf &o) {
+        std::swap(ptr, o.ptr);
+        std::swap(count, o.count);
+    }
+    ~DevBuf() { release(); }
+    DevBuf() = default;
+    DevBuf(const DevBuf &) = delete;
+    DevBuf &operator=(const DevBuf &) = delete;
+};
+
+struct PinnedBuf {
+    void *ptr = nullptr;
+    size_t bytes = 0;
+    bool ensure(size_t b) {
+        if (b <= bytes) return true;
+        release();
+        if (cudaMallocHost(&ptr, b) != cudaSuccess) {
+            ptr = nullptr;
+            return false;
+        }
+        bytes = b;
+        return true;
+    }
+    void release() {
+        if (ptr) cudaFreeHost(ptr);
+        ptr = nullptr;
+        bytes = 0;
+    }
+    ~PinnedBuf() { release(); }
+};
+
+struct ParticleBuffers {
+    DevBuf<float> x, v, C, F, pl;
+    DevBuf<uint32_t> cls, widx;
+    size_t cap = 0;
+    cudaError_t alloc(size_t c) {
+        cudaError_t e;
+        if ((e = x.alloc(3 * c)) || (e = v.alloc(3 * c)) || (e = C.alloc(9 * c)) || (e = F.alloc(9 * c)) ||
+            (e = pl.alloc(3 * c)) || (e = cls.alloc(c)) || (e = widx.alloc(c)))
+            return e;
+        cap = c;
+        return cudaSuccess;
+    }
+    void swap(ParticleBuffers &o) {
+        x.swap(o.x);
+        v.swap(o.v);
+        C.swap(o.C);
+        F.swap(o.F);
+        pl.swap(o.pl);
+        cls.swap(o.cls);
+        widx.swap(o.widx);
+        std::swap(cap, o.cap);
+    }
+    ParticleSoA view(float *force, size_t force_stride) const {
+        ParticleSoA p;
+        p.x = x.ptr;
+        p.v = v.ptr;
+        p.C = C.ptr;
+        p.F = F.ptr;
+        p.pl = pl.ptr;
+        p.force = force;
+        p.cls = cls.ptr;
+        p.widx = widx.ptr;
+        p.cap = cap;
+        p.force_stride = force_stride;
+        return p;
+    }
+};
+
+struct GridBuffers {
+    DevBuf<unsigned long long> keys;
+    DevBuf<uint32_t> vals, count;
+    DevBuf<float4> pool;
+    DevBuf<int4> coords;
+    uint32_t capacity = 0, max_blocks = 0;
+    cudaError_t alloc(uint32_t blocks) {
+        uint32_t cap = 1024;
+        while (cap < 2u * blocks) cap <<= 1;
+        cudaError_t e;
+        if ((e = keys.alloc(cap)) || (e = vals.alloc(cap)) || (e = count.alloc(1)) ||
+            (e = pool.alloc(static_cast<size_t>(blocks) * kNodesPerBlock)) || (e = coords.alloc(blocks)))
+            return e;
+        capacity = cap;
+        max_blocks = blocks;
+        return cudaSuccess;
+    }
+    GridTable view() const {
+        GridTable g;
+        g.keys = keys.ptr;
+        g.vals = vals.ptr;
+        g.count = count.ptr;
+        g.pool = pool.ptr;
+        g.coords = coords.ptr;
+        g.mask = capacity - 1;
+        g.max_blocks = max_blocks;
+        return g;
+    }
+};
+
+// Device material codes, as the reference packs them (gpu.rs:1171-1276).
+inline int class_kind(int material) {
+    switch (material) {
+    case TMPM_MAT_NEO_HOOKEAN:
+        return kMatNeoHookean;
+    case TMPM_MAT_FLUID:
+        return kMatFluid;
+    case TMPM_MAT_ELASTIC:
+        return kMatCorotated;
+    case TMPM_MAT_SNOW:
+        return kMatSnow;
+    case TMPM_MAT_SAND:
+        return kMatSand;
+    case TMPM_MAT_SAND_NEO_HOOKEAN:
+        return kMatSandNeoHookean;
+    default:
+        return 0;
+    }
+}
+
+
+// Per-scene f32 integration constants (MpmParams + the fixed substep).
+inline SceneParams scene_params(const TmpmParams &params, double dt) {
+    SceneParams sc{};
+    float h = static_cast<float>(params.cell_width);
+    sc.h = h;
+    sc.inv_h = 1.0f / h;
+    sc.inv_d = static_cast<float>(4.0 / (params.cell_width * params.cell_width));
+    sc.dt = static_cast<float>(dt);
+    sc.gx = static_cast<float>(params.gravity[0]);
+    sc.gy = static_cast<float>(params.gravity[1]);
+    sc.gz = static_cast<float>(params.gravity[2]);
+    sc.has_bounds = params.has_bounds ? 1 : 0;
+    sc.wall_mode = params.wall_mode;
+    sc.live = 1;
+    for (int k = 0; k < 3; ++k) {
+        sc.bmin[k] = static_cast<float>(params.bounds_min[k]);
+        sc.bmax[k] = static_cast<float>(params.bounds_max[k]);
+        // gpu.wgsl:962-965: floor(bound * inv_h - 0.5) -/+ 2 in f32
+        float lo = std::floor(sc.bmin[k] * sc.inv_h - 0.5f), hi = std::floor(sc.bmax[k] * sc.inv_h - 0.5f);
+        sc.first_base[k] = static_cast<int>(std::max(lo, -1.0e9f)) - 2;
+        sc.last_base[k] = static_cast<int>(std::min(hi, 1.0e9f)) + 2;
+    }
+    return sc;
+}
+
+// Load and validate caller arrays (MpmWorld::add_particle checks, world.rs:492-503).
+inline TmpmStatus load_checked(const TmpmParticleArrays *particles, HostWorld &out, std::string &err) {
+    if (!particles || particles->count == 0) {
+        out.resize(0);
+        return TMPM_OK;
+    }
+    if (!particles->position || !particles->velocity || !particles->mass || !particles->rest_volume ||
+        !particles->radius || !particles->material || !particles->material_params) {
+        err = "required particle arrays are missing";
+        return TMPM_ERR_INVALID_INPUT;
+    }
+    out.load(*particles);
+    std::atomic<bool> bad{false};
+    parallel_for(out.n, [&](size_t lo, size_t hi) {
+        for (size_t i = lo; i < hi && !bad.load(std::memory_order_relaxed); ++i)
+            if (!valid_particle(out, i)) bad = true;
+    });
+    if (bad) {
+        err = "invalid MPM input";
+        return TMPM_ERR_MPM_INVALID_INPUT;
+    }
+    return TMPM_OK;
+}
+
+// Deduplicated device material classes (one DevClass per distinct particle
+// constant set; particles carry a class index).
+struct ClassTable {
+    std::vector<DevClass> table;
+    std::unordered_map<std::string, uint32_t> index;
+    uint32_t intern(const DevClass &k) {
+        std::string key(reinterpret_cast<const char *>(&k), sizeof(DevClass));
+        auto it = index.find(key);
+        if (it != index.end()) return it->second;
+        uint32_t id = static_cast<uint32_t>(table.size());
+        table.push_back(k);
+        index.emplace(std::move(key), id);
+        return id;
+    }
+    bool plastic() const {
+        for (const DevClass &k : table)
+            if (k.kind >= kMatSnow) return true;
+        return false;
+    }
+};
+
+// Where pack_world writes: `base` holds 27 component rows of `stride` floats
+// (x 0-2, v 3-5, C 6-14, F 15-23, plastic 24-26, matrices column-major),
+// `cls` and `widx` one entry per enabled particle.
+struct PackTarget {
+    float *base = nullptr;
+    uint32_t *cls = nullptr;
+    uint32_t *widx = nullptr;
+    size_t stride = 0;
+};
+
+struct PackResult {
+    TmpmStatus st = TMPM_OK;
+    const char *msg = "";
+    size_t enabled = 0;
+    std::vector<unsigned long long> blocks;  // distinct occupied home blocks (namespace included), sorted
+};
+
+// Validate the world's f32 representation and pack its enabled particles (the
+// device half of GpuMpmTransfers::prepare, gpu.rs:1091-1600).  Runs in two
+// parallel passes over contiguous particle chunks: pass 1 validates, builds
+// per-chunk class tables and block lists and counts enabled particles; then
+// `alloc(n_enabled)` supplies the PackTarget and pass 2 writes the f32 rows
+// at compacted positions.  Results equal a serial pass in world order.
+// `ns_high` is OR-ed into every class's grid namespace (multi-scene batches).
+template <typename Alloc>
+PackResult pack_world(const HostWorld &world, float inv_h, uint32_t ns_high, ClassTable &ct, Alloc alloc) {
+    PackResult res;
+    const size_t N = world.n;
+    struct ChunkOut {
+        size_t first_bad = std::numeric_limits<size_t>::max();
+        TmpmStatus st = TMPM_OK;
+        const char *msg = "";
+        size_t enabled = 0;
+        std::vector<DevClass> classes;
+        std::vector<unsigned long long> blocks;
+    };
+    const unsigned T = host_threads();
+    std::vector<ChunkOut> co(T + 1);
+    std::vector<uint32_t> lcls(std::max<size_t>(N, 1));
+    parallel_chunks(N, [&](size_t c, size_t lo, size_t hi) {
+        ChunkOut &o = co[c];
+        std::unordered_map<std::string, uint32_t> index;
+        DevClass last{};
+        uint32_t last_ci = kClassMask;
+        unsigned long long last_block = ~0ull;
+        auto bad = [&](size_t i, TmpmStatus st, const char *msg) {
+            o.first_bad = i;
+            o.st = st;
+            o.msg = msg;
+        };
+        for (size_t i = lo; i < hi; ++i) {
+            float f4[4];
+            for (int k = 0; k < 3; ++k)
+                if (!f32_ok(world.pos[3 * i + k], f4[k]) || !f32_ok(world.vel[3 * i + k], f4[3]) ||
+                    !f32_ok(world.force[3 * i + k], f4[3]))
+                    return bad(i, TMPM_ERR_INVALID_INPUT, "particle state not representable in f32");
+            float m32, v32, r32, d32;
+            if (!f32_ok(world.enabled[i] ? world.mass[i] : 0.0, m32) || !f32_ok(world.vol[i], v32) ||
+                !f32_ok(world.radius[i], r32) || !f32_ok(world.damping[i], d32))
+                return bad(i, TMPM_ERR_INVALID_INPUT, "particle scalars not representable in f32");
+            if (world.enabled[i] && (m32 <= 0.0f || v32 <= 0.0f))
+                return bad(i, TMPM_ERR_INVALID_INPUT, "particle mass or volume underflows f32");
+            if (r32 <= 0.0f || world.damping[i] < 0.0)
+                return bad(i, TMPM_ERR_INVALID_INPUT, "particle radius or damping invalid");
+            for (int k = 0; k < 9; ++k) {
+                float t;
+                if (!f32_ok(world.F[9 * i + k], t) || !f32_ok(world.C[9 * i + k], t))
+                    return bad(i, TMPM_ERR_INVALID_INPUT, "particle matrices not representable in f32");
+            }
+            if (!world.enabled[i]) continue;
+            int base[3];
+            for (int k = 0; k < 3; ++k) {
+                float xk = static_cast<float>(world.pos[3 * i + k]);
+                float cf = std::floor(xk * inv_h - 0.5f);
+                if (!std::isfinite(cf) || cf < -131000.0f || cf > 131000.0f)
+                    return bad(i, TMPM_ERR_INVALID_INPUT, "particle cell outside the representable grid");
+                base[k] = static_cast<int>(cf);
+            }
+            int kind = class_kind(world.material[i]);
+            const double *mp = &world.mparams[5 * i];
+            if (kind == kMatCorotated || kind == kMatSand || kind == kMatSnow) {
+                // use_cpu_corotated (gpu.rs:1156-1170): ill-conditioned F is a CPU case
+                const double *Fm = &world.F[9 * i];
+                double nrm = fro9(Fm), inrm = std::numeric_limits<double>::infinity();
+                inverse_norm9(Fm, inrm);
+                if (std::fabs(det9(Fm)) < 1e-5 || !(nrm >= 1e-5 && nrm <= 20.0) || nrm * inrm > 100.0) kind = 0;
+            }
+            if (kind == 0)
+                return bad(i, TMPM_ERR_RESIDENT_UNAVAILABLE,
+                           "particle material or deformation needs the CPU path (plastic material or "
+                           "ill-conditioned F)");
+            DevClass k{};
+            k.mass = m32;
+            k.volume = v32;
+            k.radius = r32;
+            k.damping = d32;
+            k.kind = kind;
+            k.color = ns_high | world.color[i];
+            float rho = std::max(m32 / v32, 1e-12f);
+            if (kind == kMatFluid) {
+                float b, g, vi, te;
+                if (!f32_ok(mp[0], b) || !f32_ok(mp[1], g) || !f32_ok(mp[2], vi) || !f32_ok(mp[3], te))
+                    return bad(i, TMPM_ERR_INVALID_INPUT, "fluid parameters not representable in f32");
+                k.p0 = b;
+                k.p1 = g;
+                k.p2 = vi;
+                k.p3 = te;
+                k.wave = std::sqrt(b * g / rho);
+            } else {
+                double lambda, mu;
+                lame(mp[0], mp[1], lambda, mu);
+                float l32, m32b;
+                if (!f32_ok(lambda, l32) || !f32_ok(mu, m32b))
+                    return bad(i, TMPM_ERR_INVALID_INPUT, "Lame parameters not representable in f32");
+                k.p0 = l32;
+                k.p1 = m32b;
+                k.wave = std::sqrt((l32 + 2.0f * m32b) / rho);
+                // sand / NH sand: friction angle, cohesion; snow: hardening, critical compression, stretch
+                bool ok = true;
+                if (kind == kMatSand || kind == kMatSandNeoHookean) {
+                    ok = f32_ok(mp[2], k.p2) && f32_ok(mp[3], k.p3);
+                } else if (kind == kMatSnow) {
+                    ok = f32_ok(mp[4], k.p2) && f32_ok(mp[2], k.p3) && f32_ok(mp[3], k.p4);
+                }
+                float t3;
+                if (kind >= kMatSnow)
+                    for (int q = 0; q < 3; ++q) ok = ok && f32_ok(world.plastic[3 * i + q], t3);
+                if (!ok) return bad(i, TMPM_ERR_INVALID_INPUT, "plastic parameters not representable in f32");
+            }
+            uint32_t ci;
+            if (last_ci != kClassMask && std::memcmp(&k, &last, sizeof(DevClass)) == 0) {
+                ci = last_ci;
+            } else {
+                std::string key(reinterpret_cast<const char *>(&k), sizeof(DevClass));
+                auto it = index.find(key);
+                if (it == index.end()) {
+                    ci = static_cast<uint32_t>(o.classes.size());
+                    o.classes.push_back(k);
+                    index.emplace(std::move(key), ci);
+                } else {
+                    ci = it->second;
+                }
+                last = k;
+                last_ci = ci;
+            }
+            lcls[i] = ci;
+            unsigned long long hb =
+                (static_cast<unsigned long long>(k.color & 0xFFFF) << 48) |
+                (static_cast<unsigned long long>(static_cast<uint32_t>((base[0] >> 2) + kBlockBias) & 0xFFFF) << 32) |
+                (static_cast<unsigned long long>(static_cast<uint32_t>((base[1] >> 2) + kBlockBias) & 0xFFFF) << 16) |
+                static_cast<unsigned long long>(static_cast<uint32_t>((base[2] >> 2) + kBlockBias) & 0xFFFF);
+            if (hb != last_block) {
+                o.blocks.push_back(hb);
+                last_block = hb;
+            }
+            ++o.enabled;
+        }
+        std::sort(o.blocks.begin(), o.blocks.end());
+        o.blocks.erase(std::unique(o.blocks.begin(), o.blocks.end()), o.blocks.end());
+    });
+    size_t worst = std::numeric_limits<size_t>::max();
+    for (const ChunkOut &o : co)
+        if (o.first_bad < worst) {
+            worst = o.first_bad;
+            res.st = o.st;
+            res.msg = o.msg;
+        }
+    if (res.st != TMPM_OK) return res;
+    // merge class tables and block lists (small), compute compacted offsets
+    std::vector<std::vector<uint32_t>> remap(co.size());
+    std::vector<size_t> offset(co.size(), 0);
+    size_t n_enabled = 0;
+    for (size_t c = 0; c < co.size(); ++c) {
+        offset[c] = n_enabled;
+        n_enabled += co[c].enabled;
+        for (const DevClass &k : co[c].classes) remap[c].push_back(ct.intern(k));
+        res.blocks.insert(res.blocks.end(), co[c].blocks.begin(), co[c].blocks.end());
+    }
+    std::sort(res.blocks.begin(), res.blocks.end());
+    res.blocks.erase(std::unique(res.blocks.begin(), res.blocks.end()), res.blocks.end());
+    if (ct.table.size() > kClassMask) {
+        res.st = TMPM_ERR_CAPACITY;
+        res.msg = "too many distinct particle classes";
+        return res;
+    }
+    res.enabled = n_enabled;
+    PackTarget tg = alloc(n_enabled);
+    if (!tg.base) {
+        res.st = TMPM_ERR_DEVICE;
+        res.msg = "pinned staging allocation failed";
+        return res;
+    }
+    const size_t S = tg.stride;
+    float *hx = tg.base, *hv = hx + 3 * S, *hC = hv + 3 * S, *hF = hC + 9 * S, *hpl = hF + 9 * S;
+    parallel_chunks(N, [&](size_t c, size_t lo, size_t hi) {
+        size_t j = offset[c];
+        const std::vector<uint32_t> &rm = remap[c];
+        for (size_t i = lo; i < hi; ++i) {
+            if (!world.enabled[i]) continue;
+            for (int k3 = 0; k3 < 3; ++k3) {
+                hx[k3 * S + j] = static_cast<float>(world.pos[3 * i + k3]);
+                hv[k3 * S + j] = static_cast<float>(world.vel[3 * i + k3]);
+            }
+            for (int k9 = 0; k9 < 9; ++k9) {
+                hC[k9 * S + j] = static_cast<float>(world.C[9 * i + k9]);
+                hF[k9 * S + j] = static_cast<float>(world.F[9 * i + k9]);
+            }
+            for (int k3 = 0; k3 < 3; ++k3) hpl[k3 * S + j] = static_cast<float>(world.plastic[3 * i + k3]);
+            tg.cls[j] = rm[lcls[i]] | (world.fixed[i] ? kFixedBit : 0u);
+            tg.widx[j] = static_cast<uint32_t>(i);
+            ++j;
+        }
+    });
+    return res;
+}
+
+}  // namespace tmpm

@@ -57,10 +57,26 @@ struct DevClass {
     float p0, p1, p2, p3;
     int32_t kind;          // kMat*
     float wave;            // CFL wave speed sqrt((lambda + 2 mu) / rho) or sqrt(K gamma / rho)
-    uint32_t color;        // transfer colour (separate grid namespace)
+    uint32_t color;        // grid namespace: the transfer colour; in a multi-scene batch (scene << 8) | colour
     float p4;
 };
 static_assert(sizeof(DevClass) == 48, "DevClass layout");
+
+// Per-scene integration parameters (MpmParams + the fixed substep), one entry
+// per scene of a batch; a single-scene session has one entry.
+struct SceneParams {
+    float h, inv_h, inv_d, dt;
+    float gx, gy, gz;
+    int has_bounds;
+    float bmin[3];
+    int wall_mode;
+    float bmax[3];
+    int steps;                        // substeps this scene advances in the current batch
+    int first_base[3];                // escape window of base cells (bounded worlds)
+    int live;                         // 0 = removed: dropped by the next re-sort
+    int last_base[3], pad;
+};
+static_assert(sizeof(SceneParams) == 96, "SceneParams layout");
 
 struct DevObstacle {
     int32_t shape, boundary, cpic_group, plane_offset;
@@ -83,13 +99,20 @@ struct GridTable {
     uint32_t max_blocks;
 };
 
+// Grid namespace of a particle class in a multi-scene batch: scene << kSceneShift | colour.
+constexpr int kSceneShift = 8;
+constexpr int kMaxScenes = 256;   // scenes per batch (16-bit namespace field of the block key)
+constexpr int kMaxBatchColors = 256;
+constexpr int kSortBitsScene = 21;            // single scene: 21-bit block Morton key
+constexpr int kSortBitsBatch = 30;            // batch: scene << 21 | Morton, plus the removed-scene bit
+constexpr uint32_t kDeadKey = 0x3FFFFFFFu;
+
 struct SimParams {
-    float h, inv_h, inv_d, dt;
-    float gx, gy, gz;
-    int has_bounds;
-    float bmin[3], bmax[3];
-    int first_base[3], last_base[3];  // escape window of base cells (bounded worlds)
-    int wall_mode;
+    SceneParams s0;             // the scene of a single-scene session (kernel parameter, constant bank)
+    const SceneParams *scenes;  // multi-scene batch: device scene table, indexed by namespace >> kSceneShift
+    uint32_t *scene_status;     // multi-scene batch: per-scene resident failure flags
+    int multi;                  // 1 = multi-scene batch (per-particle scene lookup and step gating)
+    int step_index;             // substep completed by this launch's G2P (-1 for the opening P2G)
     int num_obstacles;
     int reactions;
     int apply_force;
@@ -131,10 +154,12 @@ void launch_grid_update(const GridTable &g, const GridTable &next, const SimPara
                         const DevObstacle *obstacles, const float *planes, double *reactions,
                         uint32_t *status, cudaStream_t stream);
 void launch_clear_table(const GridTable &g, cudaStream_t stream);
-void launch_resort(ParticleSoA &src, ParticleSoA &dst, int n, const SimParams &sp, SortBuffers &sb,
-                   cudaStream_t stream);
-void launch_bin_keys(const ParticleSoA &P, int n, const SimParams &sp, int32_t *cells, uint32_t *keys,
-                     cudaStream_t stream);
+// Re-sort by block key into `dst`; particles of removed scenes sort last and the
+// first `keep` particles are gathered.
+void launch_resort(ParticleSoA &src, ParticleSoA &dst, int n, int keep, const DevClass *classes, const SimParams &sp,
+                   SortBuffers &sb, cudaStream_t stream);
+void launch_bin_keys(const ParticleSoA &P, int n, const DevClass *classes, const SimParams &sp, int32_t *cells,
+                     uint32_t *keys, cudaStream_t stream);
 // Morton block keys (and identity values) of `n` positions stored component-major with `stride`.
 void launch_bin_keys_values(const float *x, size_t stride, int n, float inv_h, uint32_t *keys, uint32_t *vals,
                             cudaStream_t stream);
@@ -146,8 +171,8 @@ int device_sm_count();
 // Thread-local reason reported by tmpm_last_error() (tmpm_session.cu).
 void set_last_error(const std::string &msg);
 
-// Radix sort (tmpm_sort.cu): stable sort of (key, value) pairs by `bits` low key bits.
-// Result ends in sb.keys[0] / sb.vals[0].
-void radix_sort_pairs(SortBuffers &sb, int n, int bits, cudaStream_t stream);
+// Radix sort (tmpm_sort.cu): stable sort of (key, value) pairs by `bits` low key
+// bits, 8 bits per pass.  Returns r: the result is in sb.keys[r] / sb.vals[r].
+int radix_sort_pairs(SortBuffers &sb, int n, int bits, cudaStream_t stream);
 
 }  // namespace tmpm

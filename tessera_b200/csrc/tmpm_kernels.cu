@@ -171,8 +171,12 @@ __device__ __forceinline__ float pow2_scale(float total) {
 }
 
 // PLASTIC selects the variant that carries plastic state (snow, sand, NH sand);
-// scenes without plastic materials run the leaner variant.
-template <int MODE, bool PLASTIC>
+// scenes without plastic materials run the leaner variant.  MULTI selects the
+// multi-scene batch variant: each particle reads its scene's parameters from
+// the scene table (scene = class namespace >> kSceneShift) and takes part only
+// in the substeps its scene advances in this batch; the single-scene variant
+// reads them from the kernel parameters.
+template <int MODE, bool PLASTIC, bool MULTI>
 __global__ void __launch_bounds__(kThreads, TMPM_TRANSFER_MIN_BLOCKS)
     k_transfer(ParticleSoA P, int n, const DevClass *__restrict__ classes, GridTable cur, GridTable next,
                SimParams sp, const DevObstacle *__restrict__ obstacles, const float *__restrict__ planes,
@@ -190,7 +194,6 @@ __global__ void __launch_bounds__(kThreads, TMPM_TRANSFER_MIN_BLOCKS)
     const size_t cap = P.cap;
     const int i = blockIdx.x * kThreads + threadIdx.x;
     const bool valid = i < n;
-    const float h = sp.h, inv_h = sp.inv_h, inv_d = sp.inv_d, dt = sp.dt;
     int *const cc = cache + static_cast<size_t>(blockIdx.x) * kCacheStride;
 
     if (threadIdx.x == 0) s_abort = (*reinterpret_cast<volatile uint32_t *>(status) & kFatal) != 0;
@@ -213,8 +216,21 @@ __global__ void __launch_bounds__(kThreads, TMPM_TRANSFER_MIN_BLOCKS)
         cw = P.cls[i];
         k = classes[cw & kClassMask];
     }
+    const int scene = MULTI ? static_cast<int>(k.color >> kSceneShift) : 0;
+    const SceneParams *const scn = sp.scenes + scene;
+#define SCN(f) (MULTI ? scn->f : sp.s0.f)
+    const float h = SCN(h), inv_h = SCN(inv_h), inv_d = SCN(inv_d), dt = SCN(dt);
+    // g2p_on: the particle completes substep step_index here; p2g_on: it scatters for step_index + 1.
+    bool g2p_on = valid, p2g_on = valid;
+    if (MULTI && valid) {
+        const int steps = scn->steps;
+        const bool dead = (__ldcg(sp.scene_status + scene) & kStatusResident) != 0;
+        g2p_on = !dead && sp.step_index < steps;
+        p2g_on = !dead && sp.step_index + 1 < steps;
+    }
+    uint32_t *const resident_flag = MULTI ? sp.scene_status + scene : status;
     const bool fixed = (cw & kFixedBit) != 0;
-    const bool plastic = PLASTIC && valid && k.kind >= kMatSnow;
+    const bool plastic = PLASTIC && g2p_on && k.kind >= kMatSnow;
     float pl[3] = {1.0f, 0.0f, 0.0f};
     if (plastic) {
         pl[0] = P.pl[i];
@@ -227,7 +243,7 @@ __global__ void __launch_bounds__(kThreads, TMPM_TRANSFER_MIN_BLOCKS)
     gbox.ok = 0;
 
     if (MODE == kModeP2G) {
-        if (valid) {
+        if (p2g_on) {
             v = mk(P.v[i], P.v[cap + i], P.v[2 * cap + i]);
             Cm = load_m3(P.C, cap, i);
         }
@@ -259,7 +275,7 @@ __global__ void __launch_bounds__(kThreads, TMPM_TRANSFER_MIN_BLOCKS)
                 bx.nbt = cc[15];
                 bx.ok = 1;
             } else {
-                reduce_box(valid, b, k.color, s_red, s_box);
+                reduce_box(g2p_on, b, k.color, s_red, s_box);
                 bx = s_box;
                 if (bx.ok) {
                     for (int t = threadIdx.x; t < bx.nbt; t += kThreads) {
@@ -269,7 +285,7 @@ __global__ void __launch_bounds__(kThreads, TMPM_TRANSFER_MIN_BLOCKS)
                     __syncthreads();
                 }
             }
-            bool bad = use_cache && valid &&
+            bool bad = use_cache && g2p_on &&
                        (b[0] < bx.lo[0] || b[1] < bx.lo[1] || b[2] < bx.lo[2] || b[0] + 2 >= bx.lo[0] + bx.dim[0] ||
                         b[1] + 2 >= bx.lo[1] + bx.dim[1] || b[2] + 2 >= bx.lo[2] + bx.dim[2] || k.color != bx.color);
             if (bx.ok && !bad) {
@@ -297,7 +313,7 @@ __global__ void __launch_bounds__(kThreads, TMPM_TRANSFER_MIN_BLOCKS)
         quad_weights(fx.z, wz);
         V3f vel = mk(0, 0, 0);
         M3f aff = m3_zero();
-        if (valid && !fixed) {
+        if (g2p_on && !fixed) {
             float dxs[3], dys[3], dzs[3];
 #pragma unroll
             for (int a = 0; a < 3; ++a) {
@@ -350,7 +366,7 @@ __global__ void __launch_bounds__(kThreads, TMPM_TRANSFER_MIN_BLOCKS)
             }
         }
 
-        if (valid && !fixed) {
+        if (g2p_on && !fixed) {
             // Particle update (gpu.wgsl:885-1003; world.rs:443-463).
             if (sp.apply_force) {
                 const size_t w = P.widx[i], fs = P.force_stride;
@@ -360,9 +376,9 @@ __global__ void __launch_bounds__(kThreads, TMPM_TRANSFER_MIN_BLOCKS)
             vel = vel * expf(-k.damping * dt);
             V3f pos = x + vel * dt;
             const float radius = k.radius;
-            if (sp.has_bounds) {
+            if (SCN(has_bounds)) {
                 for (int a = 0; a < 3; ++a) {
-                    float lower = sp.bmin[a] + radius, upper = sp.bmax[a] - radius;
+                    float lower = SCN(bmin[a]) + radius, upper = SCN(bmax[a]) - radius;
                     float pa = comp(pos, a), va = comp(vel, a);
                     if (pa < lower) {
                         set_comp(pos, a, lower);
@@ -403,10 +419,10 @@ __global__ void __launch_bounds__(kThreads, TMPM_TRANSFER_MIN_BLOCKS)
             bool representable = ncx >= -131000.0f && ncx <= 131000.0f && ncy >= -131000.0f && ncy <= 131000.0f &&
                                  ncz >= -131000.0f && ncz <= 131000.0f;
             failed = failed || !representable;
-            if (!failed && sp.has_bounds) {
+            if (!failed && SCN(has_bounds)) {
                 int nb3[3] = {static_cast<int>(ncx), static_cast<int>(ncy), static_cast<int>(ncz)};
                 for (int a = 0; a < 3; ++a)
-                    failed = failed || nb3[a] < sp.first_base[a] || nb3[a] > sp.last_base[a];
+                    failed = failed || nb3[a] < SCN(first_base[a]) || nb3[a] > SCN(last_base[a]);
             }
             if (sp.resident_checks) {
                 if (k.kind == kMatCorotated || k.kind == kMatSnow || k.kind == kMatSand)
@@ -418,18 +434,18 @@ __global__ void __launch_bounds__(kThreads, TMPM_TRANSFER_MIN_BLOCKS)
                     failed = failed || dt * (k.wave + len(vel)) > 0.4f * h * (1.0f + 1e-4f);
                 }
                 failed = failed || !plastic_ok;
-                if (failed) atomicOr(status, kStatusResident);
+                if (failed) atomicOr(resident_flag, kStatusResident);
             } else {
                 if (finite3(pos) && !representable) atomicOr(status, kStatusCapacity);  // beyond the key range
                 // no CPU fallback on this path: an unprojectable plastic state is unavailable here
-                if (!plastic_ok) atomicOr(status, kStatusResident);
+                if (!plastic_ok) atomicOr(resident_flag, kStatusResident);
             }
             x = pos;
             v = vel;
             Cm = aff;
             F = Fn;
         }
-        if (valid) {
+        if (g2p_on) {
             P.x[i] = x.x;
             P.x[cap + i] = x.y;
             P.x[2 * cap + i] = x.z;
@@ -439,7 +455,8 @@ __global__ void __launch_bounds__(kThreads, TMPM_TRANSFER_MIN_BLOCKS)
                 P.pl[cap + i] = pl[1];
                 P.pl[2 * cap + i] = pl[2];
             }
-            if (MODE == kModeG2P) {
+            // the last substep of the batch (per scene in a multi-scene batch) writes v and C back
+            if (MODE == kModeG2P || (MULTI && !p2g_on)) {
                 P.v[i] = v.x;
                 P.v[cap + i] = v.y;
                 P.v[2 * cap + i] = v.z;
@@ -455,8 +472,11 @@ __global__ void __launch_bounds__(kThreads, TMPM_TRANSFER_MIN_BLOCKS)
     const bool in_range =
         block_representable(b[0] >> kBlockShift, b[1] >> kBlockShift, b[2] >> kBlockShift) &&
         block_representable((b[0] + 2) >> kBlockShift, (b[1] + 2) >> kBlockShift, (b[2] + 2) >> kBlockShift);
-    const bool active = valid && in_range;
-    if (valid && !in_range) atomicOr(status, sp.resident_checks ? kStatusResident : kStatusCapacity);
+    const bool active = p2g_on && in_range;
+    if (p2g_on && !in_range) {
+        if (sp.resident_checks) atomicOr(resident_flag, kStatusResident);
+        else atomicOr(status, kStatusCapacity);
+    }
     reduce_box(active, b, k.color, s_red, s_box);
     if (MODE == kModeP2G && s_abort) return;
     const Box bx = s_box;
@@ -607,9 +627,13 @@ __global__ void __launch_bounds__(kThreads, TMPM_TRANSFER_MIN_BLOCKS)
                     }
         }
     }
+#undef SCN
 }
 
 // Grid update over all allocated blocks; also zeroes those blocks in the other pool.
+// MULTI: each block takes its scene's parameters from the scene table
+// (scene = block namespace >> kSceneShift).
+template <bool MULTI>
 __global__ void __launch_bounds__(256) k_grid(GridTable g, GridTable nxt, SimParams sp,
                                                const DevObstacle *__restrict__ obstacles,
                                                const float *__restrict__ planes, double *reactions, uint32_t *status) {
@@ -621,7 +645,6 @@ __global__ void __launch_bounds__(256) k_grid(GridTable g, GridTable nxt, SimPar
     const size_t stride = static_cast<size_t>(gridDim.x) * blockDim.x;
     uint32_t nblocks = min(*g.count, g.max_blocks);
     const size_t nodes = static_cast<size_t>(nblocks) * kNodesPerBlock;
-    const float h = sp.h;
     float4 *next_pool = nxt.pool;
     for (size_t node = gtid; node < nodes; node += stride) {
         float4 mp = g.pool[node];
@@ -634,21 +657,26 @@ __global__ void __launch_bounds__(256) k_grid(GridTable g, GridTable nxt, SimPar
         int4 c = g.coords[node >> 6];
         int l = static_cast<int>(node & 63);
         int cx = c.x * 4 + (l >> 4), cy = c.y * 4 + ((l >> 2) & 3), cz = c.z * 4 + (l & 3);
-        V3f vel = mk(mp.y / mp.x + sp.gx * sp.dt, mp.z / mp.x + sp.gy * sp.dt, mp.w / mp.x + sp.gz * sp.dt);
+        const SceneParams *const scn = sp.scenes + (MULTI ? (static_cast<uint32_t>(c.w) >> kSceneShift) : 0u);
+#define SCN(f) (MULTI ? scn->f : sp.s0.f)
+        const float h = SCN(h), dt = SCN(dt);
+        V3f vel = mk(mp.y / mp.x + SCN(gx) * dt, mp.z / mp.x + SCN(gy) * dt, mp.w / mp.x + SCN(gz) * dt);
         V3f pos = mk(static_cast<float>(cx) * h, static_cast<float>(cy) * h, static_cast<float>(cz) * h);
-        if (sp.has_bounds) {
-            if (sp.wall_mode == 1) {
+        if (SCN(has_bounds)) {
+            if (SCN(wall_mode) == 1) {
                 bool near = false;
                 for (int a = 0; a < 3; ++a)
-                    near = near || comp(pos, a) <= sp.bmin[a] + h || comp(pos, a) >= sp.bmax[a] - h;
+                    near = near || comp(pos, a) <= SCN(bmin[a]) + h || comp(pos, a) >= SCN(bmax[a]) - h;
                 if (near) vel = mk(0, 0, 0);
             } else {
                 for (int a = 0; a < 3; ++a) {
                     float pa = comp(pos, a), va = comp(vel, a);
-                    if ((pa <= sp.bmin[a] + h && va < 0.0f) || (pa >= sp.bmax[a] - h && va > 0.0f)) set_comp(vel, a, 0.0f);
+                    if ((pa <= SCN(bmin[a]) + h && va < 0.0f) || (pa >= SCN(bmax[a]) - h && va > 0.0f))
+                        set_comp(vel, a, 0.0f);
                 }
             }
         }
+#undef SCN
         for (int oi = 0; oi < sp.num_obstacles; ++oi) {
             const DevObstacle &o = obstacles[oi];
             if (!obstacle_may_contact(o, pos, h)) continue;
@@ -676,17 +704,30 @@ __global__ void k_clear_table(GridTable g) {
     if (gtid == 0) *g.count = 0;
 }
 
-__global__ void k_bin_keys(const float *x, size_t cap, int n, float inv_h, int32_t *cells, uint32_t *keys,
-                           uint32_t *vals) {
+// Block sort key of each particle.  With a scene table (multi-scene batch) the
+// scene comes from the particle's class and its cell width from the table.
+__global__ void k_bin_keys(const float *x, size_t cap, int n, float inv_h, const uint32_t *__restrict__ cls,
+                           const DevClass *__restrict__ classes, const SceneParams *__restrict__ scenes,
+                           int32_t *cells, uint32_t *keys, uint32_t *vals) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
+    uint32_t scene = 0;
+    if (scenes) {
+        scene = classes[cls[i] & kClassMask].color >> kSceneShift;
+        if (!scenes[scene].live) {  // removed scene: sorts after every live particle
+            keys[i] = kDeadKey;
+            if (vals) vals[i] = static_cast<uint32_t>(i);
+            return;
+        }
+        inv_h = scenes[scene].inv_h;
+    }
     int b0 = base_cell(x[i], inv_h), b1 = base_cell(x[cap + i], inv_h), b2 = base_cell(x[2 * cap + i], inv_h);
     if (cells) {
         cells[3 * i] = b0;
         cells[3 * i + 1] = b1;
         cells[3 * i + 2] = b2;
     }
-    keys[i] = morton_block(b0 >> kBlockShift, b1 >> kBlockShift, b2 >> kBlockShift);
+    keys[i] = morton_block(b0 >> kBlockShift, b1 >> kBlockShift, b2 >> kBlockShift, scene);
     if (vals) vals[i] = static_cast<uint32_t>(i);
 }
 
@@ -751,27 +792,33 @@ void launch_transfer(int mode, const ParticleSoA &P, int n, const DevClass *clas
                      double *reactions, uint32_t *status, int *cache, cudaStream_t stream) {
     if (n <= 0) return;
     dim3 grid((n + kThreads - 1) / kThreads);
-#define TMPM_LAUNCH(M, PL) \
-    k_transfer<M, PL><<<grid, kThreads, 0, stream>>>(P, n, classes, cur, next, sp, obstacles, planes, reactions, status, cache)
+#define TMPM_LAUNCH(M, PL, MU) \
+    k_transfer<M, PL, MU><<<grid, kThreads, 0, stream>>>(P, n, classes, cur, next, sp, obstacles, planes, reactions, status, cache)
+#define TMPM_LAUNCH_MODE(M)                          \
+    do {                                             \
+        if (sp.multi) {                              \
+            if (pl) TMPM_LAUNCH(M, true, true);      \
+            else TMPM_LAUNCH(M, false, true);        \
+        } else {                                     \
+            if (pl) TMPM_LAUNCH(M, true, false);     \
+            else TMPM_LAUNCH(M, false, false);       \
+        }                                            \
+    } while (0)
     const bool pl = sp.has_plastic != 0;
     switch (mode) {
-    case kModeP2G:
-        if (pl) TMPM_LAUNCH(kModeP2G, true); else TMPM_LAUNCH(kModeP2G, false);
-        break;
-    case kModeG2P2G:
-        if (pl) TMPM_LAUNCH(kModeG2P2G, true); else TMPM_LAUNCH(kModeG2P2G, false);
-        break;
-    default:
-        if (pl) TMPM_LAUNCH(kModeG2P, true); else TMPM_LAUNCH(kModeG2P, false);
-        break;
+    case kModeP2G: TMPM_LAUNCH_MODE(kModeP2G); break;
+    case kModeG2P2G: TMPM_LAUNCH_MODE(kModeG2P2G); break;
+    default: TMPM_LAUNCH_MODE(kModeG2P); break;
     }
+#undef TMPM_LAUNCH_MODE
 #undef TMPM_LAUNCH
 }
 
 void launch_grid_update(const GridTable &g, const GridTable &next, const SimParams &sp, const DevObstacle *obstacles,
                         const float *planes, double *reactions, uint32_t *status, cudaStream_t stream) {
     int blocks = device_sm_count() * 8;
-    k_grid<<<blocks, 256, 0, stream>>>(g, next, sp, obstacles, planes, reactions, status);
+    if (sp.multi) k_grid<true><<<blocks, 256, 0, stream>>>(g, next, sp, obstacles, planes, reactions, status);
+    else k_grid<false><<<blocks, 256, 0, stream>>>(g, next, sp, obstacles, planes, reactions, status);
 }
 
 void launch_clear_table(const GridTable &g, cudaStream_t stream) {
@@ -779,24 +826,27 @@ void launch_clear_table(const GridTable &g, cudaStream_t stream) {
     k_clear_table<<<blocks, 256, 0, stream>>>(g);
 }
 
-void launch_bin_keys(const ParticleSoA &P, int n, const SimParams &sp, int32_t *cells, uint32_t *keys,
-                     cudaStream_t stream) {
+void launch_bin_keys(const ParticleSoA &P, int n, const DevClass *classes, const SimParams &sp, int32_t *cells,
+                     uint32_t *keys, cudaStream_t stream) {
     if (n <= 0) return;
-    k_bin_keys<<<(n + 255) / 256, 256, 0, stream>>>(P.x, P.cap, n, sp.inv_h, cells, keys, nullptr);
+    k_bin_keys<<<(n + 255) / 256, 256, 0, stream>>>(P.x, P.cap, n, sp.s0.inv_h, P.cls, classes,
+                                                    sp.multi ? sp.scenes : nullptr, cells, keys, nullptr);
 }
 
 void launch_bin_keys_values(const float *x, size_t stride, int n, float inv_h, uint32_t *keys, uint32_t *vals,
                             cudaStream_t stream) {
     if (n <= 0) return;
-    k_bin_keys<<<(n + 255) / 256, 256, 0, stream>>>(x, stride, n, inv_h, nullptr, keys, vals);
+    k_bin_keys<<<(n + 255) / 256, 256, 0, stream>>>(x, stride, n, inv_h, nullptr, nullptr, nullptr, nullptr, keys,
+                                                    vals);
 }
 
-void launch_resort(ParticleSoA &src, ParticleSoA &dst, int n, const SimParams &sp, SortBuffers &sb,
-                   cudaStream_t stream) {
+void launch_resort(ParticleSoA &src, ParticleSoA &dst, int n, int keep, const DevClass *classes, const SimParams &sp,
+                   SortBuffers &sb, cudaStream_t stream) {
     if (n <= 0) return;
-    k_bin_keys<<<(n + 255) / 256, 256, 0, stream>>>(src.x, src.cap, n, sp.inv_h, nullptr, sb.keys[0], sb.vals[0]);
-    radix_sort_pairs(sb, n, 30, stream);
-    k_gather<<<(n + 255) / 256, 256, 0, stream>>>(src, dst, sb.vals[0], n);
+    k_bin_keys<<<(n + 255) / 256, 256, 0, stream>>>(src.x, src.cap, n, sp.s0.inv_h, src.cls, classes,
+                                                    sp.multi ? sp.scenes : nullptr, nullptr, sb.keys[0], sb.vals[0]);
+    const int r = radix_sort_pairs(sb, n, sp.multi ? kSortBitsBatch : kSortBitsScene, stream);
+    if (keep > 0) k_gather<<<(keep + 255) / 256, 256, 0, stream>>>(src, dst, sb.vals[r], keep);
 }
 
 void launch_dump_grid(const GridTable &g, int32_t *cells, float4 *values, uint32_t *count, uint32_t capacity,

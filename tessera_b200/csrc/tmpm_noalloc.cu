@@ -88,9 +88,9 @@ extern "C" TmpmStatus tmpm_sort_by_block_noalloc(const float *positions, size_t 
     // radix pass), so nothing has to start at zero.
     const int n = static_cast<int>(count);
     tmpm::launch_bin_keys_values(positions, stride, n, 1.0f / h32, sb.keys[0], sb.vals[0], s);
-    tmpm::radix_sort_pairs(sb, n, 30, s);
-    cudaMemcpyAsync(order_out, sb.vals[0], sizeof(uint32_t) * count, cudaMemcpyDeviceToDevice, s);
-    if (keys_out) cudaMemcpyAsync(keys_out, sb.keys[0], sizeof(uint32_t) * count, cudaMemcpyDeviceToDevice, s);
+    const int r = tmpm::radix_sort_pairs(sb, n, tmpm::kSortBitsScene, s);
+    cudaMemcpyAsync(order_out, sb.vals[r], sizeof(uint32_t) * count, cudaMemcpyDeviceToDevice, s);
+    if (keys_out) cudaMemcpyAsync(keys_out, sb.keys[r], sizeof(uint32_t) * count, cudaMemcpyDeviceToDevice, s);
     e = cudaGetLastError();
     if (e != cudaSuccess) return noalloc_fail(TMPM_ERR_DEVICE, std::string("launch: ") + cudaGetErrorString(e));
     return TMPM_OK;

@@ -21,517 +21,11 @@
 #include <vector>
 
 #include "../../include/tmpm.h"
+#include "tmpm_host.h"
 #include "tmpm_internal.h"
 
 using namespace tmpm;
 
-namespace {
-
-thread_local std::string g_last_error;
-
-constexpr double kSyncTimeoutSeconds = 5.0;  // gpu.rs:1853-1862
-
-unsigned host_threads() { return std::max(1u, std::min(32u, std::thread::hardware_concurrency())); }
-
-// Run fn(chunk, begin, end) over [0, n) split into contiguous chunks, one per host thread.
-template <typename Fn>
-void parallel_chunks(size_t n, Fn fn, size_t min_per_chunk = 32768) {
-    size_t chunks = std::min<size_t>(host_threads(), std::max<size_t>(1, n / min_per_chunk));
-    if (chunks <= 1) {
-        fn(size_t(0), size_t(0), n);
-        return;
-    }
-    size_t per = (n + chunks - 1) / chunks;
-    std::vector<std::thread> pool;
-    for (size_t c = 0; c < chunks; ++c) {
-        size_t a = c * per, b = std::min(n, a + per);
-        if (a >= b) break;
-        pool.emplace_back([=]() { fn(c, a, b); });
-    }
-    for (auto &t : pool) t.join();
-}
-
-template <typename Fn>
-void parallel_for(size_t n, Fn fn) {
-    parallel_chunks(n, [&](size_t, size_t a, size_t b) { fn(a, b); });
-}
-
-// --------------------------------------------------------------- host world
-
-struct HostWorld {
-    size_t n = 0;
-    std::vector<double> pos, vel, F, C, force, mass, vol, radius, damping, plastic, mparams;
-    std::vector<int32_t> material;
-    std::vector<uint8_t> enabled, fixed;
-    std::vector<uint16_t> color;
-    std::vector<uint32_t> group;
-    std::vector<uint64_t> chunk;
-
-    // Sizes every field for `count` particles; existing storage is reused and
-    // not cleared (load() writes every element).
-    void resize(size_t count) {
-        n = count;
-        pos.resize(3 * n);
-        vel.resize(3 * n);
-        F.resize(9 * n);
-        C.resize(9 * n);
-        force.resize(3 * n);
-        mass.resize(n);
-        vol.resize(n);
-        radius.resize(n);
-        damping.resize(n);
-        plastic.resize(3 * n);
-        mparams.resize(5 * n);
-        material.resize(n);
-        enabled.resize(n);
-        fixed.resize(n);
-        color.resize(n);
-        group.resize(n);
-        chunk.resize(n);
-    }
-
-    void load(const TmpmParticleArrays &a) {
-        resize(a.count);
-        parallel_for(n, [&](size_t lo, size_t hi) { load_range(a, lo, hi); });
-    }
-
-    void load_range(const TmpmParticleArrays &a, size_t lo, size_t hi) {
-        for (size_t i = lo; i < hi; ++i) {
-            for (int k = 0; k < 3; ++k) {
-                pos[3 * i + k] = a.position[3 * i + k];
-                vel[3 * i + k] = a.velocity[3 * i + k];
-                force[3 * i + k] = a.force ? a.force[3 * i + k] : 0.0;
-            }
-            for (int k = 0; k < 9; ++k) {
-                F[9 * i + k] = a.deformation ? a.deformation[9 * i + k] : ((k % 4 == 0) ? 1.0 : 0.0);
-                C[9 * i + k] = a.affine ? a.affine[9 * i + k] : 0.0;
-            }
-            mass[i] = a.mass[i];
-            vol[i] = a.rest_volume[i];
-            radius[i] = a.radius[i];
-            damping[i] = a.damping ? a.damping[i] : 0.0;
-            material[i] = a.material[i];
-            for (int k = 0; k < 5; ++k) mparams[5 * i + k] = a.material_params[5 * i + k];
-            if (a.plastic) {
-                for (int k = 0; k < 3; ++k) plastic[3 * i + k] = a.plastic[3 * i + k];
-            } else {
-                plastic[3 * i] = 1.0;
-                plastic[3 * i + 1] = (material[i] == TMPM_MAT_SAND || material[i] == TMPM_MAT_SAND_NEO_HOOKEAN) ? 1.0 : 0.0;
-                plastic[3 * i + 2] = 0.0;
-            }
-            enabled[i] = a.enabled ? (a.enabled[i] != 0) : 1;
-            fixed[i] = a.fixed ? (a.fixed[i] != 0) : 0;
-            color[i] = a.transfer_color ? a.transfer_color[i] : 0;
-            group[i] = a.group_id ? a.group_id[i] : 0;
-            chunk[i] = a.chunk_id ? a.chunk_id[i] : 0;
-        }
-    }
-
-    void store(TmpmParticleArrays &a) const {
-        parallel_for(n, [&](size_t lo, size_t hi) { store_range(a, lo, hi); });
-    }
-
-    void store_range(TmpmParticleArrays &a, size_t lo, size_t hi) const {
-        for (size_t i = lo; i < hi; ++i) {
-            for (int k = 0; k < 3; ++k) {
-                if (a.position) a.position[3 * i + k] = pos[3 * i + k];
-                if (a.velocity) a.velocity[3 * i + k] = vel[3 * i + k];
-                if (a.force) a.force[3 * i + k] = force[3 * i + k];
-                if (a.plastic) a.plastic[3 * i + k] = plastic[3 * i + k];
-            }
-            for (int k = 0; k < 9; ++k) {
-                if (a.deformation) a.deformation[9 * i + k] = F[9 * i + k];
-                if (a.affine) a.affine[9 * i + k] = C[9 * i + k];
-            }
-            if (a.mass) a.mass[i] = mass[i];
-            if (a.rest_volume) a.rest_volume[i] = vol[i];
-            if (a.radius) a.radius[i] = radius[i];
-            if (a.damping) a.damping[i] = damping[i];
-            if (a.material) a.material[i] = material[i];
-            if (a.material_params)
-                for (int k = 0; k < 5; ++k) a.material_params[5 * i + k] = mparams[5 * i + k];
-            if (a.enabled) a.enabled[i] = enabled[i];
-            if (a.fixed) a.fixed[i] = fixed[i];
-            if (a.transfer_color) a.transfer_color[i] = color[i];
-            if (a.group_id) a.group_id[i] = group[i];
-            if (a.chunk_id) a.chunk_id[i] = chunk[i];
-        }
-    }
-
-    void append(const HostWorld &o) {
-        auto cat = [](auto &dst, const auto &src) { dst.insert(dst.end(), src.begin(), src.end()); };
-        cat(pos, o.pos);
-        cat(vel, o.vel);
-        cat(F, o.F);
-        cat(C, o.C);
-        cat(force, o.force);
-        cat(mass, o.mass);
-        cat(vol, o.vol);
-        cat(radius, o.radius);
-        cat(damping, o.damping);
-        cat(plastic, o.plastic);
-        cat(mparams, o.mparams);
-        cat(material, o.material);
-        cat(enabled, o.enabled);
-        cat(fixed, o.fixed);
-        cat(color, o.color);
-        cat(group, o.group);
-        cat(chunk, o.chunk);
-        n += o.n;
-    }
-
-    // Keep particles whose chunk differs (world.rs:267-277).
-    size_t remove_chunk(uint64_t c) {
-        size_t w = 0;
-        for (size_t i = 0; i < n; ++i) {
-            if (chunk[i] == c) continue;
-            if (w != i) {
-                for (int k = 0; k < 3; ++k) {
-                    pos[3 * w + k] = pos[3 * i + k];
-                    vel[3 * w + k] = vel[3 * i + k];
-                    force[3 * w + k] = force[3 * i + k];
-                    plastic[3 * w + k] = plastic[3 * i + k];
-                }
-                for (int k = 0; k < 9; ++k) {
-                    F[9 * w + k] = F[9 * i + k];
-                    C[9 * w + k] = C[9 * i + k];
-                }
-                for (int k = 0; k < 5; ++k) mparams[5 * w + k] = mparams[5 * i + k];
-                mass[w] = mass[i];
-                vol[w] = vol[i];
-                radius[w] = radius[i];
-                damping[w] = damping[i];
-                material[w] = material[i];
-                enabled[w] = enabled[i];
-                fixed[w] = fixed[i];
-                color[w] = color[i];
-                group[w] = group[i];
-                chunk[w] = chunk[i];
-            }
-            ++w;
-        }
-        size_t removed = n - w;
-        n = w;
-        pos.resize(3 * n);
-        vel.resize(3 * n);
-        force.resize(3 * n);
-        plastic.resize(3 * n);
-        F.resize(9 * n);
-        C.resize(9 * n);
-        mparams.resize(5 * n);
-        mass.resize(n);
-        vol.resize(n);
-        radius.resize(n);
-        damping.resize(n);
-        material.resize(n);
-        enabled.resize(n);
-        fixed.resize(n);
-        color.resize(n);
-        group.resize(n);
-        chunk.resize(n);
-        return removed;
-    }
-};
-
-// ------------------------------------------------------------- host math
-
-double det9(const double *m) {  // column-major
-    return m[0] * (m[4] * m[8] - m[7] * m[5]) - m[3] * (m[1] * m[8] - m[7] * m[2]) + m[6] * (m[1] * m[5] - m[4] * m[2]);
-}
-double fro9(const double *m) {
-    double s = 0;
-    for (int k = 0; k < 9; ++k) s += m[k] * m[k];
-    return std::sqrt(s);
-}
-bool inverse_norm9(const double *m, double &out) {
-    double d = det9(m);
-    if (d == 0.0 || !std::isfinite(d)) return false;
-    // cofactors: the inverse's Frobenius norm equals that of the cofactor matrix / |det|
-    const double *a = m, *b = m + 3, *c = m + 6;
-    double bc[3] = {b[1] * c[2] - b[2] * c[1], b[2] * c[0] - b[0] * c[2], b[0] * c[1] - b[1] * c[0]};
-    double ca[3] = {c[1] * a[2] - c[2] * a[1], c[2] * a[0] - c[0] * a[2], c[0] * a[1] - c[1] * a[0]};
-    double ab[3] = {a[1] * b[2] - a[2] * b[1], a[2] * b[0] - a[0] * b[2], a[0] * b[1] - a[1] * b[0]};
-    double s = 0;
-    for (int k = 0; k < 3; ++k) s += bc[k] * bc[k] + ca[k] * ca[k] + ab[k] * ab[k];
-    out = std::sqrt(s) / std::fabs(d);
-    return std::isfinite(out);
-}
-
-void lame(double young, double poisson, double &lambda, double &mu) {  // material.rs:433-438
-    lambda = young * poisson / ((1.0 + poisson) * (1.0 - 2.0 * poisson));
-    mu = young / (2.0 * (1.0 + poisson));
-}
-
-bool valid_elasticity(double young, double poisson) {  // material.rs:429-431
-    return std::isfinite(young) && young > 0.0 && std::isfinite(poisson) && poisson >= -1.0 && poisson < 0.5;
-}
-
-bool material_valid(int kind, const double *p) {  // material.rs:171-231
-    switch (kind) {
-    case TMPM_MAT_ELASTIC:
-    case TMPM_MAT_NEO_HOOKEAN:
-        return valid_elasticity(p[0], p[1]);
-    case TMPM_MAT_SAND:
-    case TMPM_MAT_SAND_NEO_HOOKEAN:
-        return valid_elasticity(p[0], p[1]) && std::isfinite(p[2]) && p[2] >= 0.0 && p[2] < M_PI / 2.0 &&
-               std::isfinite(p[3]) && p[3] >= 0.0;
-    case TMPM_MAT_FLUID:
-        return std::isfinite(p[0]) && p[0] > 0.0 && std::isfinite(p[1]) && p[1] > 0.0 && std::isfinite(p[2]) &&
-               p[2] >= 0.0 && std::isfinite(p[3]) && p[3] >= 0.0;
-    case TMPM_MAT_SNOW:
-        return valid_elasticity(p[0], p[1]) && std::isfinite(p[2]) && p[2] >= 0.0 && p[2] < 1.0 &&
-               std::isfinite(p[3]) && p[3] >= 0.0 && std::isfinite(p[4]) && p[4] >= 0.0;
-    default:
-        return false;
-    }
-}
-
-// MaterialModel::timestep_bound_with_deformation (material.rs:378-426)
-double timestep_bound(int kind, const double *p, double density, const double *v, double h, double det_f) {
-    double speed = std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
-    double lambda, mu, wave;
-    if (kind == TMPM_MAT_SAND_NEO_HOOKEAN) {
-        lame(p[0], p[1], lambda, mu);
-        double rho = density / std::max(det_f, 1e-6);
-        double ws = std::sqrt((lambda + 2.0 * mu) / rho);
-        return 0.5 * h / std::max(ws, speed);
-    }
-    if (kind == TMPM_MAT_FLUID) {
-        wave = std::sqrt(p[0] * p[1] / std::max(density, 1e-12));
-    } else {
-        lame(p[0], p[1], lambda, mu);
-        wave = std::sqrt((lambda + 2.0 * mu) / std::max(density, 1e-12));
-    }
-    return 0.4 * h / std::max(wave + speed, 1e-12);
-}
-
-bool finite_particle(const HostWorld &w, size_t i) {  // world.rs:505-515
-    for (int k = 0; k < 3; ++k)
-        if (!std::isfinite(w.pos[3 * i + k]) || !std::isfinite(w.vel[3 * i + k]) || !std::isfinite(w.force[3 * i + k]))
-            return false;
-    for (int k = 0; k < 9; ++k)
-        if (!std::isfinite(w.F[9 * i + k]) || !std::isfinite(w.C[9 * i + k])) return false;
-    return std::isfinite(w.mass[i]) && std::isfinite(w.vol[i]) && std::isfinite(w.radius[i]) &&
-           std::isfinite(w.damping[i]);
-}
-
-bool valid_particle(const HostWorld &w, size_t i) {  // world.rs:492-503
-    const double *pl = &w.plastic[3 * i];
-    return finite_particle(w, i) && w.mass[i] > 0.0 && w.vol[i] > 0.0 && w.radius[i] > 0.0 &&
-           material_valid(w.material[i], &w.mparams[5 * i]) && w.damping[i] >= 0.0 && std::isfinite(pl[0]) &&
-           pl[0] > 0.0 && std::isfinite(pl[1]) && std::isfinite(pl[2]);
-}
-
-bool params_valid(const TmpmParams &p) {  // world.rs:51-65
-    if (!std::isfinite(p.cell_width) || p.cell_width <= 0.0 || !std::isfinite(p.max_substep) || p.max_substep <= 0.0)
-        return false;
-    for (int k = 0; k < 3; ++k)
-        if (!std::isfinite(p.gravity[k])) return false;
-    if (p.has_bounds) {
-        for (int k = 0; k < 3; ++k)
-            if (!std::isfinite(p.bounds_min[k]) || !std::isfinite(p.bounds_max[k]) || !(p.bounds_max[k] - p.bounds_min[k] > 0.0))
-                return false;
-    }
-    return p.wall_mode == 0 || p.wall_mode == 1;
-}
-
-double stable_timestep(const HostWorld &w, const TmpmParams &p) {  // world.rs:288-303
-    std::vector<double> part(host_threads() + 1, p.max_substep);
-    parallel_chunks(w.n, [&](size_t c, size_t lo, size_t hi) {
-        double dt = p.max_substep;
-        for (size_t i = lo; i < hi; ++i) {
-            if (!w.enabled[i] || w.fixed[i]) continue;
-            dt = std::min(dt, timestep_bound(w.material[i], &w.mparams[5 * i], w.mass[i] / w.vol[i], &w.vel[3 * i],
-                                             p.cell_width, det9(&w.F[9 * i])));
-        }
-        part[c] = dt;
-    });
-    double dt = p.max_substep;
-    for (double d : part) dt = std::min(dt, d);
-    return std::min(dt, p.max_substep);
-}
-
-// RigidObstacle::is_valid (obstacle.rs:264-341)
-bool obstacle_valid(const TmpmObstacle &o) {
-    auto fin = [](double v) { return std::isfinite(v); };
-    const double *d = o.dims;
-    bool shape_ok = false;
-    switch (o.shape) {
-    case TMPM_SHAPE_SPHERE:
-        shape_ok = fin(d[0]) && d[0] > 0.0;
-        break;
-    case TMPM_SHAPE_BOX:
-        shape_ok = fin(d[0]) && d[0] > 0 && fin(d[1]) && d[1] > 0 && fin(d[2]) && d[2] > 0;
-        break;
-    case TMPM_SHAPE_CAPSULE:
-        shape_ok = fin(d[0]) && d[0] >= 0.0 && fin(d[1]) && d[1] >= 0.0 && (d[0] > 0.0 || d[1] > 0.0);
-        break;
-    case TMPM_SHAPE_CYLINDER:
-    case TMPM_SHAPE_CONE:
-    case TMPM_SHAPE_GROUND:
-        shape_ok = fin(d[0]) && d[0] > 0.0 && fin(d[1]) && d[1] > 0.0;
-        break;
-    case TMPM_SHAPE_TRIANGLE_PRISM: {
-        const double *v = o.vertices;
-        double e1[3] = {v[3] - v[0], v[4] - v[1], v[5] - v[2]}, e2[3] = {v[6] - v[0], v[7] - v[1], v[8] - v[2]};
-        double c[3] = {e1[1] * e2[2] - e1[2] * e2[1], e1[2] * e2[0] - e1[0] * e2[2], e1[0] * e2[1] - e1[1] * e2[0]};
-        double area_sq = c[0] * c[0] + c[1] * c[1] + c[2] * c[2];
-        bool verts_ok = true;
-        for (int k = 0; k < 9; ++k) verts_ok = verts_ok && fin(v[k]);
-        shape_ok = fin(d[0]) && d[0] > 0.0 && verts_ok && fin(area_sq) && area_sq > 1e-24;
-        break;
-    }
-    case TMPM_SHAPE_CONVEX: {
-        shape_ok = o.plane_count >= 4 && o.planes != nullptr && fin(o.bound_radius) && o.bound_radius > 0.0;
-        for (uint32_t i = 0; shape_ok && i < o.plane_count; ++i) {
-            const double *pl = o.planes + 4 * i;
-            bool f = fin(pl[0]) && fin(pl[1]) && fin(pl[2]) && fin(pl[3]);
-            double n2 = std::fma(pl[0], pl[0], std::fma(pl[1], pl[1], pl[2] * pl[2]));
-            shape_ok = f && std::fabs(n2 - 1.0) <= 1e-4;
-        }
-        break;
-    }
-    default:
-        shape_ok = false;
-    }
-    bool cpic_ok = o.cpic_group < 0 || (o.cpic_group < 32 && o.shape == TMPM_SHAPE_TRIANGLE_PRISM);
-    bool rest = o.boundary >= 0 && o.boundary <= 4 && fin(o.friction) && o.friction >= 0.0;
-    for (int k = 0; k < 3; ++k)
-        rest = rest && fin(o.center[k]) && fin(o.linear_velocity[k]) && fin(o.angular_velocity[k]);
-    for (int k = 0; k < 4; ++k) rest = rest && fin(o.orientation[k]);
-    return shape_ok && cpic_ok && rest;
-}
-
-bool f32_ok(double v, float &out) {  // finite_f32 (gpu.rs:1992-1999)
-    out = static_cast<float>(v);
-    return std::isfinite(out);
-}
-
-// ------------------------------------------------------------ device memory
-
-template <typename T>
-struct DevBuf {
-    T *ptr = nullptr;
-    size_t count = 0;
-    cudaError_t alloc(size_t n) {
-        release();
-        if (n == 0) n = 1;
-        cudaError_t e = cudaMalloc(reinterpret_cast<void **>(&ptr), n * sizeof(T));
-        if (e == cudaSuccess) count = n;
-        else ptr = nullptr;
-        return e;
-    }
-    void release() {
-        if (ptr) cudaFree(ptr);
-        ptr = nullptr;
-        count = 0;
-    }
-    ~DevBuf() { release(); }
-    DevBuf() = default;
-    DevBuf(const DevBuf &) = delete;
-    DevBuf &operator=(const DevBuf &) = delete;
-};
-
-struct PinnedBuf {
-    void *ptr = nullptr;
-    size_t bytes = 0;
-    bool ensure(size_t b) {
-        if (b <= bytes) return true;
-        release();
-        if (cudaMallocHost(&ptr, b) != cudaSuccess) {
-            ptr = nullptr;
-            return false;
-        }
-        bytes = b;
-        return true;
-    }
-    void release() {
-        if (ptr) cudaFreeHost(ptr);
-        ptr = nullptr;
-        bytes = 0;
-    }
-    ~PinnedBuf() { release(); }
-};
-
-struct ParticleBuffers {
-    DevBuf<float> x, v, C, F, pl;
-    DevBuf<uint32_t> cls, widx;
-    size_t cap = 0;
-    cudaError_t alloc(size_t c) {
-        cudaError_t e;
-        if ((e = x.alloc(3 * c)) || (e = v.alloc(3 * c)) || (e = C.alloc(9 * c)) || (e = F.alloc(9 * c)) ||
-            (e = pl.alloc(3 * c)) || (e = cls.alloc(c)) || (e = widx.alloc(c)))
-            return e;
-        cap = c;
-        return cudaSuccess;
-    }
-    ParticleSoA view(float *force, size_t force_stride) const {
-        ParticleSoA p;
-        p.x = x.ptr;
-        p.v = v.ptr;
-        p.C = C.ptr;
-        p.F = F.ptr;
-        p.pl = pl.ptr;
-        p.force = force;
-        p.cls = cls.ptr;
-        p.widx = widx.ptr;
-        p.cap = cap;
-        p.force_stride = force_stride;
-        return p;
-    }
-};
-
-struct GridBuffers {
-    DevBuf<unsigned long long> keys;
-    DevBuf<uint32_t> vals, count;
-    DevBuf<float4> pool;
-    DevBuf<int4> coords;
-    uint32_t capacity = 0, max_blocks = 0;
-    cudaError_t alloc(uint32_t blocks) {
-        uint32_t cap = 1024;
-        while (cap < 2u * blocks) cap <<= 1;
-        cudaError_t e;
-        if ((e = keys.alloc(cap)) || (e = vals.alloc(cap)) || (e = count.alloc(1)) ||
-            (e = pool.alloc(static_cast<size_t>(blocks) * kNodesPerBlock)) || (e = coords.alloc(blocks)))
-            return e;
-        capacity = cap;
-        max_blocks = blocks;
-        return cudaSuccess;
-    }
-    GridTable view() const {
-        GridTable g;
-        g.keys = keys.ptr;
-        g.vals = vals.ptr;
-        g.count = count.ptr;
-        g.pool = pool.ptr;
-        g.coords = coords.ptr;
-        g.mask = capacity - 1;
-        g.max_blocks = max_blocks;
-        return g;
-    }
-};
-
-// Device material codes, as the reference packs them (gpu.rs:1171-1276).
-int class_kind(int material) {
-    switch (material) {
-    case TMPM_MAT_NEO_HOOKEAN:
-        return kMatNeoHookean;
-    case TMPM_MAT_FLUID:
-        return kMatFluid;
-    case TMPM_MAT_ELASTIC:
-        return kMatCorotated;
-    case TMPM_MAT_SNOW:
-        return kMatSnow;
-    case TMPM_MAT_SAND:
-        return kMatSand;
-    case TMPM_MAT_SAND_NEO_HOOKEAN:
-        return kMatSandNeoHookean;
-    default:
-        return 0;
-    }
-}
-
-}  // namespace
 
 void tmpm::set_last_error(const std::string &msg) { g_last_error = msg; }
 
@@ -594,24 +88,11 @@ struct TmpmSession {
 
     SimParams sim_params(double dt, bool resident) const {
         SimParams sp{};
-        float h = static_cast<float>(params.cell_width);
-        sp.h = h;
-        sp.inv_h = 1.0f / h;
-        sp.inv_d = static_cast<float>(4.0 / (params.cell_width * params.cell_width));
-        sp.dt = static_cast<float>(dt);
-        sp.gx = static_cast<float>(params.gravity[0]);
-        sp.gy = static_cast<float>(params.gravity[1]);
-        sp.gz = static_cast<float>(params.gravity[2]);
-        sp.has_bounds = params.has_bounds ? 1 : 0;
-        sp.wall_mode = params.wall_mode;
-        for (int k = 0; k < 3; ++k) {
-            sp.bmin[k] = static_cast<float>(params.bounds_min[k]);
-            sp.bmax[k] = static_cast<float>(params.bounds_max[k]);
-            // gpu.wgsl:962-965: floor(bound * inv_h - 0.5) -/+ 2 in f32
-            float lo = std::floor(sp.bmin[k] * sp.inv_h - 0.5f), hi = std::floor(sp.bmax[k] * sp.inv_h - 0.5f);
-            sp.first_base[k] = static_cast<int>(std::max(lo, -1.0e9f)) - 2;
-            sp.last_base[k] = static_cast<int>(std::min(hi, 1.0e9f)) + 2;
-        }
+        sp.s0 = scene_params(params, dt);
+        sp.scenes = nullptr;
+        sp.scene_status = nullptr;
+        sp.multi = 0;
+        sp.step_index = 0;
         sp.num_obstacles = static_cast<int>(obstacles.size());
         sp.reactions = 0;
         sp.apply_force = 0;
@@ -640,206 +121,31 @@ struct TmpmSession {
         float inv_h = 1.0f / h32;
         if (!std::isfinite(inv_h)) return fail(TMPM_ERR_INVALID_INPUT, "1 / cell width not representable in f32");
 
-        // Packing runs in two parallel passes over contiguous particle chunks:
-        // pass 1 validates, builds per-chunk class tables and block lists and
-        // counts enabled particles; pass 2 writes the f32 arrays (component-
-        // major with stride `cap`) straight into pinned memory at compacted
-        // positions.  Results equal a serial pass in world order.
-        const size_t N = world.n;
-        struct ChunkOut {
-            size_t first_bad = std::numeric_limits<size_t>::max();
-            TmpmStatus st = TMPM_OK;
-            const char *msg = "";
-            size_t enabled = 0;
-            std::vector<DevClass> classes;
-            std::vector<unsigned long long> blocks;
-        };
-        const unsigned T = host_threads();
-        std::vector<ChunkOut> co(T + 1);
-        std::vector<uint32_t> lcls(std::max<size_t>(N, 1));
-        parallel_chunks(N, [&](size_t c, size_t lo, size_t hi) {
-            ChunkOut &o = co[c];
-            std::unordered_map<std::string, uint32_t> index;
-            DevClass last{};
-            uint32_t last_ci = kClassMask;
-            unsigned long long last_block = ~0ull;
-            auto bad = [&](size_t i, TmpmStatus st, const char *msg) {
-                o.first_bad = i;
-                o.st = st;
-                o.msg = msg;
-            };
-            for (size_t i = lo; i < hi; ++i) {
-                float f4[4];
-                for (int k = 0; k < 3; ++k)
-                    if (!f32_ok(world.pos[3 * i + k], f4[k]) || !f32_ok(world.vel[3 * i + k], f4[3]) ||
-                        !f32_ok(world.force[3 * i + k], f4[3]))
-                        return bad(i, TMPM_ERR_INVALID_INPUT, "particle state not representable in f32");
-                float m32, v32, r32, d32;
-                if (!f32_ok(world.enabled[i] ? world.mass[i] : 0.0, m32) || !f32_ok(world.vol[i], v32) ||
-                    !f32_ok(world.radius[i], r32) || !f32_ok(world.damping[i], d32))
-                    return bad(i, TMPM_ERR_INVALID_INPUT, "particle scalars not representable in f32");
-                if (world.enabled[i] && (m32 <= 0.0f || v32 <= 0.0f))
-                    return bad(i, TMPM_ERR_INVALID_INPUT, "particle mass or volume underflows f32");
-                if (r32 <= 0.0f || world.damping[i] < 0.0)
-                    return bad(i, TMPM_ERR_INVALID_INPUT, "particle radius or damping invalid");
-                for (int k = 0; k < 9; ++k) {
-                    float t;
-                    if (!f32_ok(world.F[9 * i + k], t) || !f32_ok(world.C[9 * i + k], t))
-                        return bad(i, TMPM_ERR_INVALID_INPUT, "particle matrices not representable in f32");
-                }
-                if (!world.enabled[i]) continue;
-                int base[3];
-                for (int k = 0; k < 3; ++k) {
-                    float xk = static_cast<float>(world.pos[3 * i + k]);
-                    float cf = std::floor(xk * inv_h - 0.5f);
-                    if (!std::isfinite(cf) || cf < -131000.0f || cf > 131000.0f)
-                        return bad(i, TMPM_ERR_INVALID_INPUT, "particle cell outside the representable grid");
-                    base[k] = static_cast<int>(cf);
-                }
-                int kind = class_kind(world.material[i]);
-                const double *mp = &world.mparams[5 * i];
-                if (kind == kMatCorotated || kind == kMatSand || kind == kMatSnow) {
-                    // use_cpu_corotated (gpu.rs:1156-1170): ill-conditioned F is a CPU case
-                    const double *Fm = &world.F[9 * i];
-                    double nrm = fro9(Fm), inrm = std::numeric_limits<double>::infinity();
-                    inverse_norm9(Fm, inrm);
-                    if (std::fabs(det9(Fm)) < 1e-5 || !(nrm >= 1e-5 && nrm <= 20.0) || nrm * inrm > 100.0) kind = 0;
-                }
-                if (kind == 0)
-                    return bad(i, TMPM_ERR_RESIDENT_UNAVAILABLE,
-                               "particle material or deformation needs the CPU path (plastic material or "
-                               "ill-conditioned F)");
-                DevClass k{};
-                k.mass = m32;
-                k.volume = v32;
-                k.radius = r32;
-                k.damping = d32;
-                k.kind = kind;
-                k.color = world.color[i];
-                float rho = std::max(m32 / v32, 1e-12f);
-                if (kind == kMatFluid) {
-                    float b, g, vi, te;
-                    if (!f32_ok(mp[0], b) || !f32_ok(mp[1], g) || !f32_ok(mp[2], vi) || !f32_ok(mp[3], te))
-                        return bad(i, TMPM_ERR_INVALID_INPUT, "fluid parameters not representable in f32");
-                    k.p0 = b;
-                    k.p1 = g;
-                    k.p2 = vi;
-                    k.p3 = te;
-                    k.wave = std::sqrt(b * g / rho);
-                } else {
-                    double lambda, mu;
-                    lame(mp[0], mp[1], lambda, mu);
-                    float l32, m32b;
-                    if (!f32_ok(lambda, l32) || !f32_ok(mu, m32b))
-                        return bad(i, TMPM_ERR_INVALID_INPUT, "Lame parameters not representable in f32");
-                    k.p0 = l32;
-                    k.p1 = m32b;
-                    k.wave = std::sqrt((l32 + 2.0f * m32b) / rho);
-                    // sand / NH sand: friction angle, cohesion; snow: hardening, critical compression, stretch
-                    bool ok = true;
-                    if (kind == kMatSand || kind == kMatSandNeoHookean) {
-                        ok = f32_ok(mp[2], k.p2) && f32_ok(mp[3], k.p3);
-                    } else if (kind == kMatSnow) {
-                        ok = f32_ok(mp[4], k.p2) && f32_ok(mp[2], k.p3) && f32_ok(mp[3], k.p4);
-                    }
-                    float t3;
-                    if (kind >= kMatSnow)
-                        for (int q = 0; q < 3; ++q) ok = ok && f32_ok(world.plastic[3 * i + q], t3);
-                    if (!ok) return bad(i, TMPM_ERR_INVALID_INPUT, "plastic parameters not representable in f32");
-                }
-                uint32_t ci;
-                if (last_ci != kClassMask && std::memcmp(&k, &last, sizeof(DevClass)) == 0) {
-                    ci = last_ci;
-                } else {
-                    std::string key(reinterpret_cast<const char *>(&k), sizeof(DevClass));
-                    auto it = index.find(key);
-                    if (it == index.end()) {
-                        ci = static_cast<uint32_t>(o.classes.size());
-                        o.classes.push_back(k);
-                        index.emplace(std::move(key), ci);
-                    } else {
-                        ci = it->second;
-                    }
-                    last = k;
-                    last_ci = ci;
-                }
-                lcls[i] = ci;
-                unsigned long long hb =
-                    (static_cast<unsigned long long>(world.color[i]) << 48) |
-                    (static_cast<unsigned long long>(static_cast<uint32_t>((base[0] >> 2) + kBlockBias) & 0xFFFF) << 32) |
-                    (static_cast<unsigned long long>(static_cast<uint32_t>((base[1] >> 2) + kBlockBias) & 0xFFFF) << 16) |
-                    static_cast<unsigned long long>(static_cast<uint32_t>((base[2] >> 2) + kBlockBias) & 0xFFFF);
-                if (hb != last_block) {
-                    o.blocks.push_back(hb);
-                    last_block = hb;
-                }
-                ++o.enabled;
-            }
-            std::sort(o.blocks.begin(), o.blocks.end());
-            o.blocks.erase(std::unique(o.blocks.begin(), o.blocks.end()), o.blocks.end());
+        // Validate and pack the world straight into pinned staging (stride `cap`).
+        ClassTable ct;
+        size_t cap = 256;
+        PackResult pr = pack_world(world, inv_h, 0u, ct, [&](size_t n_enabled) {
+            PackTarget tg;
+            cap = std::max<size_t>(256, (n_enabled + 255) / 256 * 256);
+            if (n_enabled > static_cast<size_t>(std::numeric_limits<int>::max() / 2)) return tg;
+            if (!upload_staging.ensure((27 * cap + 2 * cap) * sizeof(float))) return tg;
+            tg.base = static_cast<float *>(upload_staging.ptr);
+            tg.cls = reinterpret_cast<uint32_t *>(tg.base + 27 * cap);
+            tg.widx = tg.cls + cap;
+            tg.stride = cap;
+            return tg;
         });
-        size_t worst = std::numeric_limits<size_t>::max();
-        const ChunkOut *failed = nullptr;
-        for (const ChunkOut &o : co)
-            if (o.first_bad < worst) {
-                worst = o.first_bad;
-                failed = &o;
-            }
-        if (failed) return fail(failed->st, failed->msg);
-        // merge class tables and block lists (small), compute compacted offsets
-        std::vector<DevClass> cls_table;
-        std::unordered_map<std::string, uint32_t> cls_index;
-        std::vector<std::vector<uint32_t>> remap(co.size());
-        std::vector<size_t> offset(co.size(), 0);
-        std::vector<unsigned long long> home_blocks;
-        size_t n_enabled = 0;
-        for (size_t c = 0; c < co.size(); ++c) {
-            offset[c] = n_enabled;
-            n_enabled += co[c].enabled;
-            for (const DevClass &k : co[c].classes) {
-                std::string key(reinterpret_cast<const char *>(&k), sizeof(DevClass));
-                auto it = cls_index.find(key);
-                uint32_t gi;
-                if (it == cls_index.end()) {
-                    gi = static_cast<uint32_t>(cls_table.size());
-                    cls_table.push_back(k);
-                    cls_index.emplace(std::move(key), gi);
-                } else {
-                    gi = it->second;
-                }
-                remap[c].push_back(gi);
-            }
-            home_blocks.insert(home_blocks.end(), co[c].blocks.begin(), co[c].blocks.end());
+        if (pr.st != TMPM_OK) {
+            if (pr.st == TMPM_ERR_DEVICE && pr.enabled > static_cast<size_t>(std::numeric_limits<int>::max() / 2))
+                return fail(TMPM_ERR_CAPACITY, "too many particles for one session");
+            return fail(pr.st, pr.msg);
         }
-        if (n_enabled > static_cast<size_t>(std::numeric_limits<int>::max() / 2))
-            return fail(TMPM_ERR_CAPACITY, "too many particles for one session");
-        bool plastic_classes = false;
-        for (const DevClass &k : cls_table) plastic_classes = plastic_classes || k.kind >= kMatSnow;
-        const size_t cap = std::max<size_t>(256, (n_enabled + 255) / 256 * 256);
-        if (!upload_staging.ensure((27 * cap + 2 * cap) * sizeof(float)))
-            return fail(TMPM_ERR_DEVICE, "cudaMallocHost upload staging failed");
+        const size_t n_enabled = pr.enabled;
+        const std::vector<DevClass> &cls_table = ct.table;
+        const bool plastic_classes = ct.plastic();
         float *hx = static_cast<float *>(upload_staging.ptr);
         float *hv = hx + 3 * cap, *hC = hv + 3 * cap, *hF = hC + 9 * cap, *hpl = hF + 9 * cap;
         uint32_t *hcls = reinterpret_cast<uint32_t *>(hpl + 3 * cap), *hwidx = hcls + cap;
-        parallel_chunks(N, [&](size_t c, size_t lo, size_t hi) {
-            size_t j = offset[c];
-            const std::vector<uint32_t> &rm = remap[c];
-            for (size_t i = lo; i < hi; ++i) {
-                if (!world.enabled[i]) continue;
-                for (int k3 = 0; k3 < 3; ++k3) {
-                    hx[k3 * cap + j] = static_cast<float>(world.pos[3 * i + k3]);
-                    hv[k3 * cap + j] = static_cast<float>(world.vel[3 * i + k3]);
-                }
-                for (int k9 = 0; k9 < 9; ++k9) {
-                    hC[k9 * cap + j] = static_cast<float>(world.C[9 * i + k9]);
-                    hF[k9 * cap + j] = static_cast<float>(world.F[9 * i + k9]);
-                }
-                for (int k3 = 0; k3 < 3; ++k3) hpl[k3 * cap + j] = static_cast<float>(world.plastic[3 * i + k3]);
-                hcls[j] = rm[lcls[i]] | (world.fixed[i] ? kFixedBit : 0u);
-                hwidx[j] = static_cast<uint32_t>(i);
-                ++j;
-            }
-        });
         // obstacles (pack_obstacle, gpu.rs:2025-2166)
         std::vector<DevObstacle> dobs;
         std::vector<float> dplanes;
@@ -885,8 +191,7 @@ struct TmpmSession {
         cudaError_t e;
         if ((e = cudaSetDevice(device))) return cuda_fail(e, "cudaSetDevice");
         // block pool sizing from the number of occupied home blocks
-        std::sort(home_blocks.begin(), home_blocks.end());
-        size_t unique_blocks = std::unique(home_blocks.begin(), home_blocks.end()) - home_blocks.begin();  // small
+        size_t unique_blocks = pr.blocks.size();
         uint64_t want_blocks = options.max_blocks ? options.max_blocks : std::max<uint64_t>(4096, 16 * unique_blocks + 4096);
         if (want_blocks > (1u << 27)) want_blocks = 1u << 27;
         for (int b = 0; b < 2; ++b)
@@ -1011,7 +316,7 @@ struct TmpmSession {
             sb.hist = sort_hist.ptr;
             sb.totals = sort_totals.ptr;
             sb.cap = sort_keys[0].count;
-            launch_resort(src, dst, n_dev, sp, sb, stream);
+            launch_resort(src, dst, n_dev, n_dev, classes.ptr, sp, sb, stream);
             cur ^= 1;
             since_resort = 0;
             tock(4);
@@ -1174,29 +479,6 @@ TmpmStatus session_guard(TmpmSession *s, bool require_idle) {
     }
     if (!s->valid) return s->fail(TMPM_ERR_RESIDENT_UNAVAILABLE, "session is invalid after an earlier error");
     if (require_idle && s->pending) return s->fail(TMPM_ERR_PENDING_STEPS, "GPU MPM steps are pending; synchronize first");
-    return TMPM_OK;
-}
-
-TmpmStatus load_checked(const TmpmParticleArrays *particles, HostWorld &out, std::string &err) {
-    if (!particles || particles->count == 0) {
-        out.resize(0);
-        return TMPM_OK;
-    }
-    if (!particles->position || !particles->velocity || !particles->mass || !particles->rest_volume ||
-        !particles->radius || !particles->material || !particles->material_params) {
-        err = "required particle arrays are missing";
-        return TMPM_ERR_INVALID_INPUT;
-    }
-    out.load(*particles);
-    std::atomic<bool> bad{false};
-    parallel_for(out.n, [&](size_t lo, size_t hi) {
-        for (size_t i = lo; i < hi && !bad.load(std::memory_order_relaxed); ++i)
-            if (!valid_particle(out, i)) bad = true;
-    });
-    if (bad) {
-        err = "invalid MPM input";
-        return TMPM_ERR_MPM_INVALID_INPUT;
-    }
     return TMPM_OK;
 }
 
@@ -1516,7 +798,7 @@ TmpmStatus tmpm_debug_binning(TmpmSession *s, uint32_t *world_index_out, int32_t
     if ((e = cells.alloc(3 * static_cast<size_t>(n))) || (e = keys.alloc(n))) return s->cuda_fail(e, "cudaMalloc");
     SimParams sp = s->sim_params(s->substep_dt, true);
     ParticleSoA P = s->soa();
-    launch_bin_keys(P, n, sp, cells.ptr, keys.ptr, s->stream);
+    launch_bin_keys(P, n, s->classes.ptr, sp, cells.ptr, keys.ptr, s->stream);
     if (world_index_out) cudaMemcpyAsync(world_index_out, P.widx, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost, s->stream);
     if (base_cell_out) cudaMemcpyAsync(base_cell_out, cells.ptr, sizeof(int32_t) * 3 * n, cudaMemcpyDeviceToHost, s->stream);
     if (key_out) cudaMemcpyAsync(key_out, keys.ptr, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost, s->stream);

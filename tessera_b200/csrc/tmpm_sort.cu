@@ -138,8 +138,8 @@ __global__ void __launch_bounds__(kSortThreads) k_scatter(const uint32_t *__rest
 
 }  // namespace
 
-void radix_sort_pairs(SortBuffers &sb, int n, int bits, cudaStream_t stream) {
-    if (n <= 0) return;
+int radix_sort_pairs(SortBuffers &sb, int n, int bits, cudaStream_t stream) {
+    if (n <= 0) return 0;
     const int tiles = (n + kTile - 1) / kTile;
     int cur = 0;
     for (int shift = 0; shift < bits; shift += 8) {
@@ -149,10 +149,7 @@ void radix_sort_pairs(SortBuffers &sb, int n, int bits, cudaStream_t stream) {
                                                       shift, sb.hist, tiles, sb.totals);
         cur ^= 1;
     }
-    if (cur != 0) {
-        cudaMemcpyAsync(sb.keys[0], sb.keys[1], sizeof(uint32_t) * n, cudaMemcpyDeviceToDevice, stream);
-        cudaMemcpyAsync(sb.vals[0], sb.vals[1], sizeof(uint32_t) * n, cudaMemcpyDeviceToDevice, stream);
-    }
+    return cur;
 }
 
 }  // namespace tmpm

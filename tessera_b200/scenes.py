@@ -110,3 +110,49 @@ def sphere_drop(seed=3, n_side=8, cell_width=0.05, name="sphere-drop"):
     params = make_params(cell_width, gravity=(0.0, 0.0, -9.81), max_substep=1e-3, bounds=((0, 0, 0), (1, 1, 1)))
     obstacles = [Obstacle.sphere((0.35, 0.35, 0.4), 0.1, friction=0.3)]
     return Scene(name, params, parts, 1e-4, 20, obstacles=obstacles)
+
+
+def batch_scene(seed, cells=None, density=1000.0, dt=1e-4, substeps=100, jitter=0.5, name=None):
+    """One scene of the heterogeneous batch: a block of `cells`^3 cells (8 particles
+    per cell) in the unit cube at resolution 4 * `cells` (so the block spans a
+    quarter of the domain side), at a seeded interior position; material drawn
+    uniformly from corotated elastic (E log-uniform in [1e3, 1e5], nu = 0.2) and
+    weakly compressible fluid (K = 1e4, gamma = 7).  Without `cells` the particle
+    count is drawn log-uniform in [4096, 262144] (cells 8..32, resolution 32..128).
+
+    The density is not given with the workload; rho = 1000 keeps dt = 1e-4 under
+    the CFL bound 0.4 h / c for every draw (E = 1e5 at h = 1/128 needs rho > 114).
+    """
+    rng = np.random.default_rng(seed)
+    if cells is None:
+        n = float(np.exp(rng.uniform(np.log(4096.0), np.log(262144.0))))
+        cells = int(np.clip(round((n / 8.0) ** (1.0 / 3.0)), 8, 32))
+    res = 4 * cells
+    h = 1.0 / res
+    side = cells * h
+    lo = np.array([rng.uniform(4 * h, 1.0 - side - 4 * h) for _ in range(3)])
+    lo = np.round(lo / h) * h
+    r = h / 4.0
+    pos = lattice(lo, lo + side, 2.0 * r, rng, jitter)
+    if rng.uniform() < 0.5:
+        young = float(np.exp(rng.uniform(np.log(1e3), np.log(1e5))))
+        parts = density_particles(pos, r, density, MAT_ELASTIC, (young, 0.2))
+        material = dict(material="elastic", young=young)
+    else:
+        parts = density_particles(pos, r, density, MAT_FLUID, (1e4, 7.0, 0.01, 0.25))
+        material = dict(material="fluid", bulk=1e4)
+    params = make_params(h, gravity=(0.0, 0.0, -9.8), max_substep=1e-3, bounds=((0, 0, 0), (1, 1, 1)))
+    return Scene(name or f"batch-scene-{seed}", params, parts, dt, substeps,
+                 info=dict(particles=len(pos), resolution=res, **material))
+
+
+def batch_scenes(count=256, seed=3, max_cells=None, dt=1e-4, substeps=100):
+    """The heterogeneous batch: `count` independent scenes seeded seed*1000 + k.
+    `max_cells` caps the block size (small test batches)."""
+    out = []
+    for k in range(count):
+        sc = batch_scene(seed * 1000 + k, dt=dt, substeps=substeps)
+        if max_cells is not None and sc.info["resolution"] // 4 > max_cells:
+            sc = batch_scene(seed * 1000 + k, cells=max_cells, dt=dt, substeps=substeps)
+        out.append(sc)
+    return out
