@@ -13,6 +13,13 @@ maximum, gpu.rs:303-322) over the whole scene.
          uploads the particle state from host arrays, runs 64 substeps and
          reads the state back into host f64 arrays (tmpm_write_particles +
          tmpm_step).
+  batched  256 heterogeneous scenes (4k-256k particles, resolution 32-128,
+         elastic or fluid, dt = 1e-4, 100 substeps) advanced in one multi-scene
+         batch against the same scenes one at a time through single-scene
+         sessions: device-timed and end to end (host arrays in, results out).
+  serving  Poisson arrivals of dam-break-sized requests (50-400 substeps) into
+         the continuous-batching server under a 120 GB footprint budget, against
+         the one-scene-at-a-time loop: p50/p99 time-to-result and throughput.
 
 `--impl reference` times the reference's CPU path (its C++ restatement in
 oracle/, f64, ordered-map grid) on the host cores for the same workload.
@@ -36,20 +43,25 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 BATCH = 64
-# re-sort per batch: bin keys, 4 radix passes x (hist, scan, scatter), gather
-RESORT_LAUNCHES = 1 + 4 * 3 + 1
+# re-sort per batch: bin keys, 3 radix passes (21-bit keys) x (hist, scan, scatter), gather
+RESORT_LAUNCHES = 1 + 3 * 3 + 1
 METRIC = "particle-substeps/s"
 
 
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=30)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="tessera", choices=["tessera", "reference"])
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--scale", type=float, default=1.0, help="column footprint scale (1.0 = full config)")
+    ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--batched-scenes", type=int, default=256)
+    ap.add_argument("--no-serving", action="store_true")
+    ap.add_argument("--serve-rates", default="200", help="comma-separated arrival rates (requests/s)")
+    ap.add_argument("--serve-requests", type=int, default=12)
     return ap.parse_args()
 
 
@@ -109,24 +121,39 @@ class ClockSampler:
         self.proc = None
 
     def __enter__(self):
+        import threading
+
+        self.lines = []
+        self.first = threading.Event()
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
                  "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except (FileNotFoundError, OSError):
             self.proc = None
+            return self
+
+        def reader():
+            for ln in self.proc.stdout:
+                if ln.strip():
+                    self.lines.append(ln)
+                    self.first.set()
+            self.first.set()
+
+        self.thread = threading.Thread(target=reader, daemon=True)
+        self.thread.start()
+        self.first.wait(timeout=10.0)  # start timing once sampling runs
         return self
 
     def __exit__(self, *exc):
-        self.lines = []
         if self.proc is not None:
             self.proc.terminate()
             try:
-                out, _ = self.proc.communicate(timeout=5)
+                self.proc.wait(timeout=5)
             except subprocess.TimeoutExpired:
                 self.proc.kill()
-                out, _ = self.proc.communicate()
-            self.lines = [ln for ln in out.splitlines() if ln.strip()]
+                self.proc.wait()
+            self.thread.join(timeout=5)
 
     def summary(self):
         sm, mx, reasons = [], None, set()
@@ -171,6 +198,102 @@ def cpu_baseline(scene_fn, target_seconds=15.0):
     return {"value": value, "unit": METRIC, "cores": threads, "kind": "port",
             "sample": f"{sample.particles.count} particles of the same scene (column footprint x0.1, same h, dt, "
                       f"materials) x {substeps} substeps, {threads} independent copies in parallel, {el:.1f} s"}
+
+
+def bench_batched(count: int) -> dict:
+    """256 heterogeneous scenes x 100 substeps: one multi-scene batch against one
+    session per scene, on the same device."""
+    import torch
+
+    from tessera_b200 import scenes
+    from tessera_b200.batch import Batch, PreparedScene
+    from tessera_b200.session import Session
+
+    scs = scenes.batch_scenes(count)
+    steps = scs[0].substeps
+    n = sum(s.particles.count for s in scs)
+    work = float(n) * steps
+    # batched, end to end: host arrays -> admission -> 100 substeps -> positions/velocities back
+    b = Batch()
+    b.add_scene(scs[0].params, scs[0].particles, scs[0].dt)  # warm the pinned pool and the context
+    b.close()
+    torch.cuda.synchronize()
+    from concurrent.futures import ThreadPoolExecutor
+
+    t0 = time.perf_counter()
+    b = Batch()
+    with ThreadPoolExecutor(max_workers=8) as pool:  # preparation is host work, thread-safe
+        prepared = list(pool.map(lambda s: PreparedScene(s.params, s.particles, s.dt), scs))
+    ids = [b.admit(p) for p in prepared]
+    b.run({i: steps for i in ids}, collect=ids)
+    outs = [b.read(i) for i in ids]
+    e2e_batched = time.perf_counter() - t0
+    assert all(np.all(np.isfinite(o["position"])) for o in outs)
+    # batched, device-resident: further batches of the same scenes (graph replays)
+    dev = []
+    for _ in range(3):
+        b.run({i: steps for i in ids})
+        dev.append(b.last_ms())
+    fails = sum(b.status(i) != 0 for i in ids)
+    b.close()
+    # plain: one scene at a time through a single-scene session each
+    plain_dev = 0.0
+    t0 = time.perf_counter()
+    for s in scs:
+        ses = Session(s.params, s.particles, s.dt)
+        left = steps
+        while left:
+            k = min(BATCH, left)
+            ms, _ = ses.bench_substeps(k)
+            ses.synchronize()
+            plain_dev += ms
+            left -= k
+        ses.read()
+        ses.close()
+    e2e_plain = time.perf_counter() - t0
+    batched_dev = float(np.median(dev))
+    return {
+        "workload": "config3-heterogeneous-batch", "scenes": count, "particles": n, "substeps": steps, "dt": scs[0].dt,
+        "materials": {"elastic": sum(s.info["material"] == "elastic" for s in scs),
+                      "fluid": sum(s.info["material"] == "fluid" for s in scs)},
+        "batched": {"value": work / (batched_dev / 1e3), "ms_per_batch": batched_dev, "failed_scenes": fails,
+                    "e2e": work / e2e_batched, "e2e_seconds": e2e_batched, "graph_replay": True},
+        "plain": {"value": work / (plain_dev / 1e3), "device_ms": plain_dev, "e2e": work / e2e_plain,
+                  "e2e_seconds": e2e_plain},
+        "speedup_device": plain_dev / batched_dev, "speedup_e2e": e2e_plain / e2e_batched, "unit": METRIC,
+        "timing": "value: CUDA events around each batch (plain: sum over sessions of CUDA-event time of their "
+                  "substeps); e2e: wall clock from host arrays to positions/velocities back on the host",
+    }
+
+
+def bench_serving(rates, count: int) -> dict:
+    """Poisson arrivals of dam-break requests (50-400 substeps) into the
+    continuous-batching server (120 GB budget) and into the one-scene-at-a-time loop."""
+    from tessera_b200 import scenes
+    from tessera_b200.batch import Batch
+    from tessera_b200.serve import Request, Server, poisson_arrivals, run_plain, summarize
+
+    pool = [scenes.dam_break(seed=100 + k) for k in range(4)]  # distinct seeded cube positions
+    rng = np.random.default_rng(7)
+    steps = [int(rng.integers(50, 401)) for _ in range(count)]
+    out = {"workload": "config4-serving", "requests_per_rate": count, "scene": "config2 dam break (4 seeded variants)",
+           "particles_per_request": pool[0].particles.count, "substeps": "uniform 50-400 (seeded)",
+           "hbm_budget_gb": 120, "chunk_substeps": 32, "unit": METRIC, "rates": []}
+    for rate in rates:
+        t = poisson_arrivals(rate, count, seed=int(rate))
+        reqs = [Request(k, float(t[k] - t[0]), pool[k % len(pool)], steps[k]) for k in range(count)]
+        server = Server(batch=Batch(particle_capacity=sum(r.scene.particles.count for r in reqs)), chunk=32,
+                        hbm_budget=120e9)
+        served, span = server.run(reqs)
+        s_served = summarize(served, span)
+        s_served.update(batches=server.batches, peak_resident=server.peak_resident,
+                        peak_gb=server.peak_bytes / 1e9)
+        server.batch.close()
+        plain, span_p = run_plain(reqs)
+        s_plain = summarize(plain, span_p)
+        out["rates"].append({"rate": rate, "served": s_served, "plain": s_plain,
+                             "throughput_ratio": s_served["particle_substeps_per_s"] / s_plain["particle_substeps_per_s"]})
+    return out
 
 
 def run_reference(args, world, rank):
@@ -276,6 +399,12 @@ def run_tessera(args, world, rank, local):
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(scenes.dam_break)
     clk = clocks.summary()
+    session.close()
+    batched = serving = None
+    if rank == 0 and world == 1 and not args.no_batched:
+        batched = bench_batched(args.batched_scenes)
+    if rank == 0 and world == 1 and not args.no_serving:
+        serving = bench_serving([float(r) for r in args.serve_rates.split(",") if r], args.serve_requests)
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
@@ -290,9 +419,10 @@ def run_tessera(args, world, rank, local):
             "cpu_baseline": cpu,
             "e2e": e2e,
             "clocks": clk,
+            "batched": batched,
+            "serving": serving,
         }
         print(json.dumps(line), flush=True)
-    session.close()
 
 
 def main():

@@ -353,3 +353,17 @@ def obstacles_to_c(obstacles):
         arr[i] = c
     arr._keep = keep
     return arr, len(obstacles)
+
+
+def partial_arrays(count: int, fields=("position", "velocity")):
+    """A C view that receives only `fields` (other pointers NULL) and the numpy arrays behind it."""
+    c = TmpmParticleArrays()
+    c.count = count
+    arrays = {}
+    for name in fields:
+        dtype, width = PARTICLE_FIELDS[name]
+        a = np.zeros((count,) if width == 1 else (count, width), dtype=dtype)
+        arrays[name] = a
+        setattr(c, name, a.ctypes.data if count else None)
+    c._keep = arrays
+    return c, arrays

@@ -14,7 +14,7 @@ import ctypes as C
 import numpy as np
 
 from . import _native
-from ._abi import STATUS_MESSAGES, TMPM_OK, ParticleArrays, TmpmBatchOptions, TmpmParams
+from ._abi import STATUS_MESSAGES, TMPM_OK, ParticleArrays, TmpmBatchOptions, TmpmParams, partial_arrays
 from .session import TesseraError
 
 MAX_SCENES = 256
@@ -37,8 +37,9 @@ def home_blocks(position: np.ndarray, cell_width: float) -> int:
     """Occupied 4^3 blocks of a scene (the block-pool sizing input), from f32 base cells."""
     x = np.asarray(position, dtype=np.float32)
     inv_h = np.float32(1.0) / np.float32(cell_width)
-    base = np.floor(x * inv_h - np.float32(0.5)).astype(np.int64) >> 2
-    return int(len(np.unique(base, axis=0)))
+    base = (np.floor(x * inv_h - np.float32(0.5)).astype(np.int64) >> 2) + (1 << 20)
+    keys = (base[:, 0] << 42) | (base[:, 1] << 21) | base[:, 2]
+    return int(len(np.unique(keys)))
 
 
 class PreparedScene:
@@ -158,6 +159,12 @@ class Batch:
         arrays = out.as_c()
         _check(_native.lib().tmpm_batch_read_scene(self._h, int(scene), C.byref(arrays)), self._h)
         return out
+
+    def read(self, scene: int, fields=("position", "velocity")) -> dict:
+        """Only the named fields of a scene's particles (world order), as numpy arrays."""
+        c, arrays = partial_arrays(self.count(scene), fields)
+        _check(_native.lib().tmpm_batch_read_scene(self._h, int(scene), C.byref(c)), self._h)
+        return arrays
 
     def last_ms(self) -> float:
         return float(_native.lib().tmpm_batch_last_ms(self._h))

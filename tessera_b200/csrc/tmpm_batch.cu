@@ -722,7 +722,9 @@ struct TmpmBatch {
             remap[k] = classes.intern(c);
         }
         if (classes.table.size() > kClassMask) {
-            classes.table.resize(before);  // (index entries past `before` are harmless: re-interned on use)
+            classes.table.resize(before);
+            for (auto it = classes.index.begin(); it != classes.index.end();)
+                it = it->second >= before ? classes.index.erase(it) : std::next(it);
             return fail(TMPM_ERR_CAPACITY, "too many distinct particle classes");
         }
         const size_t stride = std::max<size_t>(p->m, 1);

@@ -50,14 +50,38 @@ inline void parallel_for(size_t n, Fn fn) {
 
 // --------------------------------------------------------------- host world
 
+// Allocator whose value-less construct leaves elements uninitialised: resizing a
+// host-world array then neither zero-fills nor touches its pages on the calling
+// thread; the parallel loaders write (and first-touch) every element.
+template <typename T>
+struct NoInitAlloc : std::allocator<T> {
+    template <typename U>
+    struct rebind {
+        using other = NoInitAlloc<U>;
+    };
+    NoInitAlloc() = default;
+    template <typename U>
+    NoInitAlloc(const NoInitAlloc<U> &) noexcept {}
+    template <typename U>
+    void construct(U *p) noexcept {
+        ::new (static_cast<void *>(p)) U;
+    }
+    template <typename U, typename... Args>
+    void construct(U *p, Args &&...args) {
+        ::new (static_cast<void *>(p)) U(std::forward<Args>(args)...);
+    }
+};
+template <typename T>
+using HostVec = std::vector<T, NoInitAlloc<T>>;
+
 struct HostWorld {
     size_t n = 0;
-    std::vector<double> pos, vel, F, C, force, mass, vol, radius, damping, plastic, mparams;
-    std::vector<int32_t> material;
-    std::vector<uint8_t> enabled, fixed;
-    std::vector<uint16_t> color;
-    std::vector<uint32_t> group;
-    std::vector<uint64_t> chunk;
+    HostVec<double> pos, vel, F, C, force, mass, vol, radius, damping, plastic, mparams;
+    HostVec<int32_t> material;
+    HostVec<uint8_t> enabled, fixed;
+    HostVec<uint16_t> color;
+    HostVec<uint32_t> group;
+    HostVec<uint64_t> chunk;
 
     // Sizes every field for `count` particles; existing storage is reused and
     // not cleared (load() writes every element).

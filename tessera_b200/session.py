@@ -15,7 +15,7 @@ import numpy as np
 
 from . import _native
 from ._abi import (
-    STATUS_MESSAGES, TMPM_OK, ParticleArrays, TmpmParams, TmpmSessionOptions, obstacles_to_c,
+    STATUS_MESSAGES, TMPM_OK, ParticleArrays, TmpmParams, TmpmSessionOptions, obstacles_to_c, partial_arrays,
 )
 
 
@@ -122,6 +122,12 @@ class Session:
         arrays = out.as_c()
         _check(_native.lib().tmpm_read_particles(self._h, C.byref(arrays)), self._h)
         return out
+
+    def read(self, fields=("position", "velocity")) -> dict:
+        """Only the named fields of the world's particles, as numpy arrays."""
+        c, arrays = partial_arrays(self.count(), fields)
+        _check(_native.lib().tmpm_read_particles(self._h, C.byref(c)), self._h)
+        return arrays
 
     def write_particles(self, particles: ParticleArrays) -> None:
         arrays = particles.as_c()
