@@ -349,6 +349,39 @@ size_t tmpm_batch_scene_bytes(size_t particles, size_t home_blocks);
 
 const char *tmpm_batch_last_error_message(const TmpmBatch *batch);
 
+/* ------------------------- differentiable rollout ------------------------- */
+
+/* No counterpart in the reference (tessera-mpm has no adjoint).  A rollout of
+ * `substeps` fixed substeps of MpmWorld::substep (world.rs:361-467) for
+ * corotated elastic particles (material.rs:440-455) in a bounded domain, and
+ * its hand-written adjoint: gradients of a loss on the final positions and
+ * velocities with respect to the initial velocities and the per-particle
+ * Young's moduli.  The forward stores the state every `checkpoint_every`
+ * substeps; the backward replays each segment from its checkpoint.  All
+ * arrays are host f64: 3 per particle for vectors, 1 for Young's modulus, in
+ * the particle order given at creation. */
+typedef struct TmpmAdjoint TmpmAdjoint;
+
+TmpmStatus tmpm_adjoint_create(const TmpmParams *params, const TmpmParticleArrays *particles,
+                               double substep_dt, uint32_t substeps, uint32_t checkpoint_every,
+                               int32_t device, TmpmAdjoint **out);
+void tmpm_adjoint_destroy(TmpmAdjoint *adjoint);
+size_t tmpm_adjoint_particle_count(const TmpmAdjoint *adjoint);
+
+/* Run the rollout from the creation state with the given initial velocities
+ * and Young's moduli (NULL keeps the creation values); writes the final
+ * positions and velocities (either may be NULL). */
+TmpmStatus tmpm_adjoint_forward(TmpmAdjoint *adjoint, const double *velocity0, const double *young,
+                                double *position_out, double *velocity_out);
+
+/* Adjoint of the last forward: given dL/dx_T and dL/dv_T (NULL = zero),
+ * writes dL/dv_0 and dL/dE (either may be NULL). */
+TmpmStatus tmpm_adjoint_backward(TmpmAdjoint *adjoint, const double *position_grad,
+                                 const double *velocity_grad, double *velocity0_grad,
+                                 double *young_grad);
+
+const char *tmpm_adjoint_last_error_message(const TmpmAdjoint *adjoint);
+
 /* ------------------------------ diagnostics ------------------------------ */
 
 /* Human-readable reason for the last failed call on this session. */

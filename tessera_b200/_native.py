@@ -128,6 +128,19 @@ def lib():
     L.tmpm_scene_prepared_bytes.restype = C.c_size_t
     L.tmpm_batch_admit.argtypes = [P, P, C.POINTER(U32)]
     L.tmpm_batch_admit.restype = S
+    L.tmpm_adjoint_create.argtypes = [C.POINTER(TmpmParams), C.POINTER(TmpmParticleArrays), C.c_double, U32, U32,
+                                      C.c_int32, C.POINTER(P)]
+    L.tmpm_adjoint_create.restype = S
+    L.tmpm_adjoint_destroy.argtypes = [P]
+    L.tmpm_adjoint_destroy.restype = None
+    L.tmpm_adjoint_particle_count.argtypes = [P]
+    L.tmpm_adjoint_particle_count.restype = C.c_size_t
+    L.tmpm_adjoint_forward.argtypes = [P, P, P, P, P]
+    L.tmpm_adjoint_forward.restype = S
+    L.tmpm_adjoint_backward.argtypes = [P, P, P, P, P]
+    L.tmpm_adjoint_backward.restype = S
+    L.tmpm_adjoint_last_error_message.argtypes = [P]
+    L.tmpm_adjoint_last_error_message.restype = C.c_char_p
     L.tmpm_batch_last_error_message.argtypes = [P]
     L.tmpm_batch_last_error_message.restype = C.c_char_p
     _lib = L

@@ -93,7 +93,7 @@ __device__ __forceinline__ bool regular_corotated(const M3f &F) {
 // Corotated Kirchhoff stress 2 mu (F - R) F^T + lambda (J - 1) J I, scaled by
 // snow's hardening factor (material.rs:272-283, 440-455).  Out of line: its
 // polar iteration would otherwise raise register pressure for every particle.
-__device__ __noinline__ M3f corotated_stress(const DevClass &k, const M3f &F, float J, float plastic_det) {
+static __device__ __noinline__ M3f corotated_stress(const DevClass &k, const M3f &F, float J, float plastic_det) {
     float factor = 1.0f;
     if (k.kind == kMatSnow) factor = fminf(fmaxf(expf(k.p2 * (1.0f - plastic_det)), 0.01f), 100.0f);
     float lambda = k.p0 * factor, mu = k.p1 * factor;
@@ -209,7 +209,7 @@ __device__ __forceinline__ M3f replace_stretches(const M3f &F, const M3f &V, V3f
 // f32; `pl` = (plastic_det, hardening, log_volume_gain).  Returns false when
 // F is too ill-conditioned to project on the device (the reference's GPU
 // marks those particles for its CPU path, gpu.wgsl:569-573).
-__device__ __noinline__ bool project_plastic(const DevClass &k, M3f &F, float pl[3]) {
+static __device__ __noinline__ bool project_plastic(const DevClass &k, M3f &F, float pl[3]) {
     if ((k.kind == kMatSand || k.kind == kMatSandNeoHookean) && k.p0 == 0.0f) return true;  // lambda == 0
     V3f w;
     M3f V;
@@ -298,7 +298,7 @@ __device__ inline V3f closest_point_triangle(V3f p, V3f a, V3f b, V3f c) {
 __device__ __forceinline__ V3f normalize(V3f v) { return v * (1.0f / len(v)); }
 
 // Signed distance and outward world normal (obstacle.rs:372-472).
-__device__ __noinline__ float obstacle_surface(const DevObstacle &o, const float *planes, V3f point, V3f &normal) {
+static __device__ __noinline__ float obstacle_surface(const DevObstacle &o, const float *planes, V3f point, V3f &normal) {
     V3f rel = point - mk(o.center[0], o.center[1], o.center[2]);
     if (o.shape == 0) {  // sphere
         float n = len(rel);
