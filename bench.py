@@ -20,6 +20,9 @@ maximum, gpu.rs:303-322) over the whole scene.
   serving  Poisson arrivals of dam-break-sized requests (50-400 substeps) into
          the continuous-batching server under a 120 GB footprint budget, against
          the one-scene-at-a-time loop: p50/p99 time-to-result and throughput.
+  adjoint  the differentiable rollout (64k-particle corotated block, 256
+         substeps, checkpoints every 16): forward and adjoint wall time through
+         the C ABI (host arrays in and out).
 
 `--impl reference` times the reference's CPU path (its C++ restatement in
 oracle/, f64, ordered-map grid) on the host cores for the same workload.
@@ -62,6 +65,9 @@ def parse():
     ap.add_argument("--no-serving", action="store_true")
     ap.add_argument("--serve-rates", default="200", help="comma-separated arrival rates (requests/s)")
     ap.add_argument("--serve-requests", type=int, default=12)
+    ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--only", choices=["batched", "serving", "adjoint"],
+                    help="run one section alone and print its result (profiling; not the benchmark line)")
     return ap.parse_args()
 
 
@@ -296,6 +302,37 @@ def bench_serving(rates, count: int) -> dict:
     return out
 
 
+def bench_adjoint() -> dict:
+    """Forward + adjoint of the 64k-particle rollout (256 substeps, checkpoints every 16)."""
+    from tessera_b200 import scenes
+    from tessera_b200.adjoint import Rollout
+
+    sc = scenes.adjoint_block()
+    n = sc.particles.count
+    sim = Rollout(sc.params, sc.particles, sc.dt, sc.substeps, checkpoint_every=16)
+    v0 = sc.particles.velocity.copy()
+    E = np.full(n, 5e3)
+    target = np.asarray(sc.info["target"])
+    fw, bw = [], []
+    for it in range(4):
+        t0 = time.perf_counter()
+        x, _ = sim.forward(v0, E)
+        t1 = time.perf_counter()
+        sim.backward(np.tile(2.0 * (x.mean(0) - target) / n, (n, 1)))
+        t2 = time.perf_counter()
+        if it > 0:
+            fw.append(t1 - t0)
+            bw.append(t2 - t1)
+    sim.close()
+    work = float(n) * sc.substeps
+    f, b = float(np.median(fw)), float(np.median(bw))
+    return {"workload": "config5-differentiable", "particles": n, "substeps": sc.substeps, "checkpoint_every": 16,
+            "forward_s": f, "backward_s": b, "forward": work / f, "backward": work / b,
+            "forward_plus_backward": work / (f + b), "unit": METRIC,
+            "timing": "wall clock through the C ABI (host f64 arrays in and out, synchronous calls)",
+            "parity": "gradients vs central differences of the oracle: tests/test_gpu_adjoint.py"}
+
+
 def run_reference(args, world, rank):
     if rank != 0:
         return
@@ -405,6 +442,9 @@ def run_tessera(args, world, rank, local):
         batched = bench_batched(args.batched_scenes)
     if rank == 0 and world == 1 and not args.no_serving:
         serving = bench_serving([float(r) for r in args.serve_rates.split(",") if r], args.serve_requests)
+    adjoint = None
+    if rank == 0 and world == 1 and not args.no_adjoint:
+        adjoint = bench_adjoint()
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
@@ -421,12 +461,22 @@ def run_tessera(args, world, rank, local):
             "clocks": clk,
             "batched": batched,
             "serving": serving,
+            "adjoint": adjoint,
         }
         print(json.dumps(line), flush=True)
 
 
 def main():
     args = parse()
+    if args.only:
+        if args.only == "batched":
+            res = bench_batched(args.batched_scenes)
+        elif args.only == "serving":
+            res = bench_serving([float(r) for r in args.serve_rates.split(",") if r], args.serve_requests)
+        else:
+            res = bench_adjoint()
+        print(json.dumps(res), flush=True)
+        return
     world, rank, local = dist_setup()
     try:
         if args.impl == "reference":

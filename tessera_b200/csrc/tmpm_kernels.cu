@@ -47,6 +47,22 @@ struct Box {
 
 __device__ __forceinline__ int node_local(int cx, int cy, int cz) { return ((cx & 3) * 4 + (cy & 3)) * 4 + (cz & 3); }
 
+// Split a row-major tile index t (dims d0 x d1 x d2, t < 2^20) into (tx, ty, tz)
+// without integer division: (t + 0.5) / d lies at least 1 / (2 d) from an
+// integer, far above the f32 error of (t + 0.5) * (1 / d), so truncation is exact.
+struct Split3 {
+    int d1, d2;
+    float inv_d1, inv_d2;
+    __device__ __forceinline__ Split3(int d1_, int d2_)
+        : d1(d1_), d2(d2_), inv_d1(1.0f / static_cast<float>(d1_)), inv_d2(1.0f / static_cast<float>(d2_)) {}
+    __device__ __forceinline__ void operator()(int t, int &tx, int &ty, int &tz) const {
+        const int q = static_cast<int>((static_cast<float>(t) + 0.5f) * inv_d2);
+        tz = t - q * d2;
+        tx = static_cast<int>((static_cast<float>(q) + 0.5f) * inv_d1);
+        ty = q - tx * d1;
+    }
+};
+
 // Block-wide min/max of base cells and colours; thread 0 fills `box`.
 __device__ __forceinline__ void reduce_box(bool valid, const int b[3], uint32_t color, int (*red)[8], Box &box) {
     int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -278,8 +294,10 @@ __global__ void __launch_bounds__(kThreads, TMPM_TRANSFER_MIN_BLOCKS)
                 reduce_box(g2p_on, b, k.color, s_red, s_box);
                 bx = s_box;
                 if (bx.ok) {
+                    const Split3 split(bx.nb[1], bx.nb[2]);
                     for (int t = threadIdx.x; t < bx.nbt; t += kThreads) {
-                        int tz = t % bx.nb[2], ty = (t / bx.nb[2]) % bx.nb[1], tx = t / (bx.nb[2] * bx.nb[1]);
+                        int tx, ty, tz;
+                        split(t, tx, ty, tz);
                         s_blk[t] = lookup_block(cur, block_key(bx.blo[0] + tx, bx.blo[1] + ty, bx.blo[2] + tz, bx.color));
                     }
                     __syncthreads();
@@ -289,8 +307,10 @@ __global__ void __launch_bounds__(kThreads, TMPM_TRANSFER_MIN_BLOCKS)
                        (b[0] < bx.lo[0] || b[1] < bx.lo[1] || b[2] < bx.lo[2] || b[0] + 2 >= bx.lo[0] + bx.dim[0] ||
                         b[1] + 2 >= bx.lo[1] + bx.dim[1] || b[2] + 2 >= bx.lo[2] + bx.dim[2] || k.color != bx.color);
             if (bx.ok && !bad) {
+                const Split3 split(bx.dim[1], bx.dim[2]);
                 for (int t = threadIdx.x; t < bx.nodes; t += kThreads) {
-                    int tz = t % bx.dim[2], ty = (t / bx.dim[2]) % bx.dim[1], tx = t / (bx.dim[2] * bx.dim[1]);
+                    int tx, ty, tz;
+                    split(t, tx, ty, tz);
                     int cx = bx.lo[0] + tx, cy = bx.lo[1] + ty, cz = bx.lo[2] + tz;
                     int tb = tile_block_index(bx, cx, cy, cz);
                     int id = use_cache ? cc[kCacheHeader + tb] : s_blk[tb];
@@ -323,23 +343,43 @@ __global__ void __launch_bounds__(kThreads, TMPM_TRANSFER_MIN_BLOCKS)
             }
             if (bx.ok) {
                 const int ox = b[0] - bx.lo[0], oy = b[1] - bx.lo[1], oz = b[2] - bx.lo[2];
+                // Paired f32 arithmetic (Blackwell FFMA2): accumulators
+                // p0..p2 = (vel, C column 0) and q0..q2 = (C column 1, C column 2)
+                // for the x, y, z components; per node (w, w dx) and (w dy, w dz).
+                float2 p0 = make_float2(0.f, 0.f), p1 = p0, p2 = p0, q0 = p0, q1 = p0, q2 = p0;
+                float2 z1[3], z2[3];
+#pragma unroll
+                for (int e = 0; e < 3; ++e) {
+                    z1[e] = make_float2(wz[e], wz[e]);
+                    z2[e] = make_float2(wz[e], wz[e] * dzs[e]);
+                }
 #pragma unroll
                 for (int a = 0; a < 3; ++a)
 #pragma unroll
                     for (int c = 0; c < 3; ++c) {
                         const float wac = wx[a] * wy[c];
+                        const float2 pa = make_float2(wac, wac * dxs[a]);
+                        const float2 pb = make_float2(wac * dys[c], wac);
                         const int row = ((ox + a) * bx.dim[1] + (oy + c)) * bx.dim[2] + oz;
 #pragma unroll
                         for (int e = 0; e < 3; ++e) {
-                            const float w = wac * wz[e];
                             const float4 g4 = s_gv[row + e];
-                            const V3f nv = mk(g4.x, g4.y, g4.z);
-                            vel = vel + nv * w;
-                            aff.c0 = aff.c0 + nv * (dxs[a] * w);
-                            aff.c1 = aff.c1 + nv * (dys[c] * w);
-                            aff.c2 = aff.c2 + nv * (dzs[e] * w);
+                            const float2 s1 = __fmul2_rn(pa, z1[e]);  // (w, w dx)
+                            const float2 s2 = __fmul2_rn(pb, z2[e]);  // (w dy, w dz)
+                            const float2 nx = make_float2(g4.x, g4.x), ny = make_float2(g4.y, g4.y),
+                                         nz = make_float2(g4.z, g4.z);
+                            p0 = __ffma2_rn(nx, s1, p0);
+                            p1 = __ffma2_rn(ny, s1, p1);
+                            p2 = __ffma2_rn(nz, s1, p2);
+                            q0 = __ffma2_rn(nx, s2, q0);
+                            q1 = __ffma2_rn(ny, s2, q1);
+                            q2 = __ffma2_rn(nz, s2, q2);
                         }
                     }
+                vel = mk(p0.x, p1.x, p2.x);
+                aff.c0 = mk(p0.y, p1.y, p2.y);
+                aff.c1 = mk(q0.x, q1.x, q2.x);
+                aff.c2 = mk(q0.y, q1.y, q2.y);
             } else {
                 unsigned long long last_key = kEmptyKey;
                 int last_id = -1;
@@ -519,6 +559,12 @@ __global__ void __launch_bounds__(kThreads, TMPM_TRANSFER_MIN_BLOCKS)
                 dys[a] = (a - fx.y) * h;
                 dzs[a] = (a - fx.z) * h;
             }
+            // Paired f32 arithmetic: per node (m w s_m, w s_p) from (w_ac, w_ac) x (w_z m s_m, w_z s_p),
+            // and the momentum's (x, y) pair.
+            float2 zs[3];
+#pragma unroll
+            for (int e = 0; e < 3; ++e) zs[e] = make_float2(wz[e] * msc, wz[e] * spv);
+            const float2 c2xy = make_float2(A.c2.x, A.c2.y);
 #pragma unroll
             for (int a = 0; a < 3; ++a) {
                 const V3f qa = mv + A.c0 * dxs[a];
@@ -526,17 +572,20 @@ __global__ void __launch_bounds__(kThreads, TMPM_TRANSFER_MIN_BLOCKS)
                 for (int c = 0; c < 3; ++c) {
                     const V3f qac = qa + A.c1 * dys[c];
                     const float wac = wx[a] * wy[c];
+                    const float2 wac2 = make_float2(wac, wac);
+                    const float2 qacxy = make_float2(qac.x, qac.y);
                     const int row = ((ox + a) * bx.dim[1] + (oy + c)) * bx.dim[2] + oz;
 #pragma unroll
                     for (int e = 0; e < 3; ++e) {
-                        const V3f q = qac + A.c2 * dzs[e];
-                        const float w = wac * wz[e];
-                        const float wp = w * spv;
+                        const float2 qxy = __ffma2_rn(c2xy, make_float2(dzs[e], dzs[e]), qacxy);
+                        const float qz = qac.z + A.c2.z * dzs[e];
+                        const float2 mw = __fmul2_rn(wac2, zs[e]);  // (w m s_m, w s_p)
+                        const float2 pxy = __fmul2_rn(qxy, make_float2(mw.y, mw.y));
                         const int t = row + e;
-                        atomicAdd(reinterpret_cast<unsigned *>(&s_sc[0][t]), static_cast<unsigned>(__float2int_rn(w * msc)));
-                        atomicAdd(reinterpret_cast<unsigned *>(&s_sc[1][t]), static_cast<unsigned>(__float2int_rn(q.x * wp)));
-                        atomicAdd(reinterpret_cast<unsigned *>(&s_sc[2][t]), static_cast<unsigned>(__float2int_rn(q.y * wp)));
-                        atomicAdd(reinterpret_cast<unsigned *>(&s_sc[3][t]), static_cast<unsigned>(__float2int_rn(q.z * wp)));
+                        atomicAdd(reinterpret_cast<unsigned *>(&s_sc[0][t]), static_cast<unsigned>(__float2int_rn(mw.x)));
+                        atomicAdd(reinterpret_cast<unsigned *>(&s_sc[1][t]), static_cast<unsigned>(__float2int_rn(pxy.x)));
+                        atomicAdd(reinterpret_cast<unsigned *>(&s_sc[2][t]), static_cast<unsigned>(__float2int_rn(pxy.y)));
+                        atomicAdd(reinterpret_cast<unsigned *>(&s_sc[3][t]), static_cast<unsigned>(__float2int_rn(qz * mw.y)));
                     }
                 }
             }
@@ -554,10 +603,12 @@ __global__ void __launch_bounds__(kThreads, TMPM_TRANSFER_MIN_BLOCKS)
             s_used[(bx1 * bx.nb[1] + by1) * bx.nb[2] + bz1] = 1;
         }
         __syncthreads();
+        const Split3 split_b(bx.nb[1], bx.nb[2]);
         for (int t = threadIdx.x; t < bx.nbt; t += kThreads) {
             int id = -1;
             if (s_used[t]) {
-                int tz = t % bx.nb[2], ty = (t / bx.nb[2]) % bx.nb[1], tx = t / (bx.nb[2] * bx.nb[1]);
+                int tx, ty, tz;
+                split_b(t, tx, ty, tz);
                 int gx = bx.blo[0] + tx, gy = bx.blo[1] + ty, gz = bx.blo[2] + tz;
                 // reuse the id the G2P box already holds for this block (same table)
                 if (gbox.ok && gbox.color == bx.color) {
@@ -592,10 +643,12 @@ __global__ void __launch_bounds__(kThreads, TMPM_TRANSFER_MIN_BLOCKS)
         }
         __syncthreads();
         const float inv_sm = 1.0f / sm, inv_sp = 1.0f / spv;
+        const Split3 split_n(bx.dim[1], bx.dim[2]);
         for (int t = threadIdx.x; t < bx.nodes; t += kThreads) {
             const int m = s_sc[0][t], px = s_sc[1][t], py = s_sc[2][t], pz = s_sc[3][t];
             if ((m | px | py | pz) == 0) continue;
-            int tz = t % bx.dim[2], ty = (t / bx.dim[2]) % bx.dim[1], tx = t / (bx.dim[2] * bx.dim[1]);
+            int tx, ty, tz;
+            split_n(t, tx, ty, tz);
             int cx = bx.lo[0] + tx, cy = bx.lo[1] + ty, cz = bx.lo[2] + tz;
             int id = s_blk2[tile_block_index(bx, cx, cy, cz)];
             if (id < 0) continue;
