@@ -231,7 +231,7 @@ def bench_batched(count: int) -> dict:
     with ThreadPoolExecutor(max_workers=8) as pool:  # preparation is host work, thread-safe
         prepared = list(pool.map(lambda s: PreparedScene(s.params, s.particles, s.dt), scs))
     ids = [b.admit(p) for p in prepared]
-    b.run({i: steps for i in ids}, collect=ids)
+    b.run({i: steps for i in ids})
     outs = [b.read(i) for i in ids]
     e2e_batched = time.perf_counter() - t0
     assert all(np.all(np.isfinite(o["position"])) for o in outs)

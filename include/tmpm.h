@@ -286,7 +286,7 @@ TmpmStatus tmpm_batch_create(const TmpmBatchOptions *options, TmpmBatch **out);
 void tmpm_batch_destroy(TmpmBatch *batch);
 
 /* A scene validated like validate_resident_world (gpu.rs:664-677) and packed
- * into pinned host memory, not yet attached to a batch.  Preparing does no
+ * into host memory, not yet attached to a batch.  Preparing does no
  * device work and touches no batch, so scenes may be prepared on any thread,
  * also while a batch is in flight. */
 typedef struct TmpmPreparedScene TmpmPreparedScene;
@@ -313,13 +313,9 @@ TmpmStatus tmpm_batch_add_scene(TmpmBatch *batch, const TmpmParams *params,
 TmpmStatus tmpm_batch_remove_scene(TmpmBatch *batch, uint32_t scene);
 
 /* Queue one batch: scene ids[k] advances steps[k] substeps (1..4096); scenes
- * not listed stay put.  When collect is not NULL and collect[k] != 0, the
- * scene's rows are copied to pinned host memory right after the batch, so
- * tmpm_batch_read_scene needs no device work for it (and may run while the
- * next batch is in flight).  Asynchronous, like submit_steps
- * (gpu.rs:303-322); one batch may be in flight. */
-TmpmStatus tmpm_batch_submit(TmpmBatch *batch, const uint32_t *ids, const uint32_t *steps,
-                             const uint8_t *collect, size_t count);
+ * not listed stay put.  Asynchronous, like submit_steps (gpu.rs:303-322); one
+ * batch may be in flight. */
+TmpmStatus tmpm_batch_submit(TmpmBatch *batch, const uint32_t *ids, const uint32_t *steps, size_t count);
 
 /* Wait for the batch in flight (bounded, as gpu.rs:1853-1862) and record each
  * scene's outcome.  A scene whose resident checks failed (CFL, escape,
@@ -331,8 +327,9 @@ int32_t tmpm_batch_pending(const TmpmBatch *batch);
 
 /* Per-scene state: outcome (TMPM_OK or the failure), completed substeps,
  * particle count, and the particles themselves (like world() after
- * synchronize, gpu.rs:654-661): from the collected rows, else read back from
- * the device, which needs no batch in flight. */
+ * synchronize, gpu.rs:654-661).  Reading a scene that the batch in flight does
+ * not advance runs concurrently with that batch; a scene in the batch in
+ * flight returns TMPM_ERR_PENDING_STEPS. */
 TmpmStatus tmpm_batch_scene_status(const TmpmBatch *batch, uint32_t scene);
 uint64_t tmpm_batch_scene_substeps(const TmpmBatch *batch, uint32_t scene);
 size_t tmpm_batch_scene_particle_count(const TmpmBatch *batch, uint32_t scene);

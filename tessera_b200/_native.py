@@ -98,7 +98,7 @@ def lib():
     L.tmpm_batch_add_scene.restype = S
     L.tmpm_batch_remove_scene.argtypes = [P, U32]
     L.tmpm_batch_remove_scene.restype = S
-    L.tmpm_batch_submit.argtypes = [P, P, P, P, C.c_size_t]
+    L.tmpm_batch_submit.argtypes = [P, P, P, C.c_size_t]
     L.tmpm_batch_submit.restype = S
     L.tmpm_batch_synchronize.argtypes = [P]
     L.tmpm_batch_synchronize.restype = S

@@ -124,21 +124,17 @@ class Batch:
         _check(_native.lib().tmpm_batch_remove_scene(self._h, int(scene)), self._h)
         self._counts.pop(int(scene), None)
 
-    def submit(self, steps: dict[int, int], collect=()) -> None:
-        """Queue one batch: scene -> substeps.  Scenes in `collect` have their rows
-        copied back right after the batch (read them without device work)."""
+    def submit(self, steps: dict[int, int]) -> None:
+        """Queue one batch: scene -> substeps.  Scenes not in it stay readable while it runs."""
         ids = np.ascontiguousarray(list(steps.keys()), dtype=np.uint32)
         n = np.ascontiguousarray(list(steps.values()), dtype=np.uint32)
-        col = set(collect)
-        flags = np.ascontiguousarray([1 if int(i) in col else 0 for i in ids], dtype=np.uint8)
-        _check(_native.lib().tmpm_batch_submit(self._h, ids.ctypes.data, n.ctypes.data, flags.ctypes.data, len(ids)),
-               self._h)
+        _check(_native.lib().tmpm_batch_submit(self._h, ids.ctypes.data, n.ctypes.data, len(ids)), self._h)
 
     def synchronize(self) -> None:
         _check(_native.lib().tmpm_batch_synchronize(self._h), self._h)
 
-    def run(self, steps: dict[int, int], collect=()) -> None:
-        self.submit(steps, collect)
+    def run(self, steps: dict[int, int]) -> None:
+        self.submit(steps)
         self.synchronize()
 
     def pending(self) -> bool:

@@ -13,13 +13,18 @@
 // Device rows stay sorted by (scene, block) after every batch's re-sort, so a
 // scene occupies one contiguous range and is read back with a few strided
 // copies.  Admission is split for overlap with device work: a scene is
-// validated and packed into pinned memory by tmpm_scene_prepare (any thread,
+// validated and packed into host memory by tmpm_scene_prepare (any thread,
 // no device work), attached to the batch by tmpm_batch_admit (allowed while a
 // batch is in flight) and copied to the device at the next submit, appended
 // after the resident rows.  A retired scene is marked removed: the next
-// re-sort moves its rows past the live ones and drops them.  Finished scenes
-// can be collected: their rows are copied to pinned memory right after the
-// batch that finishes them, so reading them needs no device work.
+// re-sort moves its rows past the live ones and drops them.  A batch re-sorts
+// from one row buffer into the other and only reads the first, so while it
+// runs, every scene it does not advance can still be read from the first
+// buffer, on a side stream, concurrently with the batch.
+//
+// Host staging is ordinary (pageable) memory: pinning a scene-sized buffer
+// costs more than the staged copy it would speed up, and scenes are prepared
+// once and read once.
 
 #include <chrono>
 #include <cstdio>
@@ -34,92 +39,6 @@ using namespace tmpm;
 
 namespace {
 
-// Pinned host buffers are expensive to create (page locking), so released ones
-// are kept for reuse, up to kPoolKeepBytes in total.
-constexpr size_t kPoolKeepBytes = size_t(8) << 30;
-
-struct PinnedPool {
-    std::mutex mu;
-    std::vector<std::pair<void *, size_t>> free_list;
-    size_t free_bytes = 0;
-
-    void *acquire(size_t bytes, size_t &got) {
-        {
-            std::lock_guard<std::mutex> lock(mu);
-            size_t best = free_list.size();
-            for (size_t k = 0; k < free_list.size(); ++k) {
-                size_t b = free_list[k].second;
-                if (b >= bytes && b <= 2 * bytes + (size_t(64) << 20) &&
-                    (best == free_list.size() || b < free_list[best].second))
-                    best = k;
-            }
-            if (best != free_list.size()) {
-                void *p = free_list[best].first;
-                got = free_list[best].second;
-                free_bytes -= got;
-                free_list.erase(free_list.begin() + best);
-                return p;
-            }
-        }
-        void *p = nullptr;
-        if (cudaMallocHost(&p, bytes) != cudaSuccess) return nullptr;
-        got = bytes;
-        return p;
-    }
-
-    void release(void *p, size_t bytes) {
-        if (!p) return;
-        std::vector<void *> drop;
-        {
-            std::lock_guard<std::mutex> lock(mu);
-            free_list.emplace_back(p, bytes);
-            free_bytes += bytes;
-            while (free_bytes > kPoolKeepBytes && !free_list.empty()) {
-                drop.push_back(free_list.front().first);
-                free_bytes -= free_list.front().second;
-                free_list.erase(free_list.begin());
-            }
-        }
-        for (void *q : drop) cudaFreeHost(q);
-    }
-};
-
-PinnedPool &pinned_pool() {
-    static PinnedPool *pool = new PinnedPool();  // outlives every batch (never destroyed at exit)
-    return *pool;
-}
-
-// A pinned buffer borrowed from the pool.
-struct PinnedLease {
-    void *ptr = nullptr;
-    size_t bytes = 0;
-    bool ensure(size_t b) {
-        if (b <= bytes) return true;
-        release();
-        ptr = pinned_pool().acquire(b, bytes);
-        if (!ptr) bytes = 0;
-        return ptr != nullptr;
-    }
-    void release() {
-        pinned_pool().release(ptr, bytes);
-        ptr = nullptr;
-        bytes = 0;
-    }
-    PinnedLease() = default;
-    PinnedLease(const PinnedLease &) = delete;
-    PinnedLease &operator=(const PinnedLease &) = delete;
-    PinnedLease(PinnedLease &&o) noexcept { *this = std::move(o); }
-    PinnedLease &operator=(PinnedLease &&o) noexcept {
-        if (this != &o) {
-            release();
-            std::swap(ptr, o.ptr);
-            std::swap(bytes, o.bytes);
-        }
-        return *this;
-    }
-    ~PinnedLease() { release(); }
-};
-
 // Per-particle device bytes: two row sets of 27 floats + class + index, sort
 // keys and values (double-buffered); per home block the pool sizing rule
 // (16 blocks per occupied block) x two pools of 64 float4 nodes + coords +
@@ -127,11 +46,12 @@ struct PinnedLease {
 constexpr size_t kBytesPerRow = 2 * (27 * 4 + 2 * 4) + 4 * 4;
 constexpr size_t kBytesPerPoolBlock = 2 * kNodesPerBlock * 16 + 16 + 2 * (8 + 4);
 
-// Rows of one scene in pinned memory: 27 f32 component rows of `stride`, then
-// class and world-index rows.
-float *row_base(PinnedLease &l) { return static_cast<float *>(l.ptr); }
-uint32_t *row_cls(PinnedLease &l, size_t stride) { return reinterpret_cast<uint32_t *>(row_base(l) + 27 * stride); }
-uint32_t *row_widx(PinnedLease &l, size_t stride) { return row_cls(l, stride) + stride; }
+// Rows of one scene in host memory: 27 f32 component rows of `stride`, then
+// class and world-index rows (29 rows of 4-byte words).
+using HostRows = HostVec<float>;
+float *row_base(HostRows &l) { return l.data(); }
+uint32_t *row_cls(HostRows &l, size_t stride) { return reinterpret_cast<uint32_t *>(row_base(l) + 27 * stride); }
+uint32_t *row_widx(HostRows &l, size_t stride) { return row_cls(l, stride) + stride; }
 
 }  // namespace
 
@@ -141,7 +61,7 @@ struct TmpmPreparedScene {
     double dt = 0.0;
     HostWorld world;
     ClassTable classes;     // local classes (namespace 0)
-    PinnedLease rows;       // packed rows, class ids local
+    HostRows rows;          // packed rows, class ids local
     size_t m = 0;           // enabled particles (device rows)
     size_t blocks = 0;      // occupied home blocks
 };
@@ -185,7 +105,7 @@ TmpmStatus prepare_scene(const TmpmParams &params, const TmpmParticleArrays *par
     PackResult pr = pack_world(p.world, 1.0f / h32, 0u, p.classes, [&](size_t n_enabled) {
         PackTarget tg;
         stride = std::max<size_t>(n_enabled, 1);
-        if (!p.rows.ensure(29 * stride * sizeof(float))) return tg;
+        p.rows.resize(29 * stride);
         tg.base = row_base(p.rows);
         tg.cls = row_cls(p.rows, stride);
         tg.widx = row_widx(p.rows, stride);
@@ -216,9 +136,7 @@ struct BatchScene {
     size_t blocks = 0;       // occupied home blocks at admission (pool sizing)
     uint32_t queued = 0;     // substeps in the batch in flight
     std::unique_ptr<TmpmPreparedScene> staged;  // admitted, rows not yet on the device
-    PinnedLease result;      // rows collected at the end of a batch
-    bool collect = false;    // the batch in flight copies this scene's rows back
-    bool collected = false;  // `result` holds the scene's latest rows
+    size_t prev_offset = 0;  // first row in the buffer the batch in flight reads
     TmpmStatus status = TMPM_OK;
     std::string error;
 };
@@ -246,9 +164,10 @@ struct TmpmBatch {
     DevBuf<SceneParams> dscenes;
     DevBuf<int> cta_cache;
     DevBuf<uint32_t> sort_keys[2], sort_vals[2], sort_hist, sort_totals;
-    PinnedBuf staging, table_staging;
+    PinnedBuf table_staging;
     std::vector<std::unique_ptr<TmpmPreparedScene>> in_flight_uploads;  // kept until the copies complete
-    std::vector<std::unique_ptr<PinnedLease>> in_flight_results;        // results of scenes removed mid-flight
+    cudaStream_t read_stream = nullptr;  // reads of scenes the batch in flight does not advance
+    HostRows read_staging;
     uint64_t epoch = 1;  // bumps whenever a device pointer a graph holds changes
     bool pending = false;
     double last_ms = 0.0;
@@ -270,6 +189,7 @@ struct TmpmBatch {
         if (done) cudaEventDestroy(done);
         if (t_begin) cudaEventDestroy(t_begin);
         if (t_end) cudaEventDestroy(t_end);
+        if (read_stream) cudaStreamDestroy(read_stream);
         if (stream) cudaStreamDestroy(stream);
     }
 
@@ -509,6 +429,9 @@ struct TmpmBatch {
         if ((st = commit_staged()) != TMPM_OK) return st;
         if ((e = upload_table())) return cuda_fail(e, "scene table upload");
         if ((e = cudaEventRecord(t_begin, stream))) return cuda_fail(e, "cudaEventRecord");
+        for (BatchScene &s : scenes)
+            if (s.live) s.prev_offset = s.dev_offset;
+        prev_buf = cur;
         if (n_phys > 0) {
             if (options.use_graphs) {
                 GraphKey key{steps, n_phys, n_live, cur, epoch};
@@ -534,32 +457,30 @@ struct TmpmBatch {
         }
         assign_offsets();
         if ((e = cudaEventRecord(t_end, stream))) return cuda_fail(e, "cudaEventRecord");
-        // collected scenes: rows back to pinned memory right after the batch
-        for (BatchScene &s : scenes) {
-            if (!s.live || !s.collect) continue;
-            if ((st = queue_readback(s, s.result)) != TMPM_OK) return st;
-        }
         if ((e = cudaGetLastError())) return cuda_fail(e, "kernel launch");
         return TMPM_OK;
     }
+    int prev_buf = 0;  // row buffer the batch in flight re-sorts from (and only reads)
 
-    // Queue the copy of a scene's rows into `dst` (27 rows + widx, stride m).
-    TmpmStatus queue_readback(BatchScene &s, PinnedLease &dst) {
+    // Copy a scene's rows (27 f32 rows + widx, stride m) from row buffer `buf`
+    // at row `off` into `dst` on `st`, and wait for the copy.
+    TmpmStatus read_rows(BatchScene &s, int buf, size_t off, cudaStream_t st, HostRows &dst) {
         const size_t m = s.dev_count, stride = std::max<size_t>(m, 1);
-        if (!dst.ensure(28 * stride * sizeof(float))) return fail(TMPM_ERR_DEVICE, "cudaMallocHost readback failed");
+        dst.resize(28 * stride);
         if (!m) return TMPM_OK;
-        const size_t pc = pbuf[cur].cap, off = s.dev_offset;
-        float *h = row_base(dst);
-        const ParticleBuffers &pb = pbuf[cur];
+        const size_t pc = pbuf[buf].cap;
+        float *h = dst.data();
+        const ParticleBuffers &pb = pbuf[buf];
         auto rows = [&](float *d, const float *src, int r) {
-            return cudaMemcpy2DAsync(d, stride * 4, src + off, pc * 4, m * 4, r, cudaMemcpyDeviceToHost, stream);
+            return cudaMemcpy2DAsync(d, stride * 4, src + off, pc * 4, m * 4, r, cudaMemcpyDeviceToHost, st);
         };
         cudaError_t e;
         if ((e = rows(h, pb.x.ptr, 3)) || (e = rows(h + 3 * stride, pb.v.ptr, 3)) ||
             (e = rows(h + 6 * stride, pb.C.ptr, 9)) || (e = rows(h + 15 * stride, pb.F.ptr, 9)) ||
             (e = rows(h + 24 * stride, pb.pl.ptr, 3)) ||
             (e = cudaMemcpyAsync(reinterpret_cast<uint32_t *>(h + 27 * stride), pb.widx.ptr + off, m * 4,
-                                 cudaMemcpyDeviceToHost, stream)))
+                                 cudaMemcpyDeviceToHost, st)) ||
+            (e = cudaStreamSynchronize(st)))
             return cuda_fail(e, "scene readback");
         return TMPM_OK;
     }
@@ -590,7 +511,6 @@ struct TmpmBatch {
         TmpmStatus st = wait_done();
         if (st != TMPM_OK) return st;
         in_flight_uploads.clear();
-        in_flight_results.clear();
         float ms = 0.f;
         cudaEventElapsedTime(&ms, t_begin, t_end);
         last_ms = ms;
@@ -615,23 +535,20 @@ struct TmpmBatch {
                     s.status = TMPM_ERR_RESIDENT_UNAVAILABLE;
                     s.error = "GPU MPM resident substeps require a CPU fallback; scene state is the last one read";
                 }
-                s.result.release();
             } else if (s.status == TMPM_OK) {
                 s.substeps += s.queued;
                 s.stale = true;
-                if (s.collect) s.collected = true;
             }
             s.queued = 0;
-            s.collect = false;
         }
         return TMPM_OK;
     }
 
     // Apply rows (27 f32 rows + widx, stride m) to a scene's host world
     // (collect_prepared + apply_gpu_transfers, gpu.rs:1821-1989, 2295-2329).
-    TmpmStatus apply_rows(BatchScene &s, PinnedLease &src) {
+    TmpmStatus apply_rows(BatchScene &s, HostRows &src) {
         const size_t m = s.dev_count, stride = std::max<size_t>(m, 1);
-        const float *h = row_base(src);
+        const float *h = src.data();
         const uint32_t *widx = reinterpret_cast<const uint32_t *>(h + 27 * stride);
         std::atomic<bool> bad{false};
         parallel_for(m, [&](size_t a, size_t b) {
@@ -672,29 +589,23 @@ struct TmpmBatch {
         return TMPM_OK;
     }
 
-    // Bring a scene's host world up to date: from collected rows (no device
-    // work), else from the device (idle only).
+    // Bring a scene's host world up to date from the device: from the current
+    // rows when idle; while a batch runs, for a scene that batch does not
+    // advance, from the buffer the batch re-sorts from, on the side stream.
     TmpmStatus refresh(BatchScene &s) {
-        if (s.collected) {
-            TmpmStatus st = apply_rows(s, s.result);
-            s.result.release();
-            s.collected = false;
-            s.stale = false;
-            return st;
-        }
+        if (pending && s.queued) return fail(TMPM_ERR_PENDING_STEPS, "the scene is in the batch in flight");
         if (!s.stale) return TMPM_OK;
-        if (pending) return fail(TMPM_ERR_PENDING_STEPS, "a batch is in flight; synchronize first");
-        if (!staging_lease.ensure(28 * std::max<size_t>(s.dev_count, 1) * sizeof(float)))
-            return fail(TMPM_ERR_DEVICE, "cudaMallocHost staging failed");
-        TmpmStatus st = queue_readback(s, staging_lease);
+        TmpmStatus st;
+        if (pending) {
+            st = read_rows(s, prev_buf, s.prev_offset, read_stream, read_staging);
+        } else {
+            st = read_rows(s, cur, s.dev_offset, stream, read_staging);
+        }
         if (st != TMPM_OK) return st;
-        cudaError_t e = cudaStreamSynchronize(stream);
-        if (e) return cuda_fail(e, "scene readback");
-        st = apply_rows(s, staging_lease);
+        st = apply_rows(s, read_staging);
         s.stale = false;
         return st;
     }
-    PinnedLease staging_lease;
 
     int free_id() const {
         for (size_t id = 0; id < scenes.size(); ++id)
@@ -751,10 +662,6 @@ struct TmpmBatch {
         BatchScene *s = scene_at(id);
         if (!s) return fail(TMPM_ERR_INVALID_INPUT, "unknown scene id");
         n_live -= s->dev_count;
-        if (pending && s->queued) {
-            // the batch in flight may still write this scene's collected rows
-            in_flight_results.push_back(std::make_unique<PinnedLease>(std::move(s->result)));
-        }
         const bool had_rows = !s->staged;
         scenes[id] = BatchScene();
         scenes[id].draining = had_rows;  // rows on the device go at the next re-sort
@@ -842,6 +749,7 @@ TmpmStatus tmpm_batch_create(const TmpmBatchOptions *options, TmpmBatch **out) {
     b->device = b->options.device;
     cudaError_t e;
     if ((e = cudaSetDevice(b->device)) || (e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking)) ||
+        (e = cudaStreamCreateWithFlags(&b->read_stream, cudaStreamNonBlocking)) ||
         (e = cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming)) || (e = cudaEventCreate(&b->t_begin)) ||
         (e = cudaEventCreate(&b->t_end)) || (e = b->status.alloc(1)) || (e = b->scene_status.alloc(kMaxScenes)) ||
         (e = b->dscenes.alloc(kMaxScenes))) {
@@ -906,16 +814,12 @@ TmpmStatus tmpm_batch_remove_scene(TmpmBatch *b, uint32_t scene) {
     return b->remove(scene);
 }
 
-TmpmStatus tmpm_batch_submit(TmpmBatch *b, const uint32_t *ids, const uint32_t *steps, const uint8_t *collect,
-                             size_t count) {
+TmpmStatus tmpm_batch_submit(TmpmBatch *b, const uint32_t *ids, const uint32_t *steps, size_t count) {
     if (!b) return TMPM_ERR_INVALID_INPUT;
     TmpmStatus st = b->guard(true);
     if (st != TMPM_OK) return st;
     if (count && (!ids || !steps)) return b->fail(TMPM_ERR_INVALID_INPUT, "null scene or step array");
-    for (BatchScene &s : b->scenes) {
-        s.queued = 0;
-        s.collect = false;
-    }
+    for (BatchScene &s : b->scenes) s.queued = 0;
     uint32_t S = 0;
     for (size_t k = 0; k < count; ++k) {
         BatchScene *s = b->scene_at(ids[k]);
@@ -923,13 +827,7 @@ TmpmStatus tmpm_batch_submit(TmpmBatch *b, const uint32_t *ids, const uint32_t *
         if (s->status != TMPM_OK) return b->fail(s->status, "scene failed earlier: " + s->error);
         if (steps[k] == 0 || steps[k] > 4096) return b->fail(TMPM_ERR_INVALID_INPUT, "substeps per scene must be 1..4096");
         if (s->queued) return b->fail(TMPM_ERR_INVALID_INPUT, "scene listed twice");
-        if (s->collected && s->stale) {
-            // rows collected earlier are superseded by this batch: apply them first
-            st = b->refresh(*s);
-            if (st != TMPM_OK) return b->fail(st, s->error);
-        }
         s->queued = steps[k];
-        s->collect = collect && collect[k];
         S = std::max(S, steps[k]);
     }
     if (S == 0) return TMPM_OK;
@@ -970,7 +868,6 @@ TmpmStatus tmpm_batch_read_scene(TmpmBatch *b, uint32_t scene, TmpmParticleArray
     BatchScene *s = b->scene_at(scene);
     if (!s) return b->fail(TMPM_ERR_INVALID_INPUT, "unknown scene id");
     if (s->status != TMPM_OK) return b->fail(s->status, s->error);
-    if (b->pending && s->queued) return b->fail(TMPM_ERR_PENDING_STEPS, "the scene is in the batch in flight");
     if (out->count != s->world.n) return b->fail(TMPM_ERR_INVALID_INPUT, "output array count does not match the scene");
     cudaSetDevice(b->device);
     st = b->refresh(*s);

@@ -1,13 +1,13 @@
 """Serving loop: continuous batching of MPM scenes on one device.
 
 Requests (a scene and a substep count) arrive over time.  Arrived requests
-are prepared (validated and packed into pinned memory) on worker threads
+are prepared (validated and packed for upload) on worker threads
 while the device runs, admitted in arrival order while their device
 footprint fits the HBM budget and a scene slot is free, and advanced
 together: every batch moves each resident scene by up to `chunk` substeps
-in one set of launches.  A scene that finishes in a batch is collected
-(copied to pinned memory right after that batch), read while the next batch
-runs, and retired, which frees its budget.  Requests that arrive while
+in one set of launches.  A scene that finishes in a batch is read while the
+next batch runs (the batch does not touch it) and retired, which frees its
+budget.  Requests that arrive while
 others are on the device therefore join at the next batch boundary instead
 of waiting for the device to drain.
 
@@ -121,7 +121,7 @@ class Server:
         outcomes = {r.rid: Outcome(r.rid, r.arrival, r.steps, r.scene.particles.count) for r in reqs}
         waiting: deque = deque()  # [request, future]
         resident: dict[int, list] = {}  # scene id -> [request, remaining, bytes]
-        finished: list[int] = []  # collected in the last batch, to read and retire
+        finished: list[int] = []  # finished in the last batch, to read and retire
         nxt = 0
         pool = ThreadPoolExecutor(max_workers=max(1, self.workers))
         t0 = self.clock()
@@ -194,8 +194,7 @@ class Server:
                     elif nxt < len(reqs):
                         time.sleep(max(0.0, min(reqs[nxt].arrival - now(), 0.005)))
                     continue
-                collect = [sid for sid, k in active.items() if resident[sid][1] <= k]
-                self.batch.submit(active, collect)
+                self.batch.submit(active)
                 self.batches += 1
                 self.peak_resident = max(self.peak_resident, len(resident))
                 self.peak_bytes = max(self.peak_bytes, self.used)

@@ -186,7 +186,7 @@ def test_batch_rejects_invalid_requests():
     assert b.device_bytes() > scene_bytes(sc.particles.count, home_blocks(sc.particles.position, 1.0 / 16)) // 4
 
 
-def test_admission_while_a_batch_is_in_flight_and_collected_results():
+def test_admission_and_reads_while_a_batch_is_in_flight():
     from tessera_b200.batch import PreparedScene
     scs = small_scenes(count=3, cells=5, seed=17)
     b = Batch()
@@ -200,16 +200,18 @@ def test_admission_while_a_batch_is_in_flight_and_collected_results():
         b.particles(a)  # in flight
     assert e.value.status == TMPM_ERR_PENDING_STEPS
     b.synchronize()
-    b.run({a: 8, c: 8}, collect={a, c})
-    assert_close(alone(scs[0], 16), b.particles(a), what="resident scene")
-    b.submit({c: 4}, collect={c})
-    # `a` was collected and is not in flight: readable while the batch runs
-    assert_close(alone(scs[0], 16), b.particles(a), what="collected scene during a batch")
+    b.run({a: 8, c: 8})
+    b.submit({c: 4})
+    # `a` is not in the batch in flight: it is read from the rows that batch re-sorts from
+    assert_close(alone(scs[0], 16), b.particles(a), what="scene beside a running batch")
+    with pytest.raises(TesseraError) as e:
+        b.particles(c)
+    assert e.value.status == TMPM_ERR_PENDING_STEPS
     b.synchronize()
     assert_close(alone(scs[1], 12), b.particles(c), what="admitted-in-flight scene")
     # retire while a batch is in flight
     d = b.admit(PreparedScene(scs[2].params, scs[2].particles, scs[2].dt))
-    b.submit({a: 4, c: 4, d: 4}, collect={a})
+    b.submit({a: 4, c: 4, d: 4})
     b.remove_scene(a)
     b.synchronize()
     assert_close(alone(scs[1], 16), b.particles(c), what="scene beside a retired one")

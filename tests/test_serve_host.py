@@ -43,7 +43,7 @@ class FakeBatch:
         self.log.append(("admit", sid))
         return sid
 
-    def submit(self, steps, collect=()):
+    def submit(self, steps):
         assert self.in_flight is None
         self.in_flight = dict(steps)
         self.log.append(("submit", tuple(sorted(steps.items()))))
