@@ -46,8 +46,8 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 BATCH = 64
-# re-sort per batch: bin keys, 3 radix passes (21-bit keys) x (hist, scan, scatter), gather
-RESORT_LAUNCHES = 1 + 3 * 3 + 1
+# re-sort per batch: bin keys, 4 radix passes (27-bit keys) x (hist, scan, scatter), gather
+RESORT_LAUNCHES = 1 + 4 * 3 + 1
 METRIC = "particle-substeps/s"
 
 

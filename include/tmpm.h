@@ -243,9 +243,11 @@ TmpmStatus tmpm_step_cfl_with_reactions(TmpmSession *session, double dt,
  * the binning step of the substep on `count` f32 positions stored
  * component-major on the device (x[0..count), then y and z, `stride` floats
  * apart) and writes, to caller-owned device buffers, the stable order of the
- * particles by the 21-bit Morton key of their 4^3 grid block (block
- * coordinates taken modulo 128) (order_out) and, when
- * keys_out is not NULL, the sorted keys.  `stream` is a cudaStream_t (NULL =
+ * particles by their sort key (order_out) and, when
+ * keys_out is not NULL, the sorted keys.  The key is the 21-bit Morton code
+ * of the particle's 4^3 grid block (block coordinates taken modulo 128)
+ * followed by the 6-bit Morton code of its cell inside the block, the key a
+ * session's re-sort uses.  `stream` is a cudaStream_t (NULL =
  * the default stream); the call is asynchronous on it.
  * It allocates nothing: its scratch is a fixed array inside the library
  * (about 4.1 MB, held on every device that loads the library until exit), so

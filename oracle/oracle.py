@@ -288,9 +288,31 @@ def block_morton_keys(base_cells: np.ndarray, scene: int = 0) -> np.ndarray:
     return (np.uint32(scene & 0xFF) << np.uint32(21)) | m
 
 
+def cell_sort_keys(base_cells: np.ndarray) -> np.ndarray:
+    """Single-scene sort key: the block's 21-bit Morton code << 6 | the 6-bit Morton
+    code of the cell inside its 4^3 block."""
+    c = np.asarray(base_cells, dtype=np.int32).astype(np.uint32) & np.uint32(3)
+    x, y, z = c[:, 0], c[:, 1], c[:, 2]
+    cell = (((x & 2) << 4) | ((y & 2) << 3) | ((z & 2) << 2) | ((x & 1) << 2) | ((y & 1) << 1) | (z & 1))
+    return (block_morton_keys(base_cells) << np.uint32(6)) | cell.astype(np.uint32)
+
+
 def binning_reference(position_f32: np.ndarray, cell_width: float):
-    """(base cells, Morton keys, stable sort permutation) for device-order positions."""
+    """(base cells, sort keys, stable sort permutation) for device-order positions."""
     cells = base_cells_f32(position_f32, cell_width)
-    keys = block_morton_keys(cells)
+    keys = cell_sort_keys(cells)
     perm = np.argsort(keys, kind="stable").astype(np.uint32)
     return cells, keys, perm
+
+
+def storage_order(perm: np.ndarray, chunk: int = 256, group: int = 8) -> np.ndarray:
+    """Device storage order after a single-scene re-sort: each full chunk of 256
+    sorted particles is stored transposed (position kk holds sorted element
+    (kk % 32) * 8 + kk // 32 of its chunk); the last partial chunk is in order."""
+    perm = np.asarray(perm)
+    n = len(perm)
+    src = np.arange(n)
+    full = (n // chunk) * chunk
+    kk = np.arange(full) % chunk
+    src[:full] = (np.arange(full) // chunk) * chunk + (kk % 32) * group + kk // 32
+    return perm[src]

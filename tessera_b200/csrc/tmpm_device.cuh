@@ -566,6 +566,13 @@ __device__ __forceinline__ uint32_t spread10(uint32_t v) {
     return v;
 }
 
+// 6-bit Morton code of a cell's position inside its 4^3 block.
+__device__ __forceinline__ uint32_t cell_in_block(int cx, int cy, int cz) {
+    const uint32_t x = static_cast<uint32_t>(cx) & 3u, y = static_cast<uint32_t>(cy) & 3u,
+                   z = static_cast<uint32_t>(cz) & 3u;
+    return ((x & 2u) << 4) | ((y & 2u) << 3) | ((z & 2u) << 2) | ((x & 1u) << 2) | ((y & 1u) << 1) | (z & 1u);
+}
+
 // Sort key of a block: scene index (8 bits) above the 21-bit Morton code of the
 // block coordinates taken modulo 128 (512 cells per axis); bit 29 marks
 // particles of removed scenes (kDeadKey).

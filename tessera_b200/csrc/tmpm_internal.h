@@ -103,7 +103,8 @@ struct GridTable {
 constexpr int kSceneShift = 8;
 constexpr int kMaxScenes = 256;   // scenes per batch (16-bit namespace field of the block key)
 constexpr int kMaxBatchColors = 256;
-constexpr int kSortBitsScene = 21;            // single scene: 21-bit block Morton key
+constexpr int kSortBitsScene = 27;            // single scene: 21-bit block Morton key << 6 | cell in block
+constexpr int kInterleave = 8;                // particles per lane group in the storage interleave (see k_gather)
 constexpr int kSortBitsBatch = 30;            // batch: scene << 21 | Morton, plus the removed-scene bit
 constexpr uint32_t kDeadKey = 0x3FFFFFFFu;
 

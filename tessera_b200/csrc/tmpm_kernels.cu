@@ -20,7 +20,7 @@
 #include "tmpm_device.cuh"
 
 #ifndef TMPM_TRANSFER_MIN_BLOCKS
-#define TMPM_TRANSFER_MIN_BLOCKS 3  // CTAs per SM the transfer kernels are compiled for (measured best)
+#define TMPM_TRANSFER_MIN_BLOCKS 4  // CTAs per SM the transfer kernels are compiled for (measured best of 2-6)
 #endif
 
 namespace tmpm {
@@ -757,8 +757,11 @@ __global__ void k_clear_table(GridTable g) {
     if (gtid == 0) *g.count = 0;
 }
 
-// Block sort key of each particle.  With a scene table (multi-scene batch) the
-// scene comes from the particle's class and its cell width from the table.
+// Sort key of each particle.  Single scene: the block's 21-bit Morton code
+// followed by the cell's 6-bit Morton code inside the block, so particles of
+// one cell are contiguous after the sort.  With a scene table (multi-scene
+// batch): scene << 21 | block Morton, the scene from the particle's class and
+// its cell width from the table.
 __global__ void k_bin_keys(const float *x, size_t cap, int n, float inv_h, const uint32_t *__restrict__ cls,
                            const DevClass *__restrict__ classes, const SceneParams *__restrict__ scenes,
                            int32_t *cells, uint32_t *keys, uint32_t *vals) {
@@ -780,15 +783,28 @@ __global__ void k_bin_keys(const float *x, size_t cap, int n, float inv_h, const
         cells[3 * i + 1] = b1;
         cells[3 * i + 2] = b2;
     }
-    keys[i] = morton_block(b0 >> kBlockShift, b1 >> kBlockShift, b2 >> kBlockShift, scene);
+    const uint32_t block = morton_block(b0 >> kBlockShift, b1 >> kBlockShift, b2 >> kBlockShift, scene);
+    keys[i] = scenes ? block : (block << 6) | cell_in_block(b0, b1, b2);
     if (vals) vals[i] = static_cast<uint32_t>(i);
 }
 
-// dst[j] = src[perm[j]] for every particle field.
-__global__ void k_gather(ParticleSoA src, ParticleSoA dst, const uint32_t *__restrict__ perm, int n) {
+// dst[j] = src[perm[s(j)]] for every particle field.  With `interleave`, each
+// full chunk of kTransferThreads sorted particles (one transfer CTA) is stored
+// transposed: thread kk of the chunk (warp w = kk / 32, lane l = kk % 32) holds
+// sorted particle l * 8 + w, so the 32 lanes of a warp take one particle from
+// each of 32 consecutive groups of 8 (cell-sorted: ~one cell each) and their
+// stencils do not collide on the same shared-memory node.  The last, partial
+// chunk is stored in sorted order.
+__global__ void k_gather(ParticleSoA src, ParticleSoA dst, const uint32_t *__restrict__ perm, int n, int interleave) {
     int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= n) return;
-    int s = static_cast<int>(perm[j]);
+    int sj = j;
+    const int chunk = j / kTransferThreads;
+    if (interleave && (chunk + 1) * kTransferThreads <= n) {
+        const int kk = j - chunk * kTransferThreads;
+        sj = chunk * kTransferThreads + (kk % 32) * kInterleave + kk / 32;
+    }
+    int s = static_cast<int>(perm[sj]);
     const size_t cs = src.cap, cd = dst.cap;
     for (int c = 0; c < 3; ++c) {
         dst.x[c * cd + j] = src.x[c * cs + s];
@@ -899,7 +915,7 @@ void launch_resort(ParticleSoA &src, ParticleSoA &dst, int n, int keep, const De
     k_bin_keys<<<(n + 255) / 256, 256, 0, stream>>>(src.x, src.cap, n, sp.s0.inv_h, src.cls, classes,
                                                     sp.multi ? sp.scenes : nullptr, nullptr, sb.keys[0], sb.vals[0]);
     const int r = radix_sort_pairs(sb, n, sp.multi ? kSortBitsBatch : kSortBitsScene, stream);
-    if (keep > 0) k_gather<<<(keep + 255) / 256, 256, 0, stream>>>(src, dst, sb.vals[r], keep);
+    if (keep > 0) k_gather<<<(keep + 255) / 256, 256, 0, stream>>>(src, dst, sb.vals[r], keep, sp.multi ? 0 : 1);
 }
 
 void launch_dump_grid(const GridTable &g, int32_t *cells, float4 *values, uint32_t *count, uint32_t capacity,

@@ -209,10 +209,10 @@ def test_binning_and_sort_order_are_bit_exact():
     ref_cells, ref_keys, ref_perm = O.binning_reference(pos32, sc.params.cell_width)
     assert np.array_equal(cells0, ref_cells)
     assert np.array_equal(keys0, ref_keys)
-    s.submit_steps(1)  # the batch opens by re-sorting storage by block key
+    s.submit_steps(1)  # the batch opens by re-sorting storage by (block, cell) key
     s.synchronize()
     widx1, cells1, keys1 = s.debug_binning()
-    assert np.array_equal(widx1, widx0[ref_perm])
+    assert np.array_equal(widx1, widx0[O.storage_order(ref_perm)])
     # after one substep the device positions (read back exactly) re-bin identically
     pos1 = s.particles().position.astype(np.float32)[widx1]
     c1, k1, _ = O.binning_reference(pos1, sc.params.cell_width)

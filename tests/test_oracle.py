@@ -544,3 +544,12 @@ def test_binning_reference_is_stable_and_blocks_match_floor_division():
     assert np.all(perm[1:][same] > perm[:-1][same])  # stability
     blocks = np.floor_divide(cells, 4)
     assert np.array_equal(np.right_shift(cells, 2), blocks)
+    # the key orders by block first, then by cell inside the block
+    assert np.array_equal(keys >> 6, O.block_morton_keys(cells))
+    inner = cells & 3
+    assert np.array_equal(keys & 63 == 0, np.all(inner == 0, axis=1))
+    # storage order: a permutation, transposed within full 256-chunks
+    order = O.storage_order(perm)
+    assert np.array_equal(np.sort(order), np.sort(perm))
+    assert order[1] == perm[8] and order[32] == perm[1] and np.array_equal(order[-(len(perm) % 256):],
+                                                                            perm[-(len(perm) % 256):])

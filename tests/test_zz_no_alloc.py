@@ -5,7 +5,8 @@ loops, hosts that own every device buffer, graph-recording code).  The test
 calls it through the C ABI on two scenes in a row, with caller-owned device
 buffers, and checks it against the session path: the block keys must equal
 tmpm_debug_binning's keys, and the order must equal the storage order the
-session's re-sort produces.  Both are integer results, so the match is exact.
+session's re-sort produces (each full chunk of 256 sorted particles stored
+transposed).  Both are integer results, so the match is exact.
 This file sorts last so that a run stopping at the first failure has already
 run every other test.
 """
@@ -15,6 +16,7 @@ import ctypes as C
 import numpy as np
 import pytest
 
+from oracle import oracle as O
 from tessera_b200 import _native, scenes
 from tessera_b200._abi import TMPM_ERR_CAPACITY, TMPM_OK
 from tessera_b200.session import Session
@@ -58,7 +60,8 @@ def test_noalloc_binning_matches_session_on_two_calls(call):
         order, keys = noalloc_sort(scene.particles.position.astype(np.float32), scene.params.cell_width)
         ref_order, ref_keys = session_binning(scene)
         assert np.array_equal(keys, np.sort(ref_keys, kind="stable"))
-        assert np.array_equal(order, ref_order)
+        # the session stores each full 256-particle chunk of the sorted order transposed
+        assert np.array_equal(O.storage_order(order), ref_order)
 
 
 def test_noalloc_rejects_counts_beyond_the_scratch_limit():
