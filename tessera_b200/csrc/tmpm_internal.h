@@ -43,8 +43,11 @@ constexpr int kMatSnow = 4;
 constexpr int kMatSand = 5;
 constexpr int kMatSandNeoHookean = 6;
 
-constexpr int kTransferThreads = 256;  // particles per CTA of the transfer kernels
-constexpr int kCacheStride = 80;       // per-CTA record: 8-int box header + up to 64 block ids
+#ifndef TMPM_TRANSFER_THREADS
+#define TMPM_TRANSFER_THREADS 256
+#endif
+constexpr int kTransferThreads = TMPM_TRANSFER_THREADS;  // particles per CTA of the transfer kernels
+constexpr int kCacheStride = 144;      // per-CTA record: 16-int box header + up to 128 block ids
 
 constexpr uint32_t kFixedBit = 0x80000000u;
 constexpr uint32_t kClassMask = 0x7FFFFFFFu;
@@ -104,7 +107,11 @@ constexpr int kSceneShift = 8;
 constexpr int kMaxScenes = 256;   // scenes per batch (16-bit namespace field of the block key)
 constexpr int kMaxBatchColors = 256;
 constexpr int kSortBitsScene = 27;            // single scene: 21-bit block Morton key << 6 | cell in block
-constexpr int kInterleave = 8;                // particles per lane group in the storage interleave (see k_gather)
+#ifndef TMPM_RESORT_SUBSTEPS
+#define TMPM_RESORT_SUBSTEPS 64
+#endif
+constexpr uint32_t kResortSubsteps = TMPM_RESORT_SUBSTEPS;  // default substeps between re-sorts of a session
+constexpr int kInterleave = kTransferThreads / 32;  // particles per lane group in the storage interleave (k_gather)
 constexpr int kSortBitsBatch = 30;            // batch: scene << 21 | Morton, plus the removed-scene bit
 constexpr uint32_t kDeadKey = 0x3FFFFFFFu;
 

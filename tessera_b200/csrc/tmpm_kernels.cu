@@ -28,9 +28,9 @@ namespace tmpm {
 namespace {
 
 constexpr int kThreads = kTransferThreads;
-constexpr int kTileMaxDim = 12;
-constexpr int kTileMaxNodes = 1024;
-constexpr int kMaxTileBlocks = 64;
+constexpr int kTileMaxDim = 16;     // box edge in cells
+constexpr int kTileMaxNodes = 2048; // box nodes: one 32 KB shared buffer, gather tile then scatter tile
+constexpr int kMaxTileBlocks = kCacheStride - 16;
 constexpr int kCacheHeader = 16;
 constexpr uint32_t kFatal = kStatusCapacity | kStatusTimeout | kStatusResident;
 
@@ -116,6 +116,70 @@ __device__ __forceinline__ void reduce_box(bool valid, const int b[3], uint32_t 
     __syncthreads();
 }
 
+// Box of base cells and colours plus two float sums over the CTA, with one
+// barrier: each warp reduces its lanes and publishes a partial, then every
+// warp combines the partials itself (no second barrier, no shared result).
+__device__ __forceinline__ void reduce_box_sums(bool valid, const int b[3], uint32_t color, float &sum_a, float &sum_b,
+                                                int (*red)[8], float (*redf)[2], Box &box) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int r[8];
+    for (int a = 0; a < 3; ++a) {
+        r[a] = __reduce_min_sync(0xffffffffu, valid ? b[a] : INT_MAX);
+        r[3 + a] = __reduce_max_sync(0xffffffffu, valid ? b[a] : INT_MIN);
+    }
+    r[6] = __reduce_min_sync(0xffffffffu, valid ? static_cast<int>(color) : INT_MAX);
+    r[7] = __reduce_max_sync(0xffffffffu, valid ? static_cast<int>(color) : INT_MIN);
+    float fa = sum_a, fb = sum_b;
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        fa += __shfl_xor_sync(0xffffffffu, fa, off);
+        fb += __shfl_xor_sync(0xffffffffu, fb, off);
+    }
+    if (lane == 0) {
+        for (int a = 0; a < 8; ++a) red[warp][a] = r[a];
+        redf[warp][0] = fa;
+        redf[warp][1] = fb;
+    }
+    __syncthreads();
+    constexpr int kWarps = kThreads / 32;
+    const bool mine = lane < kWarps;
+    int m[8];
+    for (int a = 0; a < 3; ++a) {
+        m[a] = __reduce_min_sync(0xffffffffu, mine ? red[lane][a] : INT_MAX);
+        m[3 + a] = __reduce_max_sync(0xffffffffu, mine ? red[lane][3 + a] : INT_MIN);
+    }
+    m[6] = __reduce_min_sync(0xffffffffu, mine ? red[lane][6] : INT_MAX);
+    m[7] = __reduce_max_sync(0xffffffffu, mine ? red[lane][7] : INT_MIN);
+    fa = mine ? redf[lane][0] : 0.0f;
+    fb = mine ? redf[lane][1] : 0.0f;
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        fa += __shfl_xor_sync(0xffffffffu, fa, off);
+        fb += __shfl_xor_sync(0xffffffffu, fb, off);
+    }
+    sum_a = fa;
+    sum_b = fb;
+    bool ok = m[0] <= m[3] && m[6] == m[7];
+    int nodes = 1, nbt = 1;
+    for (int a = 0; a < 3 && ok; ++a)
+        if (static_cast<long long>(m[3 + a]) - m[a] + 3 > kTileMaxDim) ok = false;
+    if (ok) {
+        for (int a = 0; a < 3; ++a) {
+            box.lo[a] = m[a];
+            box.dim[a] = m[3 + a] - m[a] + 3;
+            box.blo[a] = m[a] >> kBlockShift;
+            box.nb[a] = ((m[3 + a] + 2) >> kBlockShift) - box.blo[a] + 1;
+            nodes *= box.dim[a];
+            nbt *= box.nb[a];
+        }
+        ok = nodes <= kTileMaxNodes && nbt <= kMaxTileBlocks;
+    }
+    box.nodes = nodes;
+    box.nbt = nbt;
+    box.ok = ok ? 1 : 0;
+    box.color = static_cast<uint32_t>(m[6]);
+}
+
 __device__ __forceinline__ void quad_weights(float f, float w[3]) {
     w[0] = 0.5f * (1.5f - f) * (1.5f - f);
     w[1] = 0.75f - (f - 1.0f) * (f - 1.0f);
@@ -157,28 +221,6 @@ __device__ __forceinline__ void add_reaction(double *reactions, int oi, V3f cent
     atomicAdd(r + 5, static_cast<double>(ang.z));
 }
 
-// Block-wide sums of two floats (all threads get the totals).
-__device__ __forceinline__ void block_sum2(float &a, float &b, float (*red)[2]) {
-    int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1) {
-        a += __shfl_xor_sync(0xffffffffu, a, off);
-        b += __shfl_xor_sync(0xffffffffu, b, off);
-    }
-    if (lane == 0) {
-        red[warp][0] = a;
-        red[warp][1] = b;
-    }
-    __syncthreads();
-    a = 0.f;
-    b = 0.f;
-#pragma unroll
-    for (int w = 0; w < kThreads / 32; ++w) {
-        a += red[w][0];
-        b += red[w][1];
-    }
-}
-
 // Largest power of two s with total * s <= 2^30 (exponent clamped to the normal range).
 __device__ __forceinline__ float pow2_scale(float total) {
     float e = floorf(30.0f - log2f(fmaxf(total, 1e-30f)));
@@ -197,8 +239,11 @@ __global__ void __launch_bounds__(kThreads, TMPM_TRANSFER_MIN_BLOCKS)
     k_transfer(ParticleSoA P, int n, const DevClass *__restrict__ classes, GridTable cur, GridTable next,
                SimParams sp, const DevObstacle *__restrict__ obstacles, const float *__restrict__ planes,
                double *reactions, uint32_t *status, int *__restrict__ cache) {
-    __shared__ float4 s_gv[kTileMaxNodes];
-    __shared__ __align__(16) int s_sc[4][kTileMaxNodes];
+    // One buffer holds the G2P gather tile (float4 per node) and then the P2G
+    // scatter tile (4 fixed-point ints per node, component-major).
+    __shared__ float4 s_tile[kTileMaxNodes];
+    float4 *const s_gv = s_tile;
+    int (*const s_sc)[kTileMaxNodes] = reinterpret_cast<int (*)[kTileMaxNodes]>(s_tile);
     __shared__ float s_fred[kThreads / 32][2];
     __shared__ int s_blk[kMaxTileBlocks];
     __shared__ int s_blk2[kMaxTileBlocks];
@@ -214,9 +259,7 @@ __global__ void __launch_bounds__(kThreads, TMPM_TRANSFER_MIN_BLOCKS)
 
     if (threadIdx.x == 0) s_abort = (*reinterpret_cast<volatile uint32_t *>(status) & kFatal) != 0;
     if (MODE != kModeG2P) {
-        // The scatter tile is zeroed up front; the first barrier of the kernel orders it.
-        int4 *z = reinterpret_cast<int4 *>(&s_sc[0][0]);
-        for (int t = threadIdx.x; t < kTileMaxNodes; t += kThreads) z[t] = make_int4(0, 0, 0, 0);
+        // The first barrier of the kernel orders these.
         for (int t = threadIdx.x; t < kMaxTileBlocks; t += kThreads) s_used[t] = 0;
     }
 
@@ -517,9 +560,6 @@ __global__ void __launch_bounds__(kThreads, TMPM_TRANSFER_MIN_BLOCKS)
         if (sp.resident_checks) atomicOr(resident_flag, kStatusResident);
         else atomicOr(status, kStatusCapacity);
     }
-    reduce_box(active, b, k.color, s_red, s_box);
-    if (MODE == kModeP2G && s_abort) return;
-    const Box bx = s_box;
     const V3f gp = mk(x.x * inv_h, x.y * inv_h, x.z * inv_h);
     const V3f fx = mk(gp.x - static_cast<float>(b[0]), gp.y - static_cast<float>(b[1]), gp.z - static_cast<float>(b[2]));
     float wx[3], wy[3], wz[3];
@@ -542,12 +582,23 @@ __global__ void __launch_bounds__(kThreads, TMPM_TRANSFER_MIN_BLOCKS)
         bound_p = fmaxf(fmaxf(fabsf(mv.x) + 1.5f * h * r0, fabsf(mv.y) + 1.5f * h * r1), fabsf(mv.z) + 1.5f * h * r2);
         if (!(bound_p < 1e30f)) bound_p = 1e30f;  // non-finite state is flagged by the G2P checks
     }
+    // the CTA's box and the sums of the bounds, with one barrier
+    float tot_m = bound_m, tot_p = bound_p;
+    Box bx;
+    reduce_box_sums(active, b, k.color, tot_m, tot_p, s_red, s_fred, bx);
+    if (MODE == kModeP2G && s_abort) return;
     if (bx.ok) {
+        // every warp has finished its gather (barrier above): the buffer becomes the scatter tile
+        for (int t = threadIdx.x; t < bx.nodes; t += kThreads) {
+            s_sc[0][t] = 0;
+            s_sc[1][t] = 0;
+            s_sc[2][t] = 0;
+            s_sc[3][t] = 0;
+        }
+        __syncthreads();
         // Shared accumulation in 32-bit fixed point: integer shared atomics are
         // native, float ones are not.  Power-of-two scales from the chunk bounds
         // keep every node sum below 2^30 (no overflow) with unbiased rounding.
-        float tot_m = bound_m, tot_p = bound_p;
-        block_sum2(tot_m, tot_p, s_fred);
         const float sm = pow2_scale(tot_m), spv = pow2_scale(tot_p);
         if (active) {
             const int ox = b[0] - bx.lo[0], oy = b[1] - bx.lo[1], oz = b[2] - bx.lo[2];
@@ -791,10 +842,11 @@ __global__ void k_bin_keys(const float *x, size_t cap, int n, float inv_h, const
 // dst[j] = src[perm[s(j)]] for every particle field.  With `interleave`, each
 // full chunk of kTransferThreads sorted particles (one transfer CTA) is stored
 // transposed: thread kk of the chunk (warp w = kk / 32, lane l = kk % 32) holds
-// sorted particle l * 8 + w, so the 32 lanes of a warp take one particle from
-// each of 32 consecutive groups of 8 (cell-sorted: ~one cell each) and their
-// stencils do not collide on the same shared-memory node.  The last, partial
-// chunk is stored in sorted order.
+// sorted particle l * G + w with G = kTransferThreads / 32, so the 32 lanes of
+// a warp take one particle from each of 32 consecutive groups of G
+// (cell-sorted: one or two cells each) and their stencils do not collide on
+// the same shared-memory node.  The last, partial chunk is stored in sorted
+// order.
 __global__ void k_gather(ParticleSoA src, ParticleSoA dst, const uint32_t *__restrict__ perm, int n, int interleave) {
     int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= n) return;

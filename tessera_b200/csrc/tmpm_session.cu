@@ -302,8 +302,16 @@ struct TmpmSession {
             cudaEventCreate(&ev[0]);
             cudaEventCreate(&ev[1]);
         }
-        uint32_t interval = options.resort_interval;
-        bool resort_now = interval == 0 ? true : since_resort >= interval;
+        // The batch runs in segments ending at re-sort points: a re-sort every
+        // `interval` substeps keeps each CTA's particles inside a compact box as
+        // they move (the fused transfer slows as boxes widen).  A segment ends
+        // with a G2P-only transfer (the fused one keeps v and C in registers)
+        // and the next opens with re-sort, table clear and P2G.
+        const uint32_t interval = options.resort_interval ? options.resort_interval : kResortSubsteps;
+        uint32_t done = 0;
+        while (done < steps) {
+        const bool resort_now = since_resort >= interval;
+        const uint32_t seg = std::min<uint32_t>(steps - done, resort_now ? interval : interval - since_resort);
         if (resort_now) {
             tick(0);
             ParticleSoA src = soa();
@@ -329,24 +337,27 @@ struct TmpmSession {
         launch_transfer(kModeP2G, P, n_dev, classes.ptr, g[1], g[0], sp, dev_obstacles.ptr, dev_planes.ptr,
                         reactions.ptr, status.ptr, cta_cache.ptr, stream);
         tock(0);
-        for (uint32_t s = 0; s < steps; ++s) {
+        for (uint32_t s = 0; s < seg; ++s) {
             const GridTable &gc = g[s & 1], &gn = g[(s + 1) & 1];
             tick(0);
             launch_grid_update(gc, gn, sp, dev_obstacles.ptr, dev_planes.ptr, reactions.ptr, status.ptr, stream);
             tock(1);
             SimParams spk = sp;
-            spk.apply_force = (s == 0 && force_dirty) ? 1 : 0;
-            bool last = s + 1 == steps;
+            const bool first = done == 0 && s == 0;
+            spk.apply_force = (first && force_dirty) ? 1 : 0;
+            bool last = s + 1 == seg;
             tick(0);
             launch_transfer(last ? kModeG2P : kModeG2P2G, P, n_dev, classes.ptr, gc, gn, spk, dev_obstacles.ptr,
                             dev_planes.ptr, reactions.ptr, status.ptr, cta_cache.ptr, stream);
             tock(last ? 3 : 2);
-            if (s == 0 && force_dirty) {
+            if (first && force_dirty) {
                 cudaMemsetAsync(force.ptr, 0, sizeof(float) * force.count, stream);
                 force_dirty = false;
             }
         }
-        since_resort += steps;
+        since_resort += seg;
+        done += seg;
+        }
         if (kernel_ms) {
             cudaEventDestroy(ev[0]);
             cudaEventDestroy(ev[1]);
