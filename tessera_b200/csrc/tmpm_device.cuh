@@ -522,6 +522,54 @@ __device__ __forceinline__ V3f contact_velocity(const DevObstacle &o, V3f point,
     return surface + tangent * sc;
 }
 
+// RigidObstacle::cpic_side for a triangle prism (obstacle.rs:343-370; the
+// reference shader's f32 form with its 1e-5 barycentric margin, gpu.wgsl:82-102):
+// distance to the triangle's plane and the side, when the point projects into
+// the triangle.
+__device__ __forceinline__ bool cpic_side(const DevObstacle &o, V3f point, float &dist, bool &positive) {
+    const V3f local = qrot_inv(o.q, point - mk(o.center[0], o.center[1], o.center[2]));
+    const V3f a = mk(o.verts[0], o.verts[1], o.verts[2]);
+    const V3f eb = mk(o.verts[4], o.verts[5], o.verts[6]) - a, ec = mk(o.verts[8], o.verts[9], o.verts[10]) - a;
+    const V3f n = normalize(cross(eb, ec));
+    const float sd = dot(local - a, n);
+    const V3f proj = local - n * sd - a;
+    const float d00 = dot(eb, eb), d01 = dot(eb, ec), d11 = dot(ec, ec), d20 = dot(proj, eb), d21 = dot(proj, ec);
+    const float den = d00 * d11 - d01 * d01;
+    const float v = (d11 * d20 - d01 * d21) / den, w = (d00 * d21 - d01 * d20) / den;
+    if (v >= -1e-5f && w >= -1e-5f && v + w <= 1.0f + 1e-5f) {
+        dist = fabsf(sd);
+        positive = sd >= 0.0f;
+        return true;
+    }
+    return false;
+}
+
+// Grid namespace of a particle (transfer_key, world.rs:470-490): the transfer
+// colour, and with CPIC the side mask of each CPIC group's closest triangle
+// prism (colour << 8 | mask; groups below kMaxCpicGroups, colours below 256).
+__device__ __forceinline__ uint32_t particle_namespace(uint32_t color, int cpic, int num_obstacles,
+                                                       const DevObstacle *obstacles, V3f x) {
+    if (!cpic) return color;
+    float best[kMaxCpicGroups];
+    uint32_t mask = 0;
+#pragma unroll
+    for (int g = 0; g < kMaxCpicGroups; ++g) best[g] = 3.0e38f;
+    for (int oi = 0; oi < num_obstacles; ++oi) {
+        const int g = obstacles[oi].cpic_group;
+        if (g < 0 || g >= kMaxCpicGroups) continue;
+        float d;
+        bool pos;
+        if (!cpic_side(obstacles[oi], x, d, pos)) continue;
+#pragma unroll
+        for (int q = 0; q < kMaxCpicGroups; ++q)
+            if (q == g && d < best[q]) {
+                best[q] = d;
+                mask = pos ? (mask | (1u << q)) : (mask & ~(1u << q));
+            }
+    }
+    return (color << 8) | mask;
+}
+
 // ---------------------------------------------------------------- binning
 
 // floor(x * inv_h - 0.5) with IEEE round-to-nearest and no contraction

@@ -126,7 +126,9 @@ struct SimParams {
     int apply_force;
     int resident_checks;  // CFL / escape / conditioning flags (resident path only, gpu.rs:1429)
     int has_plastic;      // some particle class is snow, sand or NH sand
+    int cpic;             // CPIC on: grid namespace = colour << 8 | side mask of the CPIC groups (< 8)
 };
+constexpr int kMaxCpicGroups = 8;
 
 struct ParticleSoA {
     float *x;       // 3 * cap

@@ -229,16 +229,20 @@ __device__ __forceinline__ float pow2_scale(float total) {
 }
 
 // PLASTIC selects the variant that carries plastic state (snow, sand, NH sand);
-// scenes without plastic materials run the leaner variant.  MULTI selects the
-// multi-scene batch variant: each particle reads its scene's parameters from
-// the scene table (scene = class namespace >> kSceneShift) and takes part only
-// in the substeps its scene advances in this batch; the single-scene variant
-// reads them from the kernel parameters.
-template <int MODE, bool PLASTIC, bool MULTI>
+// scenes without plastic materials run the leaner variant.  VARIANT selects
+// kPlain (one scene, parameters from the kernel parameters), kMulti (a
+// multi-scene batch: each particle reads its scene's parameters from the scene
+// table, scene = class namespace >> kSceneShift, and takes part only in the
+// substeps its scene advances in this batch) or kCpic (one scene whose grid
+// namespace includes CPIC side masks).  Each costs registers only where used.
+enum Variant { kPlain = 0, kMulti = 1, kCpic = 2 };
+template <int MODE, bool PLASTIC, int VARIANT>
 __global__ void __launch_bounds__(kThreads, TMPM_TRANSFER_MIN_BLOCKS)
     k_transfer(ParticleSoA P, int n, const DevClass *__restrict__ classes, GridTable cur, GridTable next,
                SimParams sp, const DevObstacle *__restrict__ obstacles, const float *__restrict__ planes,
                double *reactions, uint32_t *status, int *__restrict__ cache) {
+    constexpr bool MULTI = VARIANT == kMulti;
+    constexpr bool CPIC = VARIANT == kCpic;
     // One buffer holds the G2P gather tile (float4 per node) and then the P2G
     // scatter tile (4 fixed-point ints per node, component-major).
     __shared__ float4 s_tile[kTileMaxNodes];
@@ -288,6 +292,8 @@ __global__ void __launch_bounds__(kThreads, TMPM_TRANSFER_MIN_BLOCKS)
         p2g_on = !dead && sp.step_index + 1 < steps;
     }
     uint32_t *const resident_flag = MULTI ? sp.scene_status + scene : status;
+    // grid namespace at the current positions (colour, and CPIC side masks when on)
+    uint32_t ns = CPIC ? particle_namespace(k.color, 1, sp.num_obstacles, obstacles, x) : k.color;
     const bool fixed = (cw & kFixedBit) != 0;
     const bool plastic = PLASTIC && g2p_on && k.kind >= kMatSnow;
     float pl[3] = {1.0f, 0.0f, 0.0f};
@@ -334,7 +340,7 @@ __global__ void __launch_bounds__(kThreads, TMPM_TRANSFER_MIN_BLOCKS)
                 bx.nbt = cc[15];
                 bx.ok = 1;
             } else {
-                reduce_box(g2p_on, b, k.color, s_red, s_box);
+                reduce_box(g2p_on, b, ns, s_red, s_box);
                 bx = s_box;
                 if (bx.ok) {
                     const Split3 split(bx.nb[1], bx.nb[2]);
@@ -348,7 +354,7 @@ __global__ void __launch_bounds__(kThreads, TMPM_TRANSFER_MIN_BLOCKS)
             }
             bool bad = use_cache && g2p_on &&
                        (b[0] < bx.lo[0] || b[1] < bx.lo[1] || b[2] < bx.lo[2] || b[0] + 2 >= bx.lo[0] + bx.dim[0] ||
-                        b[1] + 2 >= bx.lo[1] + bx.dim[1] || b[2] + 2 >= bx.lo[2] + bx.dim[2] || k.color != bx.color);
+                        b[1] + 2 >= bx.lo[1] + bx.dim[1] || b[2] + 2 >= bx.lo[2] + bx.dim[2] || ns != bx.color);
             if (bx.ok && !bad) {
                 const Split3 split(bx.dim[1], bx.dim[2]);
                 for (int t = threadIdx.x; t < bx.nodes; t += kThreads) {
@@ -431,7 +437,7 @@ __global__ void __launch_bounds__(kThreads, TMPM_TRANSFER_MIN_BLOCKS)
                         for (int e = 0; e < 3; ++e) {
                             int cx = b[0] + a, cy = b[1] + c, cz = b[2] + e;
                             unsigned long long key =
-                                block_key(cx >> kBlockShift, cy >> kBlockShift, cz >> kBlockShift, k.color);
+                                block_key(cx >> kBlockShift, cy >> kBlockShift, cz >> kBlockShift, ns);
                             if (key != last_key) {
                                 last_key = key;
                                 last_id = lookup_block(cur, key);
@@ -583,9 +589,10 @@ __global__ void __launch_bounds__(kThreads, TMPM_TRANSFER_MIN_BLOCKS)
         if (!(bound_p < 1e30f)) bound_p = 1e30f;  // non-finite state is flagged by the G2P checks
     }
     // the CTA's box and the sums of the bounds, with one barrier
+    if (MODE != kModeP2G && CPIC) ns = particle_namespace(k.color, 1, sp.num_obstacles, obstacles, x);
     float tot_m = bound_m, tot_p = bound_p;
     Box bx;
-    reduce_box_sums(active, b, k.color, tot_m, tot_p, s_red, s_fred, bx);
+    reduce_box_sums(active, b, ns, tot_m, tot_p, s_red, s_fred, bx);
     if (MODE == kModeP2G && s_abort) return;
     if (bx.ok) {
         // every warp has finished its gather (barrier above): the buffer becomes the scatter tile
@@ -717,10 +724,10 @@ __global__ void __launch_bounds__(kThreads, TMPM_TRANSFER_MIN_BLOCKS)
                     for (int e = 0; e < 3; ++e) {
                         int cx = b[0] + a, cy = b[1] + c, cz = b[2] + e;
                         int gx = cx >> kBlockShift, gy = cy >> kBlockShift, gz = cz >> kBlockShift;
-                        unsigned long long key = block_key(gx, gy, gz, k.color);
+                        unsigned long long key = block_key(gx, gy, gz, ns);
                         if (key != last_key) {
                             last_key = key;
-                            last_id = find_or_insert_block(next, key, make_int4(gx, gy, gz, static_cast<int>(k.color)), status);
+                            last_id = find_or_insert_block(next, key, make_int4(gx, gy, gz, static_cast<int>(ns)), status);
                         }
                         if (last_id < 0) continue;
                         float w = wx[a] * wy[c] * wz[e];
@@ -913,16 +920,19 @@ void launch_transfer(int mode, const ParticleSoA &P, int n, const DevClass *clas
                      double *reactions, uint32_t *status, int *cache, cudaStream_t stream) {
     if (n <= 0) return;
     dim3 grid((n + kThreads - 1) / kThreads);
-#define TMPM_LAUNCH(M, PL, MU) \
-    k_transfer<M, PL, MU><<<grid, kThreads, 0, stream>>>(P, n, classes, cur, next, sp, obstacles, planes, reactions, status, cache)
+#define TMPM_LAUNCH(M, PL, V) \
+    k_transfer<M, PL, V><<<grid, kThreads, 0, stream>>>(P, n, classes, cur, next, sp, obstacles, planes, reactions, status, cache)
 #define TMPM_LAUNCH_MODE(M)                          \
     do {                                             \
         if (sp.multi) {                              \
-            if (pl) TMPM_LAUNCH(M, true, true);      \
-            else TMPM_LAUNCH(M, false, true);        \
+            if (pl) TMPM_LAUNCH(M, true, kMulti);    \
+            else TMPM_LAUNCH(M, false, kMulti);      \
+        } else if (sp.cpic) {                        \
+            if (pl) TMPM_LAUNCH(M, true, kCpic);     \
+            else TMPM_LAUNCH(M, false, kCpic);       \
         } else {                                     \
-            if (pl) TMPM_LAUNCH(M, true, false);     \
-            else TMPM_LAUNCH(M, false, false);       \
+            if (pl) TMPM_LAUNCH(M, true, kPlain);    \
+            else TMPM_LAUNCH(M, false, kPlain);      \
         }                                            \
     } while (0)
     const bool pl = sp.has_plastic != 0;

@@ -98,7 +98,16 @@ struct TmpmSession {
         sp.apply_force = 0;
         sp.resident_checks = resident ? 1 : 0;
         sp.has_plastic = has_plastic ? 1 : 0;
+        sp.cpic = cpic_active() ? 1 : 0;
         return sp;
+    }
+
+    // CPIC applies when enabled and some obstacle carries a CPIC group (world.rs:470-490).
+    bool cpic_active() const {
+        if (!use_cpic) return false;
+        for (const TmpmObstacle &o : obstacles)
+            if (o.cpic_group >= 0) return true;
+        return false;
     }
 
     // validate_resident_world (gpu.rs:664-677)
@@ -120,6 +129,17 @@ struct TmpmSession {
             return fail(TMPM_ERR_INVALID_INPUT, "cell width or substep not representable in f32");
         float inv_h = 1.0f / h32;
         if (!std::isfinite(inv_h)) return fail(TMPM_ERR_INVALID_INPUT, "1 / cell width not representable in f32");
+
+        // CPIC on the device: groups below kMaxCpicGroups and colours below 256
+        // (the namespace is colour << 8 | side mask); other cases need the CPU path.
+        if (cpic_active()) {
+            for (const TmpmObstacle &o : obstacles)
+                if (o.cpic_group >= kMaxCpicGroups)
+                    return fail(TMPM_ERR_RESIDENT_UNAVAILABLE, "CPIC groups above 7 need the CPU path");
+            for (size_t i = 0; i < world.n; ++i)
+                if (world.enabled[i] && world.color[i] >= 256)
+                    return fail(TMPM_ERR_RESIDENT_UNAVAILABLE, "transfer colours above 255 with CPIC need the CPU path");
+        }
 
         // Validate and pack the world straight into pinned staging (stride `cap`).
         ClassTable ct;
