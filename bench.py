@@ -87,32 +87,21 @@ def dist_setup():
 
 
 def allreduce_max(value: float, world: int) -> float:
-    if world == 1:
-        return value
-    import torch
-    import torch.distributed as dist
+    from tessera_b200.replicas import Reducer
 
-    t = torch.tensor([value], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+    return Reducer(world, "cuda").max(value)
 
 
 def allreduce_sum(value: float, world: int) -> float:
-    if world == 1:
-        return value
-    import torch
-    import torch.distributed as dist
+    from tessera_b200.replicas import Reducer
 
-    t = torch.tensor([value], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.SUM)
-    return float(t.item())
+    return Reducer(world, "cuda").sum(value)
 
 
 def barrier(world: int):
-    if world > 1:
-        import torch.distributed as dist
+    from tessera_b200.replicas import Reducer
 
-        dist.barrier()
+    Reducer(world, "cuda").barrier()
 
 
 class ClockSampler:
