@@ -488,6 +488,7 @@ struct TmpmAdjoint {
     TmpmStatus forward(const double *v0, const double *young, double *x_out, double *v_out) {
         // inputs -> the host world (for the CFL check) and the device initial state
         std::vector<float> Ef(n);
+        ++world.version;
         for (size_t i = 0; i < n; ++i) {
             double e = young ? young[i] : world.mparams[5 * i];
             if (!std::isfinite(e) || !(e > 0.0)) return fail(TMPM_ERR_MPM_INVALID_INPUT, "young's modulus must be positive");

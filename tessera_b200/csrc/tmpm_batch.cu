@@ -75,7 +75,7 @@ TmpmStatus prepare_scene(const TmpmParams &params, const TmpmParticleArrays *par
         return TMPM_ERR_MPM_INVALID_INPUT;
     }
     std::string err;
-    TmpmStatus st = load_checked(particles, p.world, err);
+    TmpmStatus st = load_checked(particles, p.world, err, &params);
     if (st != TMPM_OK) {
         g_last_error = err;
         return st;
@@ -565,6 +565,7 @@ struct TmpmBatch {
             return s.status;
         }
         HostWorld &w = s.world;
+        ++w.version;
         parallel_for(m, [&](size_t a, size_t b) {
             for (size_t j = a; j < b; ++j) {
                 size_t i = widx[j];

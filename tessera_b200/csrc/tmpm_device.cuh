@@ -62,7 +62,9 @@ __device__ __forceinline__ M3f mul_bt(const M3f &a, const M3f &b) {
 
 // Polar factor R of F by Newton's iteration R <- (R + R^-T) / 2, the iteration
 // the reference shader uses (gpu.wgsl:467-482, ten steps); it stops early once
-// the update is below f32 resolution.  R^-T = cofactor(R) / det(R).
+// the squared update falls below 1e-11: the iteration converges quadratically,
+// so the iterate it returns is then accurate to ~1e-11, below f32 resolution.
+// R^-T = cofactor(R) / det(R).
 __device__ __forceinline__ M3f polar_rotation(const M3f &F) {
     M3f R = F;
 #pragma unroll 1
@@ -74,7 +76,7 @@ __device__ __forceinline__ M3f polar_rotation(const M3f &F) {
         M3f next = M3f{(a + bc * inv) * 0.5f, (b + ca * inv) * 0.5f, (c + ab * inv) * 0.5f};
         M3f diff = sub(next, R);
         R = next;
-        if (fro2(diff) < 1e-14f) break;
+        if (fro2(diff) < 1e-11f) break;
     }
     return R;
 }

@@ -76,6 +76,11 @@ using HostVec = std::vector<T, NoInitAlloc<T>>;
 
 struct HostWorld {
     size_t n = 0;
+    // Any change of positions, velocities, deformation or materials bumps
+    // `version`; stable_timestep() caches its result per version and params.
+    uint64_t version = 0;
+    mutable uint64_t cfl_version = ~0ull;
+    mutable double cfl_h = 0.0, cfl_max = 0.0, cfl_value = 0.0;
     HostVec<double> pos, vel, F, C, force, mass, vol, radius, damping, plastic, mparams;
     HostVec<int32_t> material;
     HostVec<uint8_t> enabled, fixed;
@@ -86,6 +91,7 @@ struct HostWorld {
     // Sizes every field for `count` particles; existing storage is reused and
     // not cleared (load() writes every element).
     void resize(size_t count) {
+        ++version;
         n = count;
         pos.resize(3 * n);
         vel.resize(3 * n);
@@ -175,6 +181,7 @@ struct HostWorld {
     }
 
     void append(const HostWorld &o) {
+        ++version;
         auto cat = [](auto &dst, const auto &src) { dst.insert(dst.end(), src.begin(), src.end()); };
         cat(pos, o.pos);
         cat(vel, o.vel);
@@ -198,6 +205,7 @@ struct HostWorld {
 
     // Keep particles whose chunk differs (world.rs:267-277).
     size_t remove_chunk(uint64_t c) {
+        ++version;
         size_t w = 0;
         for (size_t i = 0; i < n; ++i) {
             if (chunk[i] == c) continue;
@@ -352,6 +360,7 @@ inline bool params_valid(const TmpmParams &p) {  // world.rs:51-65
 }
 
 inline double stable_timestep(const HostWorld &w, const TmpmParams &p) {  // world.rs:288-303
+    if (w.cfl_version == w.version && w.cfl_h == p.cell_width && w.cfl_max == p.max_substep) return w.cfl_value;
     std::vector<double> part(host_threads() + 1, p.max_substep);
     parallel_chunks(w.n, [&](size_t c, size_t lo, size_t hi) {
         double dt = p.max_substep;
@@ -364,7 +373,11 @@ inline double stable_timestep(const HostWorld &w, const TmpmParams &p) {  // wor
     });
     double dt = p.max_substep;
     for (double d : part) dt = std::min(dt, d);
-    return std::min(dt, p.max_substep);
+    w.cfl_version = w.version;
+    w.cfl_h = p.cell_width;
+    w.cfl_max = p.max_substep;
+    w.cfl_value = std::min(dt, p.max_substep);
+    return w.cfl_value;
 }
 
 // RigidObstacle::is_valid (obstacle.rs:264-341)
@@ -588,7 +601,8 @@ inline SceneParams scene_params(const TmpmParams &params, double dt) {
 }
 
 // Load and validate caller arrays (MpmWorld::add_particle checks, world.rs:492-503).
-inline TmpmStatus load_checked(const TmpmParticleArrays *particles, HostWorld &out, std::string &err) {
+inline TmpmStatus load_checked(const TmpmParticleArrays *particles, HostWorld &out, std::string &err,
+                               const TmpmParams *cfl_params = nullptr) {
     if (!particles || particles->count == 0) {
         out.resize(0);
         return TMPM_OK;
@@ -598,15 +612,41 @@ inline TmpmStatus load_checked(const TmpmParticleArrays *particles, HostWorld &o
         err = "required particle arrays are missing";
         return TMPM_ERR_INVALID_INPUT;
     }
-    out.load(*particles);
+    // Copy, validate and (with `cfl_params`) take the CFL bound in one parallel
+    // pass; each particle is checked right after it is copied, while in cache.
+    out.resize(particles->count);
     std::atomic<bool> bad{false};
-    parallel_for(out.n, [&](size_t lo, size_t hi) {
-        for (size_t i = lo; i < hi && !bad.load(std::memory_order_relaxed); ++i)
-            if (!valid_particle(out, i)) bad = true;
+    const double max_substep = cfl_params ? cfl_params->max_substep : 0.0;
+    std::vector<double> part(host_threads() + 1, max_substep);
+    parallel_chunks(out.n, [&](size_t c, size_t lo, size_t hi) {
+        double dt = max_substep;
+        constexpr size_t kStep = 256;
+        for (size_t a = lo; a < hi && !bad.load(std::memory_order_relaxed); a += kStep) {
+            const size_t b = std::min(hi, a + kStep);
+            out.load_range(*particles, a, b);
+            for (size_t i = a; i < b; ++i) {
+                if (!valid_particle(out, i)) {
+                    bad = true;
+                    break;
+                }
+                if (cfl_params && out.enabled[i] && !out.fixed[i])
+                    dt = std::min(dt, timestep_bound(out.material[i], &out.mparams[5 * i], out.mass[i] / out.vol[i],
+                                                     &out.vel[3 * i], cfl_params->cell_width, det9(&out.F[9 * i])));
+            }
+        }
+        part[c] = dt;
     });
     if (bad) {
         err = "invalid MPM input";
         return TMPM_ERR_MPM_INVALID_INPUT;
+    }
+    if (cfl_params) {  // the same value stable_timestep() computes for this world and params
+        double dt = max_substep;
+        for (double d : part) dt = std::min(dt, d);
+        out.cfl_version = out.version;
+        out.cfl_h = cfl_params->cell_width;
+        out.cfl_max = cfl_params->max_substep;
+        out.cfl_value = std::min(dt, max_substep);
     }
     return TMPM_OK;
 }

@@ -176,6 +176,8 @@ void launch_bin_keys_values(const float *x, size_t stride, int n, float inv_h, u
 void launch_dump_grid(const GridTable &g, int32_t *cells, float4 *values, uint32_t *count, uint32_t capacity,
                       cudaStream_t stream);
 void launch_snapshot(const ParticleSoA &P, int n, const DevClass *classes, float4 *out, cudaStream_t stream);
+// 27 f32 rows (x, v, C, F, plastic) of the stored particles into world order, `stride` floats per row.
+void launch_unsort(const ParticleSoA &P, int n, float *out, size_t stride, cudaStream_t stream);
 int device_sm_count();
 
 // Thread-local reason reported by tmpm_last_error() (tmpm_session.cu).

@@ -878,6 +878,25 @@ __global__ void k_gather(ParticleSoA src, ParticleSoA dst, const uint32_t *__res
     dst.widx[j] = src.widx[s];
 }
 
+// Device rows back in world order: out[c * stride + widx[j]] = row c of stored
+// particle j, for the 27 f32 components (x, v, C, F, plastic), so the host
+// applies a readback sequentially instead of scattering through the sort
+// permutation.
+__global__ void k_unsort(ParticleSoA P, int n, float *__restrict__ out, size_t stride) {
+    int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    const size_t cap = P.cap, w = P.widx[j];
+    for (int c = 0; c < 3; ++c) {
+        out[c * stride + w] = P.x[c * cap + j];
+        out[(3 + c) * stride + w] = P.v[c * cap + j];
+        out[(24 + c) * stride + w] = P.pl[c * cap + j];
+    }
+    for (int c = 0; c < 9; ++c) {
+        out[(6 + c) * stride + w] = P.C[c * cap + j];
+        out[(15 + c) * stride + w] = P.F[c * cap + j];
+    }
+}
+
 __global__ void k_dump_grid(GridTable g, int32_t *cells, float4 *values, uint32_t *count, uint32_t capacity) {
     uint32_t nblocks = min(*g.count, g.max_blocks);
     size_t nodes = static_cast<size_t>(nblocks) * kNodesPerBlock;
@@ -983,6 +1002,11 @@ void launch_resort(ParticleSoA &src, ParticleSoA &dst, int n, int keep, const De
 void launch_dump_grid(const GridTable &g, int32_t *cells, float4 *values, uint32_t *count, uint32_t capacity,
                       cudaStream_t stream) {
     k_dump_grid<<<device_sm_count() * 4, 256, 0, stream>>>(g, cells, values, count, capacity);
+}
+
+void launch_unsort(const ParticleSoA &P, int n, float *out, size_t stride, cudaStream_t stream) {
+    if (n <= 0) return;
+    k_unsort<<<(n + 255) / 256, 256, 0, stream>>>(P, n, out, stride);
 }
 
 void launch_snapshot(const ParticleSoA &P, int n, const DevClass *classes, float4 *out, cudaStream_t stream) {

@@ -62,6 +62,7 @@ struct TmpmSession {
     DevBuf<int> cta_cache;  // kCacheStride ints per transfer CTA
     DevBuf<uint32_t> sort_keys[2], sort_vals[2], sort_hist, sort_totals;
     PinnedBuf staging;         // readback
+    DevBuf<float> unsorted;    // readback rows in world order
     PinnedBuf upload_staging;  // packed f32 state for uploads
     bool force_dirty = false;
     bool has_plastic = false;  // class table holds a snow, sand or NH sand class
@@ -428,31 +429,21 @@ struct TmpmSession {
         }
         const int n = n_dev;
         if (n > 0) {
-            const size_t pc = pbuf[cur].cap;
-            size_t floats = 27 * static_cast<size_t>(n);
-            if (!staging.ensure(floats * sizeof(float) + sizeof(uint32_t) * n))
-                return fail(TMPM_ERR_DEVICE, "cudaMallocHost staging failed");
+            // rows back in world order on the device, one copy, then sequential host passes
+            const size_t N = world.n, floats = 27 * N;
+            if (unsorted.count < floats && (e = unsorted.alloc(floats))) return cuda_fail(e, "cudaMalloc readback");
+            if (!staging.ensure(floats * sizeof(float))) return fail(TMPM_ERR_DEVICE, "cudaMallocHost staging failed");
             float *h = static_cast<float *>(staging.ptr);
-            const ParticleBuffers &pb = pbuf[cur];
-            for (int k = 0; k < 3; ++k) {
-                cudaMemcpyAsync(h + (0 + k) * n, pb.x.ptr + k * pc, sizeof(float) * n, cudaMemcpyDeviceToHost, stream);
-                cudaMemcpyAsync(h + (3 + k) * n, pb.v.ptr + k * pc, sizeof(float) * n, cudaMemcpyDeviceToHost, stream);
-            }
-            for (int k = 0; k < 9; ++k) {
-                cudaMemcpyAsync(h + (6 + k) * n, pb.C.ptr + k * pc, sizeof(float) * n, cudaMemcpyDeviceToHost, stream);
-                cudaMemcpyAsync(h + (15 + k) * n, pb.F.ptr + k * pc, sizeof(float) * n, cudaMemcpyDeviceToHost, stream);
-            }
-            for (int k = 0; k < 3; ++k)
-                cudaMemcpyAsync(h + (24 + k) * n, pb.pl.ptr + k * pc, sizeof(float) * n, cudaMemcpyDeviceToHost, stream);
-            uint32_t *widx = reinterpret_cast<uint32_t *>(h + floats);
-            cudaMemcpyAsync(widx, pb.widx.ptr, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost, stream);
-            if ((e = cudaStreamSynchronize(stream))) return cuda_fail(e, "readback");
+            launch_unsort(soa(), n, unsorted.ptr, N, stream);
+            if ((e = cudaMemcpyAsync(h, unsorted.ptr, sizeof(float) * floats, cudaMemcpyDeviceToHost, stream)) ||
+                (e = cudaStreamSynchronize(stream)))
+                return cuda_fail(e, "readback");
             // collect_prepared: non-finite transfers are an error before anything is applied
             std::atomic<bool> bad{false};
-            parallel_for(static_cast<size_t>(n), [&](size_t a, size_t b) {
+            parallel_for(N, [&](size_t a, size_t b) {
                 for (size_t c = 0; c < 27 && !bad.load(std::memory_order_relaxed); ++c)
-                    for (size_t j = a; j < b; ++j)
-                        if (!std::isfinite(h[c * n + j])) {
+                    for (size_t w = a; w < b; ++w)
+                        if (world.enabled[w] && !std::isfinite(h[c * N + w])) {
                             bad = true;
                             break;
                         }
@@ -461,25 +452,26 @@ struct TmpmSession {
                 valid = false;
                 return fail(TMPM_ERR_NON_FINITE_STATE, "MPM integration produced a non-finite state");
             }
-            parallel_for(static_cast<size_t>(n), [&](size_t a, size_t b) {
-                for (size_t j = a; j < b; ++j) {
-                    size_t w = widx[j];
+            ++world.version;
+            parallel_for(N, [&](size_t a, size_t b) {
+                for (size_t w = a; w < b; ++w) {
+                    if (!world.enabled[w]) continue;
                     if (world.fixed[w]) {
                         for (int k = 0; k < 3; ++k) world.vel[3 * w + k] = 0.0;
                         for (int k = 0; k < 9; ++k) world.C[9 * w + k] = 0.0;
                         continue;
                     }
                     for (int k = 0; k < 3; ++k) {
-                        world.pos[3 * w + k] = h[(0 + k) * n + j];
-                        world.vel[3 * w + k] = h[(3 + k) * n + j];
+                        world.pos[3 * w + k] = h[(0 + k) * N + w];
+                        world.vel[3 * w + k] = h[(3 + k) * N + w];
                     }
                     for (int k = 0; k < 9; ++k) {
-                        world.C[9 * w + k] = h[(6 + k) * n + j];
-                        world.F[9 * w + k] = h[(15 + k) * n + j];
+                        world.C[9 * w + k] = h[(6 + k) * N + w];
+                        world.F[9 * w + k] = h[(15 + k) * N + w];
                     }
                     const int mat = world.material[w];
                     if (mat == TMPM_MAT_SAND || mat == TMPM_MAT_SNOW || mat == TMPM_MAT_SAND_NEO_HOOKEAN)
-                        for (int k = 0; k < 3; ++k) world.plastic[3 * w + k] = h[(24 + k) * n + j];
+                        for (int k = 0; k < 3; ++k) world.plastic[3 * w + k] = h[(24 + k) * N + w];
                 }
             });
         }
@@ -543,7 +535,7 @@ TmpmStatus tmpm_session_create(const TmpmParams *params, const TmpmParticleArray
         g_last_error = "invalid MPM input";
         return TMPM_ERR_MPM_INVALID_INPUT;
     }
-    TmpmStatus st = load_checked(particles, s->world, err);
+    TmpmStatus st = load_checked(particles, s->world, err, params);
     if (st != TMPM_OK) {
         g_last_error = err;
         return st;
@@ -734,7 +726,7 @@ TmpmStatus tmpm_write_particles(TmpmSession *s, const TmpmParticleArrays *partic
     // and swap it in; the previous world comes back on any failure.
     HostWorld &nw = s->spare;
     std::string err;
-    st = load_checked(particles, nw, err);
+    st = load_checked(particles, nw, err, &s->params);
     if (st != TMPM_OK) return s->fail(st, err);
     if (!particles || !particles->chunk_id) {
         for (size_t i = 0; i < nw.n && i < s->world.n; ++i) nw.chunk[i] = s->world.chunk[i];
