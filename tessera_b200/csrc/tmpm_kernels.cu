@@ -254,6 +254,7 @@ __global__ void __launch_bounds__(kThreads, TMPM_TRANSFER_MIN_BLOCKS)
     __shared__ int s_used[kMaxTileBlocks];
     __shared__ int s_red[kThreads / 32][8];
     __shared__ Box s_box;
+    __shared__ Box s_gbox;  // the G2P box, whose block ids the P2G reuses (shared: not held in registers)
     __shared__ int s_abort;
 
     const size_t cap = P.cap;
@@ -304,8 +305,7 @@ __global__ void __launch_bounds__(kThreads, TMPM_TRANSFER_MIN_BLOCKS)
     }
     V3f v = mk(0, 0, 0);
     M3f Cm = m3_zero();
-    Box gbox;
-    gbox.ok = 0;
+    if (threadIdx.x == 0) s_gbox.ok = 0;
 
     if (MODE == kModeP2G) {
         if (p2g_on) {
@@ -553,7 +553,7 @@ __global__ void __launch_bounds__(kThreads, TMPM_TRANSFER_MIN_BLOCKS)
             }
         }
         if (MODE == kModeG2P) return;
-        gbox = bx;
+        if (threadIdx.x == 0) s_gbox = bx;
     }
 
     // ----------------------------------------------------------------- P2G
@@ -669,10 +669,10 @@ __global__ void __launch_bounds__(kThreads, TMPM_TRANSFER_MIN_BLOCKS)
                 split_b(t, tx, ty, tz);
                 int gx = bx.blo[0] + tx, gy = bx.blo[1] + ty, gz = bx.blo[2] + tz;
                 // reuse the id the G2P box already holds for this block (same table)
-                if (gbox.ok && gbox.color == bx.color) {
-                    int rx = gx - gbox.blo[0], ry = gy - gbox.blo[1], rz = gz - gbox.blo[2];
-                    if (rx >= 0 && ry >= 0 && rz >= 0 && rx < gbox.nb[0] && ry < gbox.nb[1] && rz < gbox.nb[2])
-                        id = s_blk[(rx * gbox.nb[1] + ry) * gbox.nb[2] + rz];
+                if (s_gbox.ok && s_gbox.color == bx.color) {
+                    int rx = gx - s_gbox.blo[0], ry = gy - s_gbox.blo[1], rz = gz - s_gbox.blo[2];
+                    if (rx >= 0 && ry >= 0 && rz >= 0 && rx < s_gbox.nb[0] && ry < s_gbox.nb[1] && rz < s_gbox.nb[2])
+                        id = s_blk[(rx * s_gbox.nb[1] + ry) * s_gbox.nb[2] + rz];
                 }
                 if (id < 0)
                     id = find_or_insert_block(next, block_key(gx, gy, gz, bx.color),
