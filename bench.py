@@ -195,6 +195,17 @@ def cpu_baseline(scene_fn, target_seconds=15.0):
                       f"materials) x {substeps} substeps, {threads} independent copies in parallel, {el:.1f} s"}
 
 
+def shape_summary(info: dict) -> dict:
+    """The tuned transfer launch shape and what each candidate measured."""
+    k = info["shape"]
+    out = {"tuned": k is not None}
+    if k is not None:
+        out["particles_per_cta"], out["ctas_per_sm"] = info["shapes"][k]
+    out["ns_per_particle_substep"] = {f"{t}x{b}": (None if c is None else c * 1e6)
+                                      for (t, b), c in zip(info["shapes"], info["ms_per_particle_substep"])}
+    return out
+
+
 def bench_batched(count: int) -> dict:
     """256 heterogeneous scenes x 100 substeps: one multi-scene batch against one
     session per scene, on the same device."""
@@ -224,6 +235,12 @@ def bench_batched(count: int) -> dict:
     outs = [b.read(i) for i in ids]
     e2e_batched = time.perf_counter() - t0
     assert all(np.all(np.isfinite(o["position"])) for o in outs)
+    # the launch-shape tuner reads its trials (the first six batches) before the timed batches
+    for _ in range(8):
+        if b.launch_shape()["shape"] is not None:
+            break
+        b.run({i: steps for i in ids})
+    shape_info = b.launch_shape()
     # batched, device-resident: further batches of the same scenes (graph replays)
     dev = []
     for _ in range(3):
@@ -231,11 +248,12 @@ def bench_batched(count: int) -> dict:
         dev.append(b.last_ms())
     fails = sum(b.status(i) != 0 for i in ids)
     b.close()
-    # plain: one scene at a time through a single-scene session each
+    # plain: one scene at a time through a single-scene session each, at the
+    # default launch shape (a 100-substep session ends before its tuner would)
     plain_dev = 0.0
     t0 = time.perf_counter()
     for s in scs:
-        ses = Session(s.params, s.particles, s.dt)
+        ses = Session(s.params, s.particles, s.dt, launch_shape=0)
         left = steps
         while left:
             k = min(BATCH, left)
@@ -252,7 +270,8 @@ def bench_batched(count: int) -> dict:
         "materials": {"elastic": sum(s.info["material"] == "elastic" for s in scs),
                       "fluid": sum(s.info["material"] == "fluid" for s in scs)},
         "batched": {"value": work / (batched_dev / 1e3), "ms_per_batch": batched_dev, "failed_scenes": fails,
-                    "e2e": work / e2e_batched, "e2e_seconds": e2e_batched, "graph_replay": True},
+                    "e2e": work / e2e_batched, "e2e_seconds": e2e_batched, "graph_replay": True,
+                    "launch_shape": shape_summary(shape_info)},
         "plain": {"value": work / (plain_dev / 1e3), "device_ms": plain_dev, "e2e": work / e2e_plain,
                   "e2e_seconds": e2e_plain},
         "speedup_device": plain_dev / batched_dev, "speedup_e2e": e2e_plain / e2e_batched, "unit": METRIC,
@@ -360,6 +379,14 @@ def run_tessera(args, world, rank, local):
     _, mm = session.debug_p2g()
     grid_nodes = int(mm.shape[0])
 
+    # the launch-shape tuner's trials (two 64-substep segments per shape) come
+    # before the warm-up, so every timed segment runs the chosen shape
+    for _ in range(8):
+        if session.launch_shape()["shape"] is not None:
+            break
+        session.bench_substeps(BATCH)
+        session.synchronize()
+    shape_info = session.launch_shape()
     for _ in range(args.warmup):
         session.bench_substeps(BATCH)
     session.synchronize()
@@ -442,6 +469,7 @@ def run_tessera(args, world, rank, local):
             "config": {"workload": "config2-dam-break", "particles_per_gpu": n, "grid": "256^3 virtual, 4^3 blocks",
                        "active_grid_nodes": grid_nodes, "dt": sc.dt, "substeps_per_step": BATCH,
                        "l2": "inputs larger than L2 (particle state ~0.4 GB per GPU)",
+                       "launch_shape": shape_summary(shape_info),
                        "parallelism": f"replicas x{world}"},
             "gpu_launches": (2 * BATCH + 2 + RESORT_LAUNCHES) * args.steps,
             "roofline": roofline,

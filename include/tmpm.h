@@ -136,7 +136,8 @@ typedef struct TmpmSessionOptions {
     int32_t device;          /* CUDA device ordinal; default 0 */
     uint32_t max_blocks;     /* block pool capacity per grid; 0 = sized from the scene */
     uint32_t resort_interval;/* substeps between particle re-sorts; 0 = once per submit */
-    uint32_t reserved;
+    uint32_t launch_shape;   /* transfer-kernel launch shape: 0 = tuned on the first submits,
+                                k > 0 = shape k - 1 of tmpm_launch_shape_info */
     uint64_t next_chunk_id;  /* MpmWorld's next chunk id (world.rs:220); 0 = max(chunk_id) + 1 */
     uint64_t substeps;       /* MpmWorld::substeps of the uploaded world (world.rs:215) */
 } TmpmSessionOptions;
@@ -280,7 +281,7 @@ typedef struct TmpmBatchOptions {
     int32_t device;            /* CUDA device ordinal */
     uint32_t max_blocks;       /* 0 = size the block pool from the scenes' occupied blocks */
     uint32_t use_graphs;       /* 1 = replay each batch as a CUDA graph (captured once per shape) */
-    uint32_t reserved;
+    uint32_t launch_shape;     /* as TmpmSessionOptions::launch_shape */
     uint64_t particle_capacity; /* initial device rows (0 = grow on demand) */
 } TmpmBatchOptions;
 
@@ -413,6 +414,26 @@ TmpmStatus tmpm_debug_p2g(TmpmSession *session, int32_t *cells_out, float *mass_
  * g2p2g, g2p, resort when kernel_ms is non-NULL. */
 TmpmStatus tmpm_bench_substeps(TmpmSession *session, uint32_t steps, double *ms,
                                double *kernel_ms, size_t kernel_count);
+
+/* ---------------- launch-shape tuning (no reference counterpart) ----------------
+ * The transfer kernels (G2P, P2G and the fused G2P2G) are built for several
+ * launch shapes: particles per CTA and CTAs resident per SM.  Unless the
+ * options fix one, a session or batch runs its first submitted segments under
+ * each shape in turn (two rounds, real work; results differ between shapes
+ * only by f32 summation order) and keeps the one with the least device time per
+ * particle-substep, as CUDA events on its stream measured it.  Plastic
+ * materials and CPIC run shape 0 only. */
+
+/* Shape `shape` (0 ..< count): particles per CTA and CTAs per SM. */
+uint32_t tmpm_launch_shape_count(void);
+TmpmStatus tmpm_launch_shape_info(uint32_t shape, uint32_t *threads_per_cta, uint32_t *ctas_per_sm);
+
+/* The shape in use: -1 while trials are outstanding, else its index.  When
+ * `ms_per_unit` is non-NULL, it receives (up to `count` entries) the best
+ * measured milliseconds per particle-substep of each shape (infinity where no
+ * trial has been read). */
+int32_t tmpm_session_launch_shape(TmpmSession *session, double *ms_per_unit, size_t count);
+int32_t tmpm_batch_launch_shape(TmpmBatch *batch, double *ms_per_unit, size_t count);
 
 #ifdef __cplusplus
 }

@@ -124,7 +124,7 @@ class TmpmSessionOptions(C.Structure):
         ("device", C.c_int32),
         ("max_blocks", C.c_uint32),
         ("resort_interval", C.c_uint32),
-        ("reserved", C.c_uint32),
+        ("launch_shape", C.c_uint32),
         ("next_chunk_id", C.c_uint64),
         ("substeps", C.c_uint64),
     ]
@@ -135,7 +135,7 @@ class TmpmBatchOptions(C.Structure):
         ("device", C.c_int32),
         ("max_blocks", C.c_uint32),
         ("use_graphs", C.c_uint32),
-        ("reserved", C.c_uint32),
+        ("launch_shape", C.c_uint32),
         ("particle_capacity", C.c_uint64),
     ]
 

@@ -143,9 +143,41 @@ def lib():
     L.tmpm_adjoint_last_error_message.restype = C.c_char_p
     L.tmpm_batch_last_error_message.argtypes = [P]
     L.tmpm_batch_last_error_message.restype = C.c_char_p
+    L.tmpm_launch_shape_count.argtypes = []
+    L.tmpm_launch_shape_count.restype = U32
+    L.tmpm_launch_shape_info.argtypes = [U32, C.POINTER(U32), C.POINTER(U32)]
+    L.tmpm_launch_shape_info.restype = S
+    L.tmpm_session_launch_shape.argtypes = [P, P, C.c_size_t]
+    L.tmpm_session_launch_shape.restype = C.c_int32
+    L.tmpm_batch_launch_shape.argtypes = [P, P, C.c_size_t]
+    L.tmpm_batch_launch_shape.restype = C.c_int32
     _lib = L
     return L
 
 
 def version() -> str:
     return lib().tmpm_version().decode()
+
+
+def launch_shapes() -> list[tuple[int, int]]:
+    """(particles per CTA, CTAs per SM) of each transfer launch shape, by index."""
+    L = lib()
+    out = []
+    for k in range(int(L.tmpm_launch_shape_count())):
+        t, b = C.c_uint32(0), C.c_uint32(0)
+        if L.tmpm_launch_shape_info(k, C.byref(t), C.byref(b)) != 0:
+            raise RuntimeError(f"launch shape {k}: {L.tmpm_last_error().decode()}")
+        out.append((int(t.value), int(b.value)))
+    return out
+
+
+def query_launch_shape(fn, handle) -> dict:
+    """The shape in use (None while tuning) and the measured ms per
+    particle-substep of each shape (None where not measured)."""
+    import numpy as np
+
+    n = int(lib().tmpm_launch_shape_count())
+    costs = np.full(n, np.inf)
+    shape = int(fn(handle, costs.ctypes.data, n))
+    return {"shape": None if shape < 0 else shape, "shapes": launch_shapes(),
+            "ms_per_particle_substep": [None if not np.isfinite(c) else float(c) for c in costs]}

@@ -77,13 +77,16 @@ class PreparedScene:
 class Batch:
     """Resident multi-scene batch on one device."""
 
-    def __init__(self, device: int = 0, max_blocks: int = 0, use_graphs: bool = True, particle_capacity: int = 0):
+    def __init__(self, device: int = 0, max_blocks: int = 0, use_graphs: bool = True, particle_capacity: int = 0,
+                 launch_shape: int | None = None):
         L = _native.lib()
         opts = TmpmBatchOptions()
         opts.device = device
         opts.max_blocks = max_blocks
         opts.use_graphs = 1 if use_graphs else 0
         opts.particle_capacity = particle_capacity
+        # None: tuned on the first batches; k: launch shape k (see _native.launch_shapes())
+        opts.launch_shape = 0 if launch_shape is None else int(launch_shape) + 1
         handle = C.c_void_p()
         self._h = None
         _check(L.tmpm_batch_create(C.byref(opts), C.byref(handle)))
@@ -164,6 +167,11 @@ class Batch:
 
     def last_ms(self) -> float:
         return float(_native.lib().tmpm_batch_last_ms(self._h))
+
+    def launch_shape(self) -> dict:
+        """Transfer launch shape in use (None while trials are outstanding) and
+        the measured cost of each shape."""
+        return _native.query_launch_shape(_native.lib().tmpm_batch_launch_shape, self._h)
 
     def device_bytes(self) -> int:
         return int(_native.lib().tmpm_batch_device_bytes(self._h))

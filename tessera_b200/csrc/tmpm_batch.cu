@@ -171,14 +171,17 @@ struct TmpmBatch {
     uint64_t epoch = 1;  // bumps whenever a device pointer a graph holds changes
     bool pending = false;
     double last_ms = 0.0;
+    LaunchTuner tuner;  // transfer launch shape (tuned on the first batches unless fixed)
 
     struct GraphKey {
         uint32_t steps;
         size_t n_phys, n_live;
         int cur;
         uint64_t epoch;
+        int shape;
         bool operator<(const GraphKey &o) const {
-            return std::tie(steps, n_phys, n_live, cur, epoch) < std::tie(o.steps, o.n_phys, o.n_live, o.cur, o.epoch);
+            return std::tie(steps, n_phys, n_live, cur, epoch, shape) <
+                   std::tie(o.steps, o.n_phys, o.n_live, o.cur, o.epoch, o.shape);
         }
     };
     std::map<GraphKey, cudaGraphExec_t> graphs;
@@ -278,7 +281,7 @@ struct TmpmBatch {
             ++epoch;
         }
         const size_t cap = pbuf[cur].cap;
-        const size_t ctas = (cap + kTransferThreads - 1) / kTransferThreads;
+        const size_t ctas = (cap + kMinTransferThreads - 1) / kMinTransferThreads;
         if (cta_cache.count < ctas * kCacheStride) {
             if ((e = cta_cache.alloc(ctas * kCacheStride))) return cuda_fail(e, "cudaMalloc cache");
             ++epoch;
@@ -398,8 +401,9 @@ struct TmpmBatch {
     }
 
     // The kernels of one batch of `steps` substeps (captured into a graph or launched directly).
-    void launch_batch(uint32_t steps) {
+    void launch_batch(uint32_t steps, int shape) {
         SimParams sp = sim_params();
+        sp.shape = shape;
         ParticleSoA src = pbuf[cur].view(nullptr, 1), dst = pbuf[cur ^ 1].view(nullptr, 1);
         SortBuffers sb = sort_buffers();
         launch_resort(src, dst, static_cast<int>(n_phys), static_cast<int>(n_live), dclasses.ptr, sp, sb, stream);
@@ -433,15 +437,19 @@ struct TmpmBatch {
             if (s.live) s.prev_offset = s.dev_offset;
         prev_buf = cur;
         if (n_phys > 0) {
+            // Plastic classes run the default shape only.
+            const bool tunable = !classes.plastic();
+            const int shape = tunable ? tuner.shape() : 0;
+            const double work = static_cast<double>(n_live) * steps;
             if (options.use_graphs) {
-                GraphKey key{steps, n_phys, n_live, cur, epoch};
+                GraphKey key{steps, n_phys, n_live, cur, epoch, shape};
                 auto it = graphs.find(key);
                 if (it == graphs.end()) {
                     if (graphs.size() > 16) drop_graphs();
                     cudaGraph_t graph = nullptr;
                     if ((e = cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal)))
                         return cuda_fail(e, "cudaStreamBeginCapture");
-                    launch_batch(steps);
+                    launch_batch(steps, shape);
                     if ((e = cudaStreamEndCapture(stream, &graph))) return cuda_fail(e, "cudaStreamEndCapture");
                     cudaGraphExec_t exec = nullptr;
                     e = cudaGraphInstantiate(&exec, graph, 0);
@@ -449,10 +457,13 @@ struct TmpmBatch {
                     if (e) return cuda_fail(e, "cudaGraphInstantiate");
                     it = graphs.emplace(key, exec).first;
                 }
+                if (tunable) tuner.begin(shape, stream);
                 if ((e = cudaGraphLaunch(it->second, stream))) return cuda_fail(e, "cudaGraphLaunch");
             } else {
-                launch_batch(steps);
+                if (tunable) tuner.begin(shape, stream);
+                launch_batch(steps, shape);
             }
+            if (tunable) tuner.end(work, stream);
             cur ^= 1;
         }
         assign_offsets();
@@ -748,6 +759,7 @@ TmpmStatus tmpm_batch_create(const TmpmBatchOptions *options, TmpmBatch **out) {
     if (options) b->options = *options;
     else b->options.use_graphs = 1;
     b->device = b->options.device;
+    b->tuner.reset(b->options.launch_shape);
     cudaError_t e;
     if ((e = cudaSetDevice(b->device)) || (e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking)) ||
         (e = cudaStreamCreateWithFlags(&b->read_stream, cudaStreamNonBlocking)) ||
@@ -878,6 +890,17 @@ TmpmStatus tmpm_batch_read_scene(TmpmBatch *b, uint32_t scene, TmpmParticleArray
 }
 
 double tmpm_batch_last_ms(const TmpmBatch *b) { return b ? b->last_ms : 0.0; }
+
+int32_t tmpm_batch_launch_shape(TmpmBatch *b, double *ms_per_unit, size_t count) {
+    if (!b) return -1;
+    if (b->tuner.tuning()) {
+        cudaSetDevice(b->device);
+        b->tuner.poll();
+    }
+    if (ms_per_unit) b->tuner.costs(ms_per_unit, static_cast<uint32_t>(count));
+    if (b->classes.plastic()) return 0;  // variants built for the default shape only
+    return b->tuner.chosen;
+}
 
 size_t tmpm_batch_device_bytes(const TmpmBatch *b) { return b ? b->device_bytes() : 0; }
 

@@ -554,6 +554,106 @@ struct GridBuffers {
     }
 };
 
+// Launch-shape tuner of the transfer kernels.  The first submitted segments
+// (real work, not a rehearsal) run under each candidate shape in turn, `kRounds`
+// times each, timed with CUDA events on the submitting stream; the shape with
+// the least time per particle-substep (best of its rounds, so the first launch
+// of a kernel, which loads its module, does not count against it) is kept once
+// every trial has completed.  Nothing waits for a trial: completed events are
+// read when the next segment asks for its shape.
+struct LaunchTuner {
+    static constexpr int kRounds = 2;
+    static constexpr int kTrials = kRounds * kNumLaunchShapes;
+    int fixed = -1;   // >= 0: the caller's shape; no tuning
+    int chosen = -1;  // the tuned shape, -1 while trials are outstanding
+    int issued = 0;   // trials started
+    int read = 0;     // trials whose time has been read
+    double best[kNumLaunchShapes];
+    struct Trial {
+        int shape = 0;
+        double work = 0.0;
+        cudaEvent_t a = nullptr, b = nullptr;
+    };
+    std::vector<Trial> trials;
+    int open = -1;  // index of the trial being recorded
+
+    LaunchTuner() { reset(0); }
+    ~LaunchTuner() { release(); }
+    LaunchTuner(const LaunchTuner &) = delete;
+    LaunchTuner &operator=(const LaunchTuner &) = delete;
+
+    void release() {
+        for (Trial &t : trials) {
+            if (t.a) cudaEventDestroy(t.a);
+            if (t.b) cudaEventDestroy(t.b);
+        }
+        trials.clear();
+        open = -1;
+    }
+    // `option`: 0 = tune, k > 0 = fixed shape k - 1 (out of range: shape 0).
+    void reset(uint32_t option) {
+        release();
+        fixed = option == 0 ? -1 : (option <= static_cast<uint32_t>(kNumLaunchShapes) ? static_cast<int>(option) - 1 : 0);
+        chosen = fixed;
+        issued = read = 0;
+        for (double &b : best) b = std::numeric_limits<double>::infinity();
+    }
+    bool tuning() const { return chosen < 0; }
+    void poll() {
+        while (read < static_cast<int>(trials.size()) && read != open) {
+            Trial &t = trials[read];
+            if (cudaEventQuery(t.b) != cudaSuccess) {
+                cudaGetLastError();  // cudaErrorNotReady is not an error of the stream
+                return;
+            }
+            float ms = 0.f;
+            if (cudaEventElapsedTime(&ms, t.a, t.b) == cudaSuccess && t.work > 0)
+                best[t.shape] = std::min(best[t.shape], ms / t.work);
+            ++read;
+        }
+        if (chosen < 0 && issued == kTrials && read == issued) {
+            int s = 0;
+            for (int k = 1; k < kNumLaunchShapes; ++k)
+                if (best[k] < best[s]) s = k;
+            chosen = s;
+            release();
+        }
+    }
+    // Shape for the next segment.
+    int shape() {
+        if (chosen >= 0) return chosen;
+        poll();
+        if (chosen >= 0) return chosen;
+        return issued < kTrials ? issued % kNumLaunchShapes : 0;
+    }
+    // Brackets one segment of `work` particle-substeps run under shape(); only
+    // trials are recorded.
+    void begin(int shape_used, cudaStream_t stream) {
+        if (chosen >= 0 || issued >= kTrials || shape_used != issued % kNumLaunchShapes) return;
+        Trial t;
+        t.shape = shape_used;
+        if (cudaEventCreate(&t.a) || cudaEventCreate(&t.b) || cudaEventRecord(t.a, stream)) {
+            if (t.a) cudaEventDestroy(t.a);
+            if (t.b) cudaEventDestroy(t.b);
+            cudaGetLastError();
+            return;
+        }
+        trials.push_back(t);
+        open = static_cast<int>(trials.size()) - 1;
+        ++issued;
+    }
+    void end(double work, cudaStream_t stream) {
+        if (open < 0) return;
+        trials[open].work = work;
+        cudaEventRecord(trials[open].b, stream);
+        open = -1;
+    }
+    // Measured ms per particle-substep of each shape (infinity: not measured).
+    void costs(double *out, uint32_t count) const {
+        for (uint32_t k = 0; k < count && k < static_cast<uint32_t>(kNumLaunchShapes); ++k) out[k] = best[k];
+    }
+};
+
 // Device material codes, as the reference packs them (gpu.rs:1171-1276).
 inline int class_kind(int material) {
     switch (material) {

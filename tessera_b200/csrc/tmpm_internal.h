@@ -43,10 +43,18 @@ constexpr int kMatSnow = 4;
 constexpr int kMatSand = 5;
 constexpr int kMatSandNeoHookean = 6;
 
-#ifndef TMPM_TRANSFER_THREADS
-#define TMPM_TRANSFER_THREADS 256
+#ifndef TMPM_TRANSFER_MIN_BLOCKS
+#define TMPM_TRANSFER_MIN_BLOCKS 4  // CTAs per SM of the default transfer launch shape (measured best of 2-6)
 #endif
-constexpr int kTransferThreads = TMPM_TRANSFER_THREADS;  // particles per CTA of the transfer kernels
+// Launch shapes of the transfer kernels the tuner chooses among (particles per
+// CTA, CTAs per SM the kernel is compiled for); shape 0 is the default and the
+// only one for plastic and CPIC variants.
+struct LaunchShape {
+    int threads, min_blocks;
+};
+constexpr LaunchShape kLaunchShapes[] = {{256, TMPM_TRANSFER_MIN_BLOCKS}, {128, 8}, {256, 3}};
+constexpr int kNumLaunchShapes = 3;
+constexpr int kMinTransferThreads = 128;  // per-CTA records are sized for the smallest shape
 constexpr int kCacheStride = 144;      // per-CTA record: 16-int box header + up to 128 block ids
 
 constexpr uint32_t kFixedBit = 0x80000000u;
@@ -111,7 +119,6 @@ constexpr int kSortBitsScene = 27;            // single scene: 21-bit block Mort
 #define TMPM_RESORT_SUBSTEPS 64
 #endif
 constexpr uint32_t kResortSubsteps = TMPM_RESORT_SUBSTEPS;  // default substeps between re-sorts of a session
-constexpr int kInterleave = kTransferThreads / 32;  // particles per lane group in the storage interleave (k_gather)
 constexpr int kSortBitsBatch = 30;            // batch: scene << 21 | Morton, plus the removed-scene bit
 constexpr uint32_t kDeadKey = 0x3FFFFFFFu;
 
@@ -127,6 +134,7 @@ struct SimParams {
     int resident_checks;  // CFL / escape / conditioning flags (resident path only, gpu.rs:1429)
     int has_plastic;      // some particle class is snow, sand or NH sand
     int cpic;             // CPIC on: grid namespace = colour << 8 | side mask of the CPIC groups (< 8)
+    int shape;            // transfer launch shape (index into kLaunchShapes)
 };
 constexpr int kMaxCpicGroups = 8;
 

@@ -19,17 +19,16 @@
 
 #include "tmpm_device.cuh"
 
-#ifndef TMPM_TRANSFER_MIN_BLOCKS
-#define TMPM_TRANSFER_MIN_BLOCKS 4  // CTAs per SM the transfer kernels are compiled for (measured best of 2-6)
-#endif
 
 namespace tmpm {
 
 namespace {
 
-constexpr int kThreads = kTransferThreads;
 constexpr int kTileMaxDim = 16;     // box edge in cells
-constexpr int kTileMaxNodes = 2048; // box nodes: one 32 KB shared buffer, gather tile then scatter tile
+// Box nodes a CTA of `threads` particles stages: 8 per particle (2048 nodes,
+// one 32 KB shared buffer, for 256), used as the gather tile and then as the
+// scatter tile.
+constexpr int tile_nodes(int threads) { return threads * 8; }
 constexpr int kMaxTileBlocks = kCacheStride - 16;
 constexpr int kCacheHeader = 16;
 constexpr uint32_t kFatal = kStatusCapacity | kStatusTimeout | kStatusResident;
@@ -64,6 +63,7 @@ struct Split3 {
 };
 
 // Block-wide min/max of base cells and colours; thread 0 fills `box`.
+template <int THREADS>
 __device__ __forceinline__ void reduce_box(bool valid, const int b[3], uint32_t color, int (*red)[8], Box &box) {
     int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     int vals[8];
@@ -84,7 +84,7 @@ __device__ __forceinline__ void reduce_box(bool valid, const int b[3], uint32_t 
     if (threadIdx.x == 0) {
         int m[8];
         for (int a = 0; a < 8; ++a) m[a] = red[0][a];
-        for (int w = 1; w < kThreads / 32; ++w) {
+        for (int w = 1; w < THREADS / 32; ++w) {
             for (int a = 0; a < 3; ++a) m[a] = min(m[a], red[w][a]);
             for (int a = 3; a < 6; ++a) m[a] = max(m[a], red[w][a]);
             m[6] = min(m[6], red[w][6]);
@@ -106,7 +106,7 @@ __device__ __forceinline__ void reduce_box(bool valid, const int b[3], uint32_t 
                 nodes *= box.dim[a];
                 nbt *= box.nb[a];
             }
-            ok = nodes <= kTileMaxNodes && nbt <= kMaxTileBlocks;
+            ok = nodes <= tile_nodes(THREADS) && nbt <= kMaxTileBlocks;
         }
         box.nodes = nodes;
         box.nbt = nbt;
@@ -119,6 +119,7 @@ __device__ __forceinline__ void reduce_box(bool valid, const int b[3], uint32_t 
 // Box of base cells and colours plus two float sums over the CTA, with one
 // barrier: each warp reduces its lanes and publishes a partial, then every
 // warp combines the partials itself (no second barrier, no shared result).
+template <int THREADS>
 __device__ __forceinline__ void reduce_box_sums(bool valid, const int b[3], uint32_t color, float &sum_a, float &sum_b,
                                                 int (*red)[8], float (*redf)[2], Box &box) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -141,7 +142,7 @@ __device__ __forceinline__ void reduce_box_sums(bool valid, const int b[3], uint
         redf[warp][1] = fb;
     }
     __syncthreads();
-    constexpr int kWarps = kThreads / 32;
+    constexpr int kWarps = THREADS / 32;
     const bool mine = lane < kWarps;
     int m[8];
     for (int a = 0; a < 3; ++a) {
@@ -172,7 +173,7 @@ __device__ __forceinline__ void reduce_box_sums(bool valid, const int b[3], uint
             nodes *= box.dim[a];
             nbt *= box.nb[a];
         }
-        ok = nodes <= kTileMaxNodes && nbt <= kMaxTileBlocks;
+        ok = nodes <= tile_nodes(THREADS) && nbt <= kMaxTileBlocks;
     }
     box.nodes = nodes;
     box.nbt = nbt;
@@ -236,8 +237,8 @@ __device__ __forceinline__ float pow2_scale(float total) {
 // substeps its scene advances in this batch) or kCpic (one scene whose grid
 // namespace includes CPIC side masks).  Each costs registers only where used.
 enum Variant { kPlain = 0, kMulti = 1, kCpic = 2 };
-template <int MODE, bool PLASTIC, int VARIANT>
-__global__ void __launch_bounds__(kThreads, TMPM_TRANSFER_MIN_BLOCKS)
+template <int MODE, bool PLASTIC, int VARIANT, int THREADS, int MINB>
+__global__ void __launch_bounds__(THREADS, MINB)
     k_transfer(ParticleSoA P, int n, const DevClass *__restrict__ classes, GridTable cur, GridTable next,
                SimParams sp, const DevObstacle *__restrict__ obstacles, const float *__restrict__ planes,
                double *reactions, uint32_t *status, int *__restrict__ cache) {
@@ -245,27 +246,28 @@ __global__ void __launch_bounds__(kThreads, TMPM_TRANSFER_MIN_BLOCKS)
     constexpr bool CPIC = VARIANT == kCpic;
     // One buffer holds the G2P gather tile (float4 per node) and then the P2G
     // scatter tile (4 fixed-point ints per node, component-major).
-    __shared__ float4 s_tile[kTileMaxNodes];
+    constexpr int kTileNodes = tile_nodes(THREADS);
+    __shared__ float4 s_tile[kTileNodes];
     float4 *const s_gv = s_tile;
-    int (*const s_sc)[kTileMaxNodes] = reinterpret_cast<int (*)[kTileMaxNodes]>(s_tile);
-    __shared__ float s_fred[kThreads / 32][2];
+    int (*const s_sc)[kTileNodes] = reinterpret_cast<int (*)[kTileNodes]>(s_tile);
+    __shared__ float s_fred[THREADS / 32][2];
     __shared__ int s_blk[kMaxTileBlocks];
     __shared__ int s_blk2[kMaxTileBlocks];
     __shared__ int s_used[kMaxTileBlocks];
-    __shared__ int s_red[kThreads / 32][8];
+    __shared__ int s_red[THREADS / 32][8];
     __shared__ Box s_box;
     __shared__ Box s_gbox;  // the G2P box, whose block ids the P2G reuses (shared: not held in registers)
     __shared__ int s_abort;
 
     const size_t cap = P.cap;
-    const int i = blockIdx.x * kThreads + threadIdx.x;
+    const int i = blockIdx.x * THREADS + threadIdx.x;
     const bool valid = i < n;
     int *const cc = cache + static_cast<size_t>(blockIdx.x) * kCacheStride;
 
     if (threadIdx.x == 0) s_abort = (*reinterpret_cast<volatile uint32_t *>(status) & kFatal) != 0;
     if (MODE != kModeG2P) {
         // The first barrier of the kernel orders these.
-        for (int t = threadIdx.x; t < kMaxTileBlocks; t += kThreads) s_used[t] = 0;
+        for (int t = threadIdx.x; t < kMaxTileBlocks; t += THREADS) s_used[t] = 0;
     }
 
     V3f x = mk(0, 0, 0);
@@ -340,11 +342,11 @@ __global__ void __launch_bounds__(kThreads, TMPM_TRANSFER_MIN_BLOCKS)
                 bx.nbt = cc[15];
                 bx.ok = 1;
             } else {
-                reduce_box(g2p_on, b, ns, s_red, s_box);
+                reduce_box<THREADS>(g2p_on, b, ns, s_red, s_box);
                 bx = s_box;
                 if (bx.ok) {
                     const Split3 split(bx.nb[1], bx.nb[2]);
-                    for (int t = threadIdx.x; t < bx.nbt; t += kThreads) {
+                    for (int t = threadIdx.x; t < bx.nbt; t += THREADS) {
                         int tx, ty, tz;
                         split(t, tx, ty, tz);
                         s_blk[t] = lookup_block(cur, block_key(bx.blo[0] + tx, bx.blo[1] + ty, bx.blo[2] + tz, bx.color));
@@ -357,7 +359,7 @@ __global__ void __launch_bounds__(kThreads, TMPM_TRANSFER_MIN_BLOCKS)
                         b[1] + 2 >= bx.lo[1] + bx.dim[1] || b[2] + 2 >= bx.lo[2] + bx.dim[2] || ns != bx.color);
             if (bx.ok && !bad) {
                 const Split3 split(bx.dim[1], bx.dim[2]);
-                for (int t = threadIdx.x; t < bx.nodes; t += kThreads) {
+                for (int t = threadIdx.x; t < bx.nodes; t += THREADS) {
                     int tx, ty, tz;
                     split(t, tx, ty, tz);
                     int cx = bx.lo[0] + tx, cy = bx.lo[1] + ty, cz = bx.lo[2] + tz;
@@ -592,11 +594,11 @@ __global__ void __launch_bounds__(kThreads, TMPM_TRANSFER_MIN_BLOCKS)
     if (MODE != kModeP2G && CPIC) ns = particle_namespace(k.color, 1, sp.num_obstacles, obstacles, x);
     float tot_m = bound_m, tot_p = bound_p;
     Box bx;
-    reduce_box_sums(active, b, ns, tot_m, tot_p, s_red, s_fred, bx);
+    reduce_box_sums<THREADS>(active, b, ns, tot_m, tot_p, s_red, s_fred, bx);
     if (MODE == kModeP2G && s_abort) return;
     if (bx.ok) {
         // every warp has finished its gather (barrier above): the buffer becomes the scatter tile
-        for (int t = threadIdx.x; t < bx.nodes; t += kThreads) {
+        for (int t = threadIdx.x; t < bx.nodes; t += THREADS) {
             s_sc[0][t] = 0;
             s_sc[1][t] = 0;
             s_sc[2][t] = 0;
@@ -662,7 +664,7 @@ __global__ void __launch_bounds__(kThreads, TMPM_TRANSFER_MIN_BLOCKS)
         }
         __syncthreads();
         const Split3 split_b(bx.nb[1], bx.nb[2]);
-        for (int t = threadIdx.x; t < bx.nbt; t += kThreads) {
+        for (int t = threadIdx.x; t < bx.nbt; t += THREADS) {
             int id = -1;
             if (s_used[t]) {
                 int tx, ty, tz;
@@ -702,7 +704,7 @@ __global__ void __launch_bounds__(kThreads, TMPM_TRANSFER_MIN_BLOCKS)
         __syncthreads();
         const float inv_sm = 1.0f / sm, inv_sp = 1.0f / spv;
         const Split3 split_n(bx.dim[1], bx.dim[2]);
-        for (int t = threadIdx.x; t < bx.nodes; t += kThreads) {
+        for (int t = threadIdx.x; t < bx.nodes; t += THREADS) {
             const int m = s_sc[0][t], px = s_sc[1][t], py = s_sc[2][t], pz = s_sc[3][t];
             if ((m | px | py | pz) == 0) continue;
             int tx, ty, tz;
@@ -846,10 +848,10 @@ __global__ void k_bin_keys(const float *x, size_t cap, int n, float inv_h, const
     if (vals) vals[i] = static_cast<uint32_t>(i);
 }
 
-// dst[j] = src[perm[s(j)]] for every particle field.  With `interleave`, each
-// full chunk of kTransferThreads sorted particles (one transfer CTA) is stored
+// dst[j] = src[perm[s(j)]] for every particle field.  With `interleave` = T,
+// each full chunk of T sorted particles (one transfer CTA) is stored
 // transposed: thread kk of the chunk (warp w = kk / 32, lane l = kk % 32) holds
-// sorted particle l * G + w with G = kTransferThreads / 32, so the 32 lanes of
+// sorted particle l * G + w with G = T / 32, so the 32 lanes of
 // a warp take one particle from each of 32 consecutive groups of G
 // (cell-sorted: one or two cells each) and their stencils do not collide on
 // the same shared-memory node.  The last, partial chunk is stored in sorted
@@ -858,10 +860,12 @@ __global__ void k_gather(ParticleSoA src, ParticleSoA dst, const uint32_t *__res
     int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= n) return;
     int sj = j;
-    const int chunk = j / kTransferThreads;
-    if (interleave && (chunk + 1) * kTransferThreads <= n) {
-        const int kk = j - chunk * kTransferThreads;
-        sj = chunk * kTransferThreads + (kk % 32) * kInterleave + kk / 32;
+    if (interleave) {  // interleave = particles per transfer CTA (0: stored in sorted order)
+        const int chunk = j / interleave;
+        if ((chunk + 1) * interleave <= n) {
+            const int kk = j - chunk * interleave;
+            sj = chunk * interleave + (kk % 32) * (interleave / 32) + kk / 32;
+        }
     }
     int s = static_cast<int>(perm[sj]);
     const size_t cs = src.cap, cd = dst.cap;
@@ -938,29 +942,39 @@ void launch_transfer(int mode, const ParticleSoA &P, int n, const DevClass *clas
                      const GridTable &next, const SimParams &sp, const DevObstacle *obstacles, const float *planes,
                      double *reactions, uint32_t *status, int *cache, cudaStream_t stream) {
     if (n <= 0) return;
-    dim3 grid((n + kThreads - 1) / kThreads);
-#define TMPM_LAUNCH(M, PL, V) \
-    k_transfer<M, PL, V><<<grid, kThreads, 0, stream>>>(P, n, classes, cur, next, sp, obstacles, planes, reactions, status, cache)
-#define TMPM_LAUNCH_MODE(M)                          \
-    do {                                             \
-        if (sp.multi) {                              \
-            if (pl) TMPM_LAUNCH(M, true, kMulti);    \
-            else TMPM_LAUNCH(M, false, kMulti);      \
-        } else if (sp.cpic) {                        \
-            if (pl) TMPM_LAUNCH(M, true, kCpic);     \
-            else TMPM_LAUNCH(M, false, kCpic);       \
-        } else {                                     \
-            if (pl) TMPM_LAUNCH(M, true, kPlain);    \
-            else TMPM_LAUNCH(M, false, kPlain);      \
-        }                                            \
-    } while (0)
+    // Launch shapes other than the default exist for the variants the tuner
+    // picks among (no plastic state; one scene or a batch).
     const bool pl = sp.has_plastic != 0;
+    const int shape = (pl || sp.cpic) ? 0 : sp.shape;
+#define TMPM_LAUNCH(M, PL, V, T, B) \
+    k_transfer<M, PL, V, T, B><<<dim3((n + (T) - 1) / (T)), T, 0, stream>>>(P, n, classes, cur, next, sp, obstacles, \
+                                                                           planes, reactions, status, cache)
+#define TMPM_LAUNCH_SHAPES(M, V)                                      \
+    do {                                                              \
+        if (shape == 1) TMPM_LAUNCH(M, false, V, 128, 8);             \
+        else if (shape == 2) TMPM_LAUNCH(M, false, V, 256, 3);        \
+        else TMPM_LAUNCH(M, false, V, 256, TMPM_TRANSFER_MIN_BLOCKS); \
+    } while (0)
+#define TMPM_LAUNCH_MODE(M)                                                      \
+    do {                                                                         \
+        if (sp.multi) {                                                          \
+            if (pl) TMPM_LAUNCH(M, true, kMulti, 256, TMPM_TRANSFER_MIN_BLOCKS); \
+            else TMPM_LAUNCH_SHAPES(M, kMulti);                                  \
+        } else if (sp.cpic) {                                                    \
+            if (pl) TMPM_LAUNCH(M, true, kCpic, 256, TMPM_TRANSFER_MIN_BLOCKS);  \
+            else TMPM_LAUNCH(M, false, kCpic, 256, TMPM_TRANSFER_MIN_BLOCKS);    \
+        } else {                                                                 \
+            if (pl) TMPM_LAUNCH(M, true, kPlain, 256, TMPM_TRANSFER_MIN_BLOCKS); \
+            else TMPM_LAUNCH_SHAPES(M, kPlain);                                  \
+        }                                                                        \
+    } while (0)
     switch (mode) {
     case kModeP2G: TMPM_LAUNCH_MODE(kModeP2G); break;
     case kModeG2P2G: TMPM_LAUNCH_MODE(kModeG2P2G); break;
     default: TMPM_LAUNCH_MODE(kModeG2P); break;
     }
 #undef TMPM_LAUNCH_MODE
+#undef TMPM_LAUNCH_SHAPES
 #undef TMPM_LAUNCH
 }
 
@@ -996,7 +1010,8 @@ void launch_resort(ParticleSoA &src, ParticleSoA &dst, int n, int keep, const De
     k_bin_keys<<<(n + 255) / 256, 256, 0, stream>>>(src.x, src.cap, n, sp.s0.inv_h, src.cls, classes,
                                                     sp.multi ? sp.scenes : nullptr, nullptr, sb.keys[0], sb.vals[0]);
     const int r = radix_sort_pairs(sb, n, sp.multi ? kSortBitsBatch : kSortBitsScene, stream);
-    if (keep > 0) k_gather<<<(keep + 255) / 256, 256, 0, stream>>>(src, dst, sb.vals[r], keep, sp.multi ? 0 : 1);
+    const int interleave = sp.multi ? 0 : kLaunchShapes[sp.shape].threads;
+    if (keep > 0) k_gather<<<(keep + 255) / 256, 256, 0, stream>>>(src, dst, sb.vals[r], keep, interleave);
 }
 
 void launch_dump_grid(const GridTable &g, int32_t *cells, float4 *values, uint32_t *count, uint32_t capacity,

@@ -67,6 +67,8 @@ struct TmpmSession {
     bool force_dirty = false;
     bool has_plastic = false;  // class table holds a snow, sand or NH sand class
     uint64_t since_resort = 0;
+    LaunchTuner tuner;       // transfer launch shape (tuned on the first segments unless fixed)
+    int stored_shape = -1;   // launch shape whose per-CTA interleave the device rows hold
 
     ~TmpmSession() {
         if (stream) {
@@ -218,7 +220,7 @@ struct TmpmSession {
         for (int b = 0; b < 2; ++b)
             if (pbuf[b].cap != cap)
                 if ((e = pbuf[b].alloc(cap))) return cuda_fail(e, "cudaMalloc particles");
-        size_t ctas = (cap + kTransferThreads - 1) / kTransferThreads;
+        size_t ctas = (cap + kMinTransferThreads - 1) / kMinTransferThreads;
         if (cta_cache.count < ctas * kCacheStride)
             if ((e = cta_cache.alloc(ctas * kCacheStride))) return cuda_fail(e, "cudaMalloc cache");
         if (force.count < 3 * std::max<size_t>(world.n, 1)) {
@@ -330,8 +332,13 @@ struct TmpmSession {
         // and the next opens with re-sort, table clear and P2G.
         const uint32_t interval = options.resort_interval ? options.resort_interval : kResortSubsteps;
         uint32_t done = 0;
+        // Plastic and CPIC variants run the default shape only.
+        const bool tunable = !has_plastic && !sp.cpic;
         while (done < steps) {
-        const bool resort_now = since_resort >= interval;
+        const int shape = tunable ? tuner.shape() : 0;
+        sp.shape = shape;
+        // the rows are re-sorted (and re-interleaved) when the shape changes
+        const bool resort_now = since_resort >= interval || shape != stored_shape;
         const uint32_t seg = std::min<uint32_t>(steps - done, resort_now ? interval : interval - since_resort);
         if (resort_now) {
             tick(0);
@@ -348,8 +355,10 @@ struct TmpmSession {
             launch_resort(src, dst, n_dev, n_dev, classes.ptr, sp, sb, stream);
             cur ^= 1;
             since_resort = 0;
+            stored_shape = shape;
             tock(4);
         }
+        if (tunable) tuner.begin(shape, stream);
         GridTable g[2];
         grid_views(g);
         ParticleSoA P = soa();
@@ -376,6 +385,7 @@ struct TmpmSession {
                 force_dirty = false;
             }
         }
+        if (tunable) tuner.end(static_cast<double>(n_dev) * seg, stream);
         since_resort += seg;
         done += seg;
         }
@@ -530,6 +540,7 @@ TmpmStatus tmpm_session_create(const TmpmParams *params, const TmpmParticleArray
     s->use_cpic = use_cpic != 0;
     s->substep_dt = substep_dt;
     s->substeps = s->options.substeps;
+    s->tuner.reset(s->options.launch_shape);
     std::string err;
     if (!params_valid(*params)) {
         g_last_error = "invalid MPM input";
@@ -896,3 +907,26 @@ TmpmStatus tmpm_bench_substeps(TmpmSession *s, uint32_t steps, double *ms, doubl
 }
 
 }  // extern "C"
+
+uint32_t tmpm_launch_shape_count(void) { return static_cast<uint32_t>(kNumLaunchShapes); }
+
+TmpmStatus tmpm_launch_shape_info(uint32_t shape, uint32_t *threads_per_cta, uint32_t *ctas_per_sm) {
+    if (shape >= static_cast<uint32_t>(kNumLaunchShapes)) {
+        g_last_error = "launch shape out of range";
+        return TMPM_ERR_INVALID_INPUT;
+    }
+    if (threads_per_cta) *threads_per_cta = static_cast<uint32_t>(kLaunchShapes[shape].threads);
+    if (ctas_per_sm) *ctas_per_sm = static_cast<uint32_t>(kLaunchShapes[shape].min_blocks);
+    return TMPM_OK;
+}
+
+int32_t tmpm_session_launch_shape(TmpmSession *s, double *ms_per_unit, size_t count) {
+    if (!s) return -1;
+    if (s->tuner.tuning()) {
+        cudaSetDevice(s->device);
+        s->tuner.poll();
+    }
+    if (ms_per_unit) s->tuner.costs(ms_per_unit, static_cast<uint32_t>(count));
+    if (s->has_plastic || s->cpic_active()) return 0;  // variants built for the default shape only
+    return s->tuner.chosen;
+}

@@ -42,7 +42,7 @@ class Session:
 
     def __init__(self, params: TmpmParams, particles: ParticleArrays, substep_dt: float, obstacles=(),
                  use_cpic: bool = True, device: int = 0, max_blocks: int = 0, resort_interval: int = 0,
-                 next_chunk_id: int = 0, substeps: int = 0):
+                 next_chunk_id: int = 0, substeps: int = 0, launch_shape: int | None = None):
         L = _native.lib()
         self._params = params
         arrays = particles.as_c()
@@ -53,6 +53,8 @@ class Session:
         opts.resort_interval = resort_interval
         opts.next_chunk_id = next_chunk_id
         opts.substeps = substeps
+        # None: tuned on the first submits; k: launch shape k (see _native.launch_shapes())
+        opts.launch_shape = 0 if launch_shape is None else int(launch_shape) + 1
         handle = C.c_void_p()
         self._h = None
         st = L.tmpm_session_create(C.byref(params), C.byref(arrays), obs, nobs, int(bool(use_cpic)),
@@ -183,6 +185,11 @@ class Session:
                                             C.byref(count)), self._h)
         n = min(int(count.value), capacity)
         return cells[:n], vals[:n]
+
+    def launch_shape(self) -> dict:
+        """Transfer launch shape in use (None while trials are outstanding) and
+        the measured cost of each shape."""
+        return _native.query_launch_shape(_native.lib().tmpm_session_launch_shape, self._h)
 
     def bench_substeps(self, steps: int, per_kernel: bool = False):
         """Device-timed substeps (CUDA events on the session stream): (ms total, per-kernel ms or None)."""

@@ -51,6 +51,18 @@ def test_struct_layouts_match_header():
     assert C.sizeof(TmpmSessionOptions) == 32
 
 
+def test_launch_shapes_are_listed_without_a_device():
+    from tessera_b200 import _native
+
+    shapes = _native.launch_shapes()
+    assert shapes[0] == (256, 4)  # the default shape: 256 particles per CTA, 4 CTAs per SM
+    assert len(shapes) == 3 and len(set(shapes)) == 3
+    for threads, ctas in shapes:
+        assert threads % 32 == 0 and threads * ctas <= 2048  # whole warps; within an SM's thread slots
+    t = C.c_uint32(0)
+    assert _native.lib().tmpm_launch_shape_info(len(shapes), C.byref(t), None) != 0
+
+
 def _one_particle(material=MAT_ELASTIC, params=(2000.0, 0.2)):
     return density_particles([(0.5, 0.5, 0.5)], 0.04, 1000.0, material, params)
 
