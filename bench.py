@@ -301,7 +301,11 @@ def bench_serving(rates, count: int) -> dict:
         served, span = server.run(reqs)
         s_served = summarize(served, span)
         s_served.update(batches=server.batches, peak_resident=server.peak_resident,
-                        peak_gb=server.peak_bytes / 1e9)
+                        peak_gb=server.peak_bytes / 1e9, launch_shape=shape_summary(server.batch.launch_shape()))
+        tm = dict(server.timing)
+        prep = tm.pop("prepare_s")
+        tm.update(prepare_mean_s=float(np.mean(prep)) if prep else None, prepare_max_s=max(prep) if prep else None)
+        s_served["timing"] = tm
         server.batch.close()
         plain, span_p = run_plain(reqs)
         s_plain = summarize(plain, span_p)

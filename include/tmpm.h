@@ -301,8 +301,11 @@ size_t tmpm_scene_prepared_particle_count(const TmpmPreparedScene *prepared);
 size_t tmpm_scene_prepared_bytes(const TmpmPreparedScene *prepared);
 
 /* Attach a prepared scene (the batch takes ownership, also on failure);
- * *scene_out receives its id (0..255).  Allowed while a batch is in flight:
- * the rows are copied to the device at the next submit. */
+ * *scene_out receives its id (0..255).  Allowed while a batch is in flight.
+ * When the allocated device rows have room, the rows are copied at once on the
+ * batch's upload stream (overlapping the batch in flight; the call returns
+ * once the host rows are staged); otherwise at the next submit, which grows
+ * the rows first.  The scene joins the next submitted batch either way. */
 TmpmStatus tmpm_batch_admit(TmpmBatch *batch, TmpmPreparedScene *prepared, uint32_t *scene_out);
 
 /* tmpm_scene_prepare + tmpm_batch_admit (GpuMpmResidentSession::new for one
@@ -337,6 +340,15 @@ TmpmStatus tmpm_batch_scene_status(const TmpmBatch *batch, uint32_t scene);
 uint64_t tmpm_batch_scene_substeps(const TmpmBatch *batch, uint32_t scene);
 size_t tmpm_batch_scene_particle_count(const TmpmBatch *batch, uint32_t scene);
 TmpmStatus tmpm_batch_read_scene(TmpmBatch *batch, uint32_t scene, TmpmParticleArrays *out);
+
+/* Read + remove in one call, for retiring a finished scene: the non-null
+ * fields of `out` receive the scene's state (as tmpm_batch_read_scene would
+ * return it) and the scene leaves the batch.  Only the requested per-particle
+ * fields are copied from the device, and the scene's host world is not
+ * brought up to date first, since the scene goes; the non-finite check of
+ * collect_prepared (gpu.rs:1940-1989) still covers every transferred field.
+ * A non-finite state fails the scene and keeps it, as a read does. */
+TmpmStatus tmpm_batch_take_scene(TmpmBatch *batch, uint32_t scene, TmpmParticleArrays *out);
 
 /* Device milliseconds of the last synchronized batch (CUDA events on the
  * batch stream around its kernels). */

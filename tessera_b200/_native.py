@@ -112,6 +112,8 @@ def lib():
     L.tmpm_batch_scene_particle_count.restype = C.c_size_t
     L.tmpm_batch_read_scene.argtypes = [P, U32, C.POINTER(TmpmParticleArrays)]
     L.tmpm_batch_read_scene.restype = S
+    L.tmpm_batch_take_scene.argtypes = [P, U32, C.POINTER(TmpmParticleArrays)]
+    L.tmpm_batch_take_scene.restype = S
     L.tmpm_batch_last_ms.argtypes = [P]
     L.tmpm_batch_last_ms.restype = C.c_double
     L.tmpm_batch_device_bytes.argtypes = [P]

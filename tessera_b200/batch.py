@@ -165,6 +165,14 @@ class Batch:
         _check(_native.lib().tmpm_batch_read_scene(self._h, int(scene), C.byref(c)), self._h)
         return arrays
 
+    def take(self, scene: int, fields=("position", "velocity")) -> dict:
+        """Read + remove: the named fields of a finished scene (world order), and
+        the scene leaves the batch.  Only those fields are copied from the device."""
+        c, arrays = partial_arrays(self.count(scene), fields)
+        _check(_native.lib().tmpm_batch_take_scene(self._h, int(scene), C.byref(c)), self._h)
+        self._counts.pop(int(scene), None)
+        return arrays
+
     def last_ms(self) -> float:
         return float(_native.lib().tmpm_batch_last_ms(self._h))
 

@@ -22,9 +22,11 @@
 // runs, every scene it does not advance can still be read from the first
 // buffer, on a side stream, concurrently with the batch.
 //
-// Host staging is ordinary (pageable) memory: pinning a scene-sized buffer
-// costs more than the staged copy it would speed up, and scenes are prepared
-// once and read once.
+// Prepared rows stay in ordinary (pageable) memory: pinning a scene-sized
+// buffer per scene costs more than the staged copy it would speed up.  An
+// admitted scene's rows are copied at once, on an upload stream, when the
+// allocated rows have room, so the copy overlaps the batch in flight; reads go
+// through one pinned buffer that the batch keeps and reuses.
 
 #include <chrono>
 #include <cstdio>
@@ -167,7 +169,21 @@ struct TmpmBatch {
     PinnedBuf table_staging;
     std::vector<std::unique_ptr<TmpmPreparedScene>> in_flight_uploads;  // kept until the copies complete
     cudaStream_t read_stream = nullptr;  // reads of scenes the batch in flight does not advance
-    HostRows read_staging;
+    PinnedBuf read_pinned;               // readback staging, reused by every read
+    HostRows read_pageable;              // fallback when pinned memory is unavailable
+    DevBuf<float> read_unsorted;         // a read scene's rows in world order (27 x its world count)
+    DevBuf<uint32_t> take_flag;          // non-finite flag of a take
+    cudaStream_t upload_stream = nullptr;  // row copies issued at admission
+    cudaEvent_t upload_done = nullptr;
+    bool uploads_open = false;  // copies on upload_stream the batch stream has not waited for yet
+    // Row copies go through two pinned staging buffers: host threads fill one
+    // while the copy engine drains the other (pageable copies are staged by
+    // the driver one small buffer at a time, several times slower).
+    static constexpr size_t kStageBytes = size_t(64) << 20;
+    PinnedBuf stage[2];
+    cudaEvent_t stage_free[2] = {nullptr, nullptr};  // recorded after the copies out of each buffer
+    bool stage_busy[2] = {false, false};
+    std::vector<std::unique_ptr<TmpmPreparedScene>> early_uploads;  // their host rows
     uint64_t epoch = 1;  // bumps whenever a device pointer a graph holds changes
     bool pending = false;
     double last_ms = 0.0;
@@ -187,7 +203,12 @@ struct TmpmBatch {
     std::map<GraphKey, cudaGraphExec_t> graphs;
 
     ~TmpmBatch() {
+        if (upload_stream) cudaStreamSynchronize(upload_stream);
         if (stream) cudaStreamSynchronize(stream);
+        if (upload_done) cudaEventDestroy(upload_done);
+        for (int k = 0; k < 2; ++k)
+            if (stage_free[k]) cudaEventDestroy(stage_free[k]);
+        if (upload_stream) cudaStreamDestroy(upload_stream);
         drop_graphs();
         if (done) cudaEventDestroy(done);
         if (t_begin) cudaEventDestroy(t_begin);
@@ -355,46 +376,159 @@ struct TmpmBatch {
         n_phys = n_live;
     }
 
-    // Copy the rows of admitted scenes to the device (appended after the
-    // resident rows).  Idle only; the packed rows stay alive until the batch
-    // that follows completes.
+    // Copy scene `id`'s staged rows to rows [n_phys, n_phys + m) of the
+    // buffer the next batch re-sorts from, and clear its failure word, on `st`.
+    // Host-to-device copies of (device destination, host source, bytes)
+    // pieces on `st` through the pinned staging buffers; pageable copies when
+    // pinned memory cannot be had.  Returns once every host source has been
+    // read (the device side may still be copying).
+    struct CopyPiece {
+        void *dst;
+        const void *src;
+        size_t bytes;
+    };
+    cudaError_t copy_h2d(const std::vector<CopyPiece> &pieces, cudaStream_t st) {
+        cudaError_t e;
+        bool pinned = true;
+        for (int k = 0; k < 2 && pinned; ++k) {
+            if (!stage_free[k] && cudaEventCreateWithFlags(&stage_free[k], cudaEventDisableTiming) != cudaSuccess) {
+                stage_free[k] = nullptr;
+                pinned = false;
+            }
+            if (pinned && !stage[k].ensure(kStageBytes)) pinned = false;
+        }
+        if (!pinned) {
+            cudaGetLastError();
+            for (const CopyPiece &c : pieces)
+                if ((e = cudaMemcpyAsync(c.dst, c.src, c.bytes, cudaMemcpyHostToDevice, st))) return e;
+            return cudaSuccess;
+        }
+        int b = 0;
+        size_t fill = 0;
+        // pieces packed into stage[b]: src = host source, dst = device destination,
+        // bytes; staged at offset `at`
+        struct Staged {
+            CopyPiece c;
+            size_t at;
+        };
+        std::vector<Staged> queued;
+        auto wait_free = [&](int k) -> cudaError_t {
+            if (!stage_busy[k]) return cudaSuccess;
+            stage_busy[k] = false;
+            return cudaEventSynchronize(stage_free[k]);
+        };
+        // fill stage[b] from the host sources (one parallel pass over its bytes),
+        // queue the copies out of it and move to the other buffer
+        auto flush = [&]() -> cudaError_t {
+            char *base = static_cast<char *>(stage[b].ptr);
+            parallel_chunks(fill, [&](size_t, size_t lo, size_t hi) {
+                for (const Staged &q : queued) {
+                    const size_t a = std::max(lo, q.at), z = std::min(hi, q.at + q.c.bytes);
+                    if (a < z) std::memcpy(base + a, static_cast<const char *>(q.c.src) + (a - q.at), z - a);
+                }
+            }, size_t(4) << 20);
+            cudaError_t err;
+            for (const Staged &q : queued)
+                if ((err = cudaMemcpyAsync(q.c.dst, base + q.at, q.c.bytes, cudaMemcpyHostToDevice, st))) return err;
+            queued.clear();
+            if ((err = cudaEventRecord(stage_free[b], st))) return err;
+            stage_busy[b] = true;
+            b ^= 1;
+            fill = 0;
+            return wait_free(b);
+        };
+        if ((e = wait_free(b))) return e;
+        for (const CopyPiece &c : pieces) {
+            size_t done = 0;
+            while (done < c.bytes) {
+                if (fill == kStageBytes && (e = flush())) return e;
+                const size_t n = std::min(c.bytes - done, kStageBytes - fill);
+                queued.push_back({{static_cast<char *>(c.dst) + done, static_cast<const char *>(c.src) + done, n}, fill});
+                fill += n;
+                done += n;
+            }
+        }
+        if (!queued.empty() && (e = flush())) return e;
+        return cudaSuccess;
+    }
+
+    cudaError_t copy_scene_rows(size_t id, cudaStream_t st) {
+        TmpmPreparedScene &p = *scenes[id].staged;
+        const size_t m = p.m, stride = std::max<size_t>(m, 1);
+        const size_t pc = pbuf[cur].cap;
+        const ParticleBuffers &pb = pbuf[cur];
+        cudaError_t e = cudaSuccess;
+        if (m) {
+            // host rows: 27 f32 component rows, class, world index (stride m);
+            // device rows: the same order across the fields (pitch cap)
+            const float *hb = row_base(p.rows);
+            std::vector<CopyPiece> pieces;
+            auto rows = [&](float *dst, int first, int count) {
+                for (int r = 0; r < count; ++r)
+                    pieces.push_back({dst + r * pc + n_phys, hb + (first + r) * stride, m * 4});
+            };
+            rows(pb.x.ptr, 0, 3);
+            rows(pb.v.ptr, 3, 3);
+            rows(pb.C.ptr, 6, 9);
+            rows(pb.F.ptr, 15, 9);
+            rows(pb.pl.ptr, 24, 3);
+            pieces.push_back({pb.cls.ptr + n_phys, row_cls(p.rows, stride), m * 4});
+            pieces.push_back({pb.widx.ptr + n_phys, row_widx(p.rows, stride), m * 4});
+            if ((e = copy_h2d(pieces, st))) return e;
+        }
+        if ((e = cudaMemsetAsync(scene_status.ptr + id, 0, sizeof(uint32_t), st))) return e;
+        scenes[id].dev_offset = n_phys;
+        n_phys += m;
+        return cudaSuccess;
+    }
+
+    // Copy an admitted scene's rows now, on the upload stream, if the
+    // allocated rows have room: rows from n_phys on in the buffer the next
+    // batch re-sorts from are free (a batch in flight writes only the first
+    // n_phys rows of it), so the copy overlaps that batch.  Without room the
+    // rows stay staged and the next submit grows the buffers and copies them.
+    TmpmStatus upload_early(size_t id) {
+        if (n_phys + scenes[id].staged->m > pbuf[cur].cap) return TMPM_OK;
+        cudaError_t e;
+        if ((e = copy_scene_rows(id, upload_stream))) return cuda_fail(e, "scene upload");
+        early_uploads.push_back(std::move(scenes[id].staged));
+        uploads_open = true;
+        return TMPM_OK;
+    }
+
+    // Order the batch stream after the copies admission issued.
+    TmpmStatus join_uploads() {
+        if (!uploads_open) return TMPM_OK;
+        cudaError_t e;
+        if ((e = cudaEventRecord(upload_done, upload_stream)) || (e = cudaStreamWaitEvent(stream, upload_done, 0)))
+            return cuda_fail(e, "scene upload");
+        for (auto &p : early_uploads) in_flight_uploads.push_back(std::move(p));
+        early_uploads.clear();
+        uploads_open = false;
+        return TMPM_OK;
+    }
+
+    // Copy the rows of admitted scenes still staged to the device (appended
+    // after the resident rows), upload the class table and size the grid.
+    // Idle only; the packed rows stay alive until the batch that follows
+    // completes.
     TmpmStatus commit_staged() {
+        TmpmStatus st;
+        if ((st = join_uploads()) != TMPM_OK) return st;
         size_t add = 0;
         for (BatchScene &s : scenes)
             if (s.live && s.staged) add += s.staged->m;
         bool any = false;
         for (BatchScene &s : scenes) any = any || (s.live && s.staged);
-        if (!any) return TMPM_OK;
-        TmpmStatus st;
-        if ((st = ensure_rows(n_phys + add)) != TMPM_OK) return st;
+        if (any && (st = ensure_rows(n_phys + add)) != TMPM_OK) return st;
         if ((st = upload_classes()) != TMPM_OK) return st;
         if ((st = ensure_grid()) != TMPM_OK) return st;
-        const size_t pc = pbuf[cur].cap;
-        const ParticleBuffers &pb = pbuf[cur];
+        if (!any) return TMPM_OK;
         cudaError_t e;
         for (size_t id = 0; id < scenes.size(); ++id) {
             BatchScene &s = scenes[id];
             if (!s.live || !s.staged) continue;
-            TmpmPreparedScene &p = *s.staged;
-            const size_t m = p.m, stride = std::max<size_t>(m, 1);
-            if (m) {
-                const float *hb = row_base(p.rows);
-                const uint32_t *hcls = row_cls(p.rows, stride), *hw = row_widx(p.rows, stride);
-                auto rows = [&](float *dst, const float *src, int r) {
-                    return cudaMemcpy2DAsync(dst + n_phys, pc * 4, src, stride * 4, m * 4, r, cudaMemcpyHostToDevice,
-                                             stream);
-                };
-                if ((e = rows(pb.x.ptr, hb, 3)) || (e = rows(pb.v.ptr, hb + 3 * stride, 3)) ||
-                    (e = rows(pb.C.ptr, hb + 6 * stride, 9)) || (e = rows(pb.F.ptr, hb + 15 * stride, 9)) ||
-                    (e = rows(pb.pl.ptr, hb + 24 * stride, 3)) ||
-                    (e = cudaMemcpyAsync(pb.cls.ptr + n_phys, hcls, m * 4, cudaMemcpyHostToDevice, stream)) ||
-                    (e = cudaMemcpyAsync(pb.widx.ptr + n_phys, hw, m * 4, cudaMemcpyHostToDevice, stream)))
-                    return cuda_fail(e, "scene upload");
-            }
-            if ((e = cudaMemsetAsync(scene_status.ptr + id, 0, sizeof(uint32_t), stream)))
-                return cuda_fail(e, "scene status");
-            s.dev_offset = n_phys;
-            n_phys += m;
+            if ((e = copy_scene_rows(id, stream))) return cuda_fail(e, "scene upload");
             in_flight_uploads.push_back(std::move(s.staged));
         }
         return TMPM_OK;
@@ -473,24 +607,36 @@ struct TmpmBatch {
     }
     int prev_buf = 0;  // row buffer the batch in flight re-sorts from (and only reads)
 
-    // Copy a scene's rows (27 f32 rows + widx, stride m) from row buffer `buf`
-    // at row `off` into `dst` on `st`, and wait for the copy.
-    TmpmStatus read_rows(BatchScene &s, int buf, size_t off, cudaStream_t st, HostRows &dst) {
-        const size_t m = s.dev_count, stride = std::max<size_t>(m, 1);
-        dst.resize(28 * stride);
+    // Host staging for a read of `m` rows: the pinned buffer (grown by half
+    // again when too small), else pageable memory.
+    float *read_staging(size_t floats) {
+        const size_t bytes = std::max<size_t>(floats, 1) * sizeof(float);
+        if (read_pinned.bytes >= bytes || read_pinned.ensure(std::max(bytes, read_pinned.bytes + read_pinned.bytes / 2)))
+            return static_cast<float *>(read_pinned.ptr);
+        read_pageable.resize(std::max<size_t>(floats, 1));
+        return read_pageable.data();
+    }
+
+    // Put a scene's rows (m stored rows at row `off` of row buffer `buf`) in
+    // world order on the device (27 f32 rows of stride N = its world count;
+    // rows of disabled particles are left unwritten), copy them into `h` on
+    // `st`, and wait: the host then applies them front to back instead of
+    // scattering by world index.
+    TmpmStatus read_rows(BatchScene &s, int buf, size_t off, cudaStream_t st, float *h) {
+        const size_t m = s.dev_count, N = s.world.n;
         if (!m) return TMPM_OK;
-        const size_t pc = pbuf[buf].cap;
-        float *h = dst.data();
-        const ParticleBuffers &pb = pbuf[buf];
-        auto rows = [&](float *d, const float *src, int r) {
-            return cudaMemcpy2DAsync(d, stride * 4, src + off, pc * 4, m * 4, r, cudaMemcpyDeviceToHost, st);
-        };
         cudaError_t e;
-        if ((e = rows(h, pb.x.ptr, 3)) || (e = rows(h + 3 * stride, pb.v.ptr, 3)) ||
-            (e = rows(h + 6 * stride, pb.C.ptr, 9)) || (e = rows(h + 15 * stride, pb.F.ptr, 9)) ||
-            (e = rows(h + 24 * stride, pb.pl.ptr, 3)) ||
-            (e = cudaMemcpyAsync(reinterpret_cast<uint32_t *>(h + 27 * stride), pb.widx.ptr + off, m * 4,
-                                 cudaMemcpyDeviceToHost, st)) ||
+        if (read_unsorted.count < 27 * N && (e = read_unsorted.alloc(27 * N))) return cuda_fail(e, "cudaMalloc readback");
+        ParticleSoA P = pbuf[buf].view(nullptr, 1);
+        P.x += off;
+        P.v += off;
+        P.C += off;
+        P.F += off;
+        P.pl += off;
+        P.cls += off;
+        P.widx += off;
+        launch_unsort(P, static_cast<int>(m), read_unsorted.ptr, N, st);
+        if ((e = cudaMemcpyAsync(h, read_unsorted.ptr, sizeof(float) * 27 * N, cudaMemcpyDeviceToHost, st)) ||
             (e = cudaStreamSynchronize(st)))
             return cuda_fail(e, "scene readback");
         return TMPM_OK;
@@ -555,17 +701,20 @@ struct TmpmBatch {
         return TMPM_OK;
     }
 
-    // Apply rows (27 f32 rows + widx, stride m) to a scene's host world
-    // (collect_prepared + apply_gpu_transfers, gpu.rs:1821-1989, 2295-2329).
-    TmpmStatus apply_rows(BatchScene &s, HostRows &src) {
-        const size_t m = s.dev_count, stride = std::max<size_t>(m, 1);
-        const float *h = src.data();
-        const uint32_t *widx = reinterpret_cast<const uint32_t *>(h + 27 * stride);
+    // Apply world-order rows (27 f32 rows of stride N, as read_rows leaves
+    // them) to a scene's host world (collect_prepared + apply_gpu_transfers,
+    // gpu.rs:1821-1989, 2295-2329): a non-finite value of an enabled particle
+    // fails the scene before anything is applied; fixed particles keep their
+    // position and get zero velocity and affine field.
+    TmpmStatus apply_rows(BatchScene &s, const float *h) {
+        HostWorld &w = s.world;
+        const size_t N = w.n;
+        if (!s.dev_count) return TMPM_OK;
         std::atomic<bool> bad{false};
-        parallel_for(m, [&](size_t a, size_t b) {
+        parallel_for(N, [&](size_t a, size_t b) {
             for (size_t c = 0; c < 27 && !bad.load(std::memory_order_relaxed); ++c)
-                for (size_t j = a; j < b; ++j)
-                    if (!std::isfinite(h[c * stride + j])) {
+                for (size_t i = a; i < b; ++i)
+                    if (w.enabled[i] && !std::isfinite(h[c * N + i])) {
                         bad = true;
                         break;
                     }
@@ -575,27 +724,26 @@ struct TmpmBatch {
             s.error = "MPM integration produced a non-finite state";
             return s.status;
         }
-        HostWorld &w = s.world;
         ++w.version;
-        parallel_for(m, [&](size_t a, size_t b) {
-            for (size_t j = a; j < b; ++j) {
-                size_t i = widx[j];
+        parallel_for(N, [&](size_t a, size_t b) {
+            for (size_t i = a; i < b; ++i) {
+                if (!w.enabled[i]) continue;
                 if (w.fixed[i]) {
                     for (int k = 0; k < 3; ++k) w.vel[3 * i + k] = 0.0;
                     for (int k = 0; k < 9; ++k) w.C[9 * i + k] = 0.0;
                     continue;
                 }
                 for (int k = 0; k < 3; ++k) {
-                    w.pos[3 * i + k] = h[(0 + k) * stride + j];
-                    w.vel[3 * i + k] = h[(3 + k) * stride + j];
+                    w.pos[3 * i + k] = h[(0 + k) * N + i];
+                    w.vel[3 * i + k] = h[(3 + k) * N + i];
                 }
                 for (int k = 0; k < 9; ++k) {
-                    w.C[9 * i + k] = h[(6 + k) * stride + j];
-                    w.F[9 * i + k] = h[(15 + k) * stride + j];
+                    w.C[9 * i + k] = h[(6 + k) * N + i];
+                    w.F[9 * i + k] = h[(15 + k) * N + i];
                 }
                 const int mat = w.material[i];
                 if (mat == TMPM_MAT_SAND || mat == TMPM_MAT_SNOW || mat == TMPM_MAT_SAND_NEO_HOOKEAN)
-                    for (int k = 0; k < 3; ++k) w.plastic[3 * i + k] = h[(24 + k) * stride + j];
+                    for (int k = 0; k < 3; ++k) w.plastic[3 * i + k] = h[(24 + k) * N + i];
             }
         });
         return TMPM_OK;
@@ -608,13 +756,14 @@ struct TmpmBatch {
         if (pending && s.queued) return fail(TMPM_ERR_PENDING_STEPS, "the scene is in the batch in flight");
         if (!s.stale) return TMPM_OK;
         TmpmStatus st;
+        float *h = read_staging(27 * s.world.n);
         if (pending) {
-            st = read_rows(s, prev_buf, s.prev_offset, read_stream, read_staging);
+            st = read_rows(s, prev_buf, s.prev_offset, read_stream, h);
         } else {
-            st = read_rows(s, cur, s.dev_offset, stream, read_staging);
+            st = read_rows(s, cur, s.dev_offset, stream, h);
         }
         if (st != TMPM_OK) return st;
-        st = apply_rows(s, read_staging);
+        st = apply_rows(s, h);
         s.stale = false;
         return st;
     }
@@ -667,7 +816,89 @@ struct TmpmBatch {
         scenes[id] = std::move(sc);
         n_live += scenes[id].dev_count;
         if (id_out) *id_out = static_cast<uint32_t>(id);
-        return TMPM_OK;
+        return upload_early(static_cast<size_t>(id));
+    }
+
+    // The scene's state into the non-null fields of `out`, then its removal
+    // (a server's retire step).  When the device holds newer state than the
+    // host world, only the requested per-particle rows cross to the host, in
+    // world order, and go straight into `out`; the host world is not updated,
+    // since the scene goes.  The non-finite check covers every transferred
+    // component, on the device (collect_prepared, gpu.rs:1940-1989); a
+    // non-finite state fails the scene and keeps it, like a read.
+    TmpmStatus take(uint32_t id, const TmpmParticleArrays &out) {
+        BatchScene &s = scenes[id];
+        if (pending && s.queued) return fail(TMPM_ERR_PENDING_STEPS, "the scene is in the batch in flight");
+        HostWorld &w = s.world;
+        if (!s.stale || !s.dev_count) {
+            w.store(const_cast<TmpmParticleArrays &>(out));
+            return remove(id);
+        }
+        const size_t m = s.dev_count, N = w.n;
+        // device components: position 0-2, velocity 3-5, affine 6-14, deformation 15-23, plastic 24-26
+        double *const dst[5] = {out.position, out.velocity, out.affine, out.deformation, out.plastic};
+        const int first[5] = {0, 3, 6, 15, 24}, width[5] = {3, 3, 9, 9, 3};
+        int at[5], rows = 0;
+        for (int f = 0; f < 5; ++f) {
+            at[f] = rows;
+            if (dst[f]) rows += width[f];
+        }
+        cudaStream_t st = pending ? read_stream : stream;
+        ParticleSoA P = pbuf[pending ? prev_buf : cur].view(nullptr, 1);
+        const size_t off = pending ? s.prev_offset : s.dev_offset;
+        P.x += off;
+        P.v += off;
+        P.C += off;
+        P.F += off;
+        P.pl += off;
+        P.cls += off;
+        P.widx += off;
+        cudaError_t e;
+        if (read_unsorted.count < 27 * N && (e = read_unsorted.alloc(27 * N))) return cuda_fail(e, "cudaMalloc readback");
+        if (!take_flag.count && (e = take_flag.alloc(1))) return cuda_fail(e, "cudaMalloc readback");
+        float *h = read_staging(static_cast<size_t>(rows) * N + 1);
+        uint32_t *hflag = reinterpret_cast<uint32_t *>(h + static_cast<size_t>(rows) * N);
+        if ((e = cudaMemsetAsync(take_flag.ptr, 0, sizeof(uint32_t), st))) return cuda_fail(e, "scene readback");
+        launch_unsort(P, static_cast<int>(m), read_unsorted.ptr, N, st, take_flag.ptr);
+        for (int f = 0; f < 5; ++f)
+            if (dst[f] && (e = cudaMemcpyAsync(h + static_cast<size_t>(at[f]) * N, read_unsorted.ptr + first[f] * N,
+                                               sizeof(float) * width[f] * N, cudaMemcpyDeviceToHost, st)))
+                return cuda_fail(e, "scene readback");
+        if ((e = cudaMemcpyAsync(hflag, take_flag.ptr, sizeof(uint32_t), cudaMemcpyDeviceToHost, st)) ||
+            (e = cudaStreamSynchronize(st)))
+            return cuda_fail(e, "scene readback");
+        if (*hflag) {
+            s.status = TMPM_ERR_NON_FINITE_STATE;
+            s.error = "MPM integration produced a non-finite state";
+            return s.status;
+        }
+        // fields the device does not hold come from the host world
+        TmpmParticleArrays rest = out;
+        rest.position = rest.velocity = rest.affine = rest.deformation = rest.plastic = nullptr;
+        w.store(rest);
+        parallel_for(N, [&](size_t a, size_t b) {
+            for (size_t i = a; i < b; ++i) {
+                const bool dev = w.enabled[i] && !w.fixed[i];
+                const int mat = w.material[i];
+                const bool plastic = mat == TMPM_MAT_SAND || mat == TMPM_MAT_SNOW || mat == TMPM_MAT_SAND_NEO_HOOKEAN;
+                for (int f = 0; f < 5; ++f) {
+                    if (!dst[f]) continue;
+                    const int k = width[f];
+                    double *d = dst[f] + k * i;
+                    const float *src = h + static_cast<size_t>(at[f]) * N + i;
+                    if (dev && (f != 4 || plastic)) {
+                        for (int c = 0; c < k; ++c) d[c] = src[c * N];
+                    } else if (w.enabled[i] && (f == 1 || f == 2)) {
+                        for (int c = 0; c < k; ++c) d[c] = 0.0;  // fixed: zero velocity and affine field
+                    } else {
+                        const double *hw = f == 0 ? w.pos.data() : f == 1 ? w.vel.data() : f == 2 ? w.C.data()
+                                         : f == 3 ? w.F.data() : w.plastic.data();
+                        for (int c = 0; c < k; ++c) d[c] = hw[k * i + c];
+                    }
+                }
+            }
+        });
+        return remove(id);
     }
 
     TmpmStatus remove(uint32_t id) {
@@ -683,6 +914,9 @@ struct TmpmBatch {
     // Drop the rows of removed scenes now (a re-sort without substeps).  Idle only.
     TmpmStatus compact() {
         for (BatchScene &s : scenes) s.queued = 0;
+        // rows copied at admission take part in the re-sort: their copies and classes first
+        TmpmStatus st;
+        if ((st = join_uploads()) != TMPM_OK || (st = upload_classes()) != TMPM_OK) return st;
         cudaError_t e;
         if ((e = upload_table())) return cuda_fail(e, "scene table upload");
         if (n_phys) {
@@ -721,6 +955,7 @@ struct TmpmBatch {
             b += static_cast<size_t>(grids[g].max_blocks) * (kNodesPerBlock * 16 + 16) +
                  static_cast<size_t>(grids[g].capacity) * 12;
         b += cta_cache.count * 4 + dclasses.count * sizeof(DevClass) + kMaxScenes * (sizeof(SceneParams) + 4);
+        b += read_unsorted.count * 4;
         return b;
     }
 };
@@ -763,6 +998,8 @@ TmpmStatus tmpm_batch_create(const TmpmBatchOptions *options, TmpmBatch **out) {
     cudaError_t e;
     if ((e = cudaSetDevice(b->device)) || (e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking)) ||
         (e = cudaStreamCreateWithFlags(&b->read_stream, cudaStreamNonBlocking)) ||
+        (e = cudaStreamCreateWithFlags(&b->upload_stream, cudaStreamNonBlocking)) ||
+        (e = cudaEventCreateWithFlags(&b->upload_done, cudaEventDisableTiming)) ||
         (e = cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming)) || (e = cudaEventCreate(&b->t_begin)) ||
         (e = cudaEventCreate(&b->t_end)) || (e = b->status.alloc(1)) || (e = b->scene_status.alloc(kMaxScenes)) ||
         (e = b->dscenes.alloc(kMaxScenes))) {
@@ -802,6 +1039,7 @@ TmpmStatus tmpm_batch_admit(TmpmBatch *b, TmpmPreparedScene *prepared, uint32_t 
     std::unique_ptr<TmpmPreparedScene> p(prepared);
     TmpmStatus st = b->guard(false);
     if (st != TMPM_OK) return st;
+    cudaSetDevice(b->device);
     return b->admit(std::move(p), scene_out);
 }
 
@@ -818,6 +1056,20 @@ TmpmStatus tmpm_batch_add_scene(TmpmBatch *b, const TmpmParams *params, const Tm
     if (st != TMPM_OK) return b->fail(st, g_last_error);
     cudaSetDevice(b->device);
     return b->admit(std::move(p), scene_out);
+}
+
+TmpmStatus tmpm_batch_take_scene(TmpmBatch *b, uint32_t scene, TmpmParticleArrays *out) {
+    if (!b || !out) return TMPM_ERR_INVALID_INPUT;
+    TmpmStatus st = b->guard(false);
+    if (st != TMPM_OK) return st;
+    BatchScene *s = b->scene_at(scene);
+    if (!s) return b->fail(TMPM_ERR_INVALID_INPUT, "unknown scene id");
+    if (s->status != TMPM_OK) return b->fail(s->status, s->error);
+    if (out->count != s->world.n) return b->fail(TMPM_ERR_INVALID_INPUT, "output array count does not match the scene");
+    cudaSetDevice(b->device);
+    st = b->take(scene, *out);
+    if (st != TMPM_OK) return b->fail(st, s->error.empty() ? b->last_error : s->error);
+    return TMPM_OK;
 }
 
 TmpmStatus tmpm_batch_remove_scene(TmpmBatch *b, uint32_t scene) {

@@ -185,7 +185,11 @@ void launch_dump_grid(const GridTable &g, int32_t *cells, float4 *values, uint32
                       cudaStream_t stream);
 void launch_snapshot(const ParticleSoA &P, int n, const DevClass *classes, float4 *out, cudaStream_t stream);
 // 27 f32 rows (x, v, C, F, plastic) of the stored particles into world order, `stride` floats per row.
-void launch_unsort(const ParticleSoA &P, int n, float *out, size_t stride, cudaStream_t stream);
+// Rows in world order: out[c * stride + widx[j]] = component c of stored row j
+// (27 f32 components: x, v, C, F, plastic); `nonfinite`, when given, gets bit 0
+// set if any of them is not finite.
+void launch_unsort(const ParticleSoA &P, int n, float *out, size_t stride, cudaStream_t stream,
+                   uint32_t *nonfinite = nullptr);
 int device_sm_count();
 
 // Thread-local reason reported by tmpm_last_error() (tmpm_session.cu).

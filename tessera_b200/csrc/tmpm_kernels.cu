@@ -886,19 +886,25 @@ __global__ void k_gather(ParticleSoA src, ParticleSoA dst, const uint32_t *__res
 // particle j, for the 27 f32 components (x, v, C, F, plastic), so the host
 // applies a readback sequentially instead of scattering through the sort
 // permutation.
-__global__ void k_unsort(ParticleSoA P, int n, float *__restrict__ out, size_t stride) {
+__global__ void k_unsort(ParticleSoA P, int n, float *__restrict__ out, size_t stride, uint32_t *nonfinite) {
     int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= n) return;
     const size_t cap = P.cap, w = P.widx[j];
+    bool finite = true;
     for (int c = 0; c < 3; ++c) {
-        out[c * stride + w] = P.x[c * cap + j];
-        out[(3 + c) * stride + w] = P.v[c * cap + j];
-        out[(24 + c) * stride + w] = P.pl[c * cap + j];
+        const float x = P.x[c * cap + j], v = P.v[c * cap + j], p = P.pl[c * cap + j];
+        finite = finite && isfinite(x) && isfinite(v) && isfinite(p);
+        out[c * stride + w] = x;
+        out[(3 + c) * stride + w] = v;
+        out[(24 + c) * stride + w] = p;
     }
     for (int c = 0; c < 9; ++c) {
-        out[(6 + c) * stride + w] = P.C[c * cap + j];
-        out[(15 + c) * stride + w] = P.F[c * cap + j];
+        const float a = P.C[c * cap + j], f = P.F[c * cap + j];
+        finite = finite && isfinite(a) && isfinite(f);
+        out[(6 + c) * stride + w] = a;
+        out[(15 + c) * stride + w] = f;
     }
+    if (nonfinite && !finite) atomicOr(nonfinite, 1u);
 }
 
 __global__ void k_dump_grid(GridTable g, int32_t *cells, float4 *values, uint32_t *count, uint32_t capacity) {
@@ -1019,9 +1025,9 @@ void launch_dump_grid(const GridTable &g, int32_t *cells, float4 *values, uint32
     k_dump_grid<<<device_sm_count() * 4, 256, 0, stream>>>(g, cells, values, count, capacity);
 }
 
-void launch_unsort(const ParticleSoA &P, int n, float *out, size_t stride, cudaStream_t stream) {
+void launch_unsort(const ParticleSoA &P, int n, float *out, size_t stride, cudaStream_t stream, uint32_t *nonfinite) {
     if (n <= 0) return;
-    k_unsort<<<(n + 255) / 256, 256, 0, stream>>>(P, n, out, stride);
+    k_unsort<<<(n + 255) / 256, 256, 0, stream>>>(P, n, out, stride, nonfinite);
 }
 
 void launch_snapshot(const ParticleSoA &P, int n, const DevClass *classes, float4 *out, cudaStream_t stream) {

@@ -5,7 +5,9 @@ are prepared (validated and packed for upload) on worker threads
 while the device runs, admitted in arrival order while their device
 footprint fits the HBM budget and a scene slot is free, and advanced
 together: every batch moves each resident scene by up to `chunk` substeps
-in one set of launches.  A scene that finishes in a batch is read while the
+in one set of launches.  Admission happens while a batch runs, so a new
+scene's rows are copied to the device during it and the scene joins the next
+batch, or at once when the device has nothing else to run.  A scene that finishes in a batch is read while the
 next batch runs (the batch does not touch it) and retired, which frees its
 budget.  Requests that arrive while
 others are on the device therefore join at the next batch boundary instead
@@ -115,6 +117,20 @@ class Server:
         self.batches = 0
         self.peak_resident = 0
         self.peak_bytes = 0.0
+        # where the run's time went (seconds): host time in submit (it copies
+        # rows admitted without room), in admission (it copies rows while a
+        # batch runs), in reading and retiring finished scenes, waiting
+        # for a batch, idle waiting for a preparation; device time of the batches
+        # (CUDA events); and each preparation's own duration on its worker
+        self.timing = {"submit_s": 0.0, "admit_s": 0.0, "retire_s": 0.0, "sync_wait_s": 0.0, "prepare_wait_s": 0.0,
+                       "device_s": 0.0, "first_submit_s": None, "prepare_s": []}
+
+    def _prepare_timed(self, params, particles, dt):
+        t = self.clock()
+        try:
+            return self.prepare(params, particles, dt)
+        finally:
+            self.timing["prepare_s"].append(self.clock() - t)
 
     def run(self, requests: list[Request]) -> tuple[list[Outcome], float]:
         reqs = sorted(requests, key=lambda r: r.arrival)
@@ -140,48 +156,73 @@ class Server:
                     break
                 if w[1] is None:
                     sc = w[0].scene
-                    w[1] = pool.submit(self.prepare, sc.params, sc.particles, sc.dt)
+                    w[1] = pool.submit(self._prepare_timed, sc.params, sc.particles, sc.dt)
 
         def retire(sid: int):
+            t_r = self.clock()
             req, _, nbytes = resident.pop(sid)
             o = outcomes[req.rid]
+            take = getattr(self.batch, "take", None)  # read + remove in one call, where the batch has it
+            removed = False
             try:
-                out = self.batch.read(sid, OUTPUT_FIELDS)
+                if take is not None:
+                    out = take(sid, OUTPUT_FIELDS)
+                    removed = True
+                else:
+                    out = self.batch.read(sid, OUTPUT_FIELDS)
                 if self.keep_outputs:
                     o.outputs = out
             except TesseraError as e:
                 o.status, o.error = e.status, e.reason
             o.finished = now()
-            self.batch.remove_scene(sid)
+            if not removed:
+                self.batch.remove_scene(sid)
             self.used -= nbytes
+            self.timing["retire_s"] += self.clock() - t_r
+
+        def admit_ready(limit=None):
+            # admission in arrival order, by device footprint (at most `limit` scenes)
+            admitted = 0
+            while waiting and waiting[0][1] is not None and waiting[0][1].done():
+                if limit is not None and admitted >= limit:
+                    break
+                req, fut = waiting[0]
+                o = outcomes[req.rid]
+                try:
+                    prepared = fut.result()
+                except TesseraError as e:
+                    waiting.popleft()
+                    o.status, o.error, o.finished = e.status, e.reason, now()
+                    continue
+                need = float(prepared.device_bytes())
+                if need > self.budget:
+                    waiting.popleft()
+                    o.status, o.error, o.finished = TMPM_ERR_CAPACITY, "scene exceeds the HBM budget", now()
+                    continue
+                if self.used + need > self.budget or len(resident) >= self.max_scenes:
+                    break
+                t_a = self.clock()
+                sid = self.batch.admit(prepared)
+                self.timing["admit_s"] += self.clock() - t_a
+                admitted += 1
+                waiting.popleft()
+                self.used += need
+                resident[sid] = [req, req.steps, need]
+                o.admitted = now()
+                arrivals()
+
+        def pending_work():
+            return {sid: min(self.chunk, st[1]) for sid, st in resident.items() if st[1] > 0}
 
         try:
             while True:
                 arrivals()
-                # admission in arrival order, by device footprint
-                while waiting and waiting[0][1] is not None and waiting[0][1].done():
-                    req, fut = waiting[0]
-                    o = outcomes[req.rid]
-                    try:
-                        prepared = fut.result()
-                    except TesseraError as e:
-                        waiting.popleft()
-                        o.status, o.error, o.finished = e.status, e.reason, now()
-                        continue
-                    need = float(prepared.device_bytes())
-                    if need > self.budget:
-                        waiting.popleft()
-                        o.status, o.error, o.finished = TMPM_ERR_CAPACITY, "scene exceeds the HBM budget", now()
-                        continue
-                    if self.used + need > self.budget or len(resident) >= self.max_scenes:
-                        break
-                    sid = self.batch.admit(prepared)
-                    waiting.popleft()
-                    self.used += need
-                    resident[sid] = [req, req.steps, need]
-                    o.admitted = now()
-                    arrivals()
-                active = {sid: min(self.chunk, st[1]) for sid, st in resident.items() if st[1] > 0}
+                active = pending_work()
+                if not active:
+                    # nothing to run: admit one scene now and start on it (otherwise admission
+                    # waits for the batch in flight, so rows are copied while the device works)
+                    admit_ready(limit=1)
+                    active = pending_work()
                 if not active:
                     for sid in finished:
                         retire(sid)
@@ -190,11 +231,17 @@ class Server:
                         break
                     # idle: the next arrival or a preparation in progress
                     if waiting and waiting[0][1] is not None:
+                        t_w = self.clock()
                         waiting[0][1].result()
+                        self.timing["prepare_wait_s"] += self.clock() - t_w
                     elif nxt < len(reqs):
                         time.sleep(max(0.0, min(reqs[nxt].arrival - now(), 0.005)))
                     continue
+                t_s = self.clock()
+                if self.timing["first_submit_s"] is None:
+                    self.timing["first_submit_s"] = t_s - t0
                 self.batch.submit(active)
+                self.timing["submit_s"] += self.clock() - t_s
                 self.batches += 1
                 self.peak_resident = max(self.peak_resident, len(resident))
                 self.peak_bytes = max(self.peak_bytes, self.used)
@@ -203,7 +250,13 @@ class Server:
                     retire(sid)
                 finished = []
                 arrivals()
+                admit_ready()  # joins the next batch
+                t_s = self.clock()
                 self.batch.synchronize()
+                self.timing["sync_wait_s"] += self.clock() - t_s
+                last_ms = getattr(self.batch, "last_ms", None)
+                if last_ms is not None:
+                    self.timing["device_s"] += float(last_ms()) / 1e3
                 for sid, k in active.items():
                     st = resident[sid]
                     status = self.batch.status(sid)

@@ -220,3 +220,41 @@ def test_admission_and_reads_while_a_batch_is_in_flight():
         b.particles(a)
     # a prepared scene that is never admitted just goes away
     PreparedScene(scs[2].params, scs[2].particles, scs[2].dt).close()
+
+
+def test_take_returns_what_a_read_returns_and_removes_the_scene():
+    """Retiring through take (only the requested rows come back, the host world
+    is not updated first) gives the state a read gives, fixed and disabled
+    particles included, and frees the scene's slot."""
+    sc = scenes.batch_scene(31, cells=6)
+    parts = sc.particles.copy()
+    parts.fixed[0] = 1
+    parts.enabled[1] = 0
+    runs = []
+    for mode in ("read", "take"):
+        b = Batch()
+        sid = b.add_scene(sc.params, parts, sc.dt)
+        other = b.add_scene(sc.params, sc.particles, sc.dt)  # a neighbour that stays
+        b.run({sid: 8, other: 8})
+        if mode == "read":
+            got = b.particles(sid)
+        else:
+            fields = ("position", "velocity", "affine", "deformation", "mass", "material")
+            arrays = b.take(sid, fields)
+            with pytest.raises(TesseraError) as e:
+                b.read(sid, ("position",))  # gone
+            assert e.value.status == TMPM_ERR_INVALID_INPUT
+            got = parts.copy()
+            for f in fields:
+                getattr(got, f)[:] = arrays[f]
+            assert np.array_equal(arrays["mass"], parts.mass) and np.array_equal(arrays["material"], parts.material)
+        runs.append(got)
+        assert np.all(np.isfinite(b.particles(other).position))  # the neighbour is intact
+        b.close()
+    read, took = runs
+    assert_close(read, took, pos=1e-6, vel=1e-5, F=1e-5, C=1e-4, what="take vs read")
+    for arr in (took, read):
+        assert np.array_equal(arr.position[0], parts.position[0])  # fixed: stays
+        assert np.all(arr.velocity[0] == 0.0) and np.all(arr.affine[0] == 0.0)
+        assert np.array_equal(arr.position[1], parts.position[1])  # disabled: untouched
+        assert np.array_equal(arr.velocity[1], parts.velocity[1])
