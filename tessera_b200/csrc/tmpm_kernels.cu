@@ -278,9 +278,10 @@ __global__ void __launch_bounds__(THREADS, MINB)
     k.color = 0;
     if (valid) {
         x = mk(P.x[i], P.x[cap + i], P.x[2 * cap + i]);
-        F = load_m3(P.F, cap, i);
         cw = P.cls[i];
-        k = classes[cw & kClassMask];
+        // the namespace and kind now; the whole record after the gather (below)
+        k.color = classes[cw & kClassMask].color;
+        k.kind = classes[cw & kClassMask].kind;
     }
     const int scene = MULTI ? static_cast<int>(k.color >> kSceneShift) : 0;
     const SceneParams *const scn = sp.scenes + scene;
@@ -310,6 +311,10 @@ __global__ void __launch_bounds__(THREADS, MINB)
     if (threadIdx.x == 0) s_gbox.ok = 0;
 
     if (MODE == kModeP2G) {
+        if (valid) {
+            F = load_m3(P.F, cap, i);
+            k = classes[cw & kClassMask];
+        }
         if (p2g_on) {
             v = mk(P.v[i], P.v[cap + i], P.v[2 * cap + i]);
             Cm = load_m3(P.C, cap, i);
@@ -457,6 +462,12 @@ __global__ void __launch_bounds__(THREADS, MINB)
             }
         }
 
+        // F is read only now: it is not needed during the gather, whose
+        // accumulators and weights are the kernel's peak register demand
+        if (valid) {
+            F = load_m3(P.F, cap, i);
+            k = classes[cw & kClassMask];
+        }
         if (g2p_on && !fixed) {
             // Particle update (gpu.wgsl:885-1003; world.rs:443-463).
             if (sp.apply_force) {
