@@ -200,9 +200,9 @@ def shape_summary(info: dict) -> dict:
     k = info["shape"]
     out = {"tuned": k is not None}
     if k is not None:
-        out["particles_per_cta"], out["ctas_per_sm"] = info["shapes"][k]
-    out["ns_per_particle_substep"] = {f"{t}x{b}": (None if c is None else c * 1e6)
-                                      for (t, b), c in zip(info["shapes"], info["ms_per_particle_substep"])}
+        out["particles_per_cta"], out["ctas_per_sm"], out["block_edge"] = info["shapes"][k]
+    out["ns_per_particle_substep"] = {f"{t}x{b}/{e}^3": (None if c is None else c * 1e6)
+                                      for (t, b, e), c in zip(info["shapes"], info["ms_per_particle_substep"])}
     return out
 
 
@@ -236,7 +236,7 @@ def bench_batched(count: int) -> dict:
     e2e_batched = time.perf_counter() - t0
     assert all(np.all(np.isfinite(o["position"])) for o in outs)
     # the launch-shape tuner reads its trials (the first six batches) before the timed batches
-    for _ in range(8):
+    for _ in range(16):
         if b.launch_shape()["shape"] is not None:
             break
         b.run({i: steps for i in ids})
@@ -385,7 +385,7 @@ def run_tessera(args, world, rank, local):
 
     # the launch-shape tuner's trials (two 64-substep segments per shape) come
     # before the warm-up, so every timed segment runs the chosen shape
-    for _ in range(8):
+    for _ in range(16):
         if session.launch_shape()["shape"] is not None:
             break
         session.bench_substeps(BATCH)

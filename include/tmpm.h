@@ -428,17 +428,21 @@ TmpmStatus tmpm_bench_substeps(TmpmSession *session, uint32_t steps, double *ms,
                                double *kernel_ms, size_t kernel_count);
 
 /* ---------------- launch-shape tuning (no reference counterpart) ----------------
- * The transfer kernels (G2P, P2G and the fused G2P2G) are built for several
- * launch shapes: particles per CTA and CTAs resident per SM.  Unless the
- * options fix one, a session or batch runs its first submitted segments under
- * each shape in turn (two rounds, real work; results differ between shapes
- * only by f32 summation order) and keeps the one with the least device time per
- * particle-substep, as CUDA events on its stream measured it.  Plastic
- * materials and CPIC run shape 0 only. */
+ * The transfer kernels (G2P, P2G and the fused G2P2G) and the grid update are
+ * built for several launch shapes: particles per CTA, CTAs resident per SM,
+ * and the edge of the sparse grid's blocks (4 or 8 cells).  Unless the options
+ * fix one, a session or batch runs its first submitted segments under each
+ * shape in turn (two rounds, real work; results differ between shapes only by
+ * f32 summation order) and keeps the one with the least device time per
+ * particle-substep, as CUDA events on its stream measured it.  8-cell blocks
+ * are tried when the block pool holds the scene in them at most twice the
+ * 4-cell pool's size (dense scenes).  Plastic materials and CPIC run shape 0
+ * only. */
 
-/* Shape `shape` (0 ..< count): particles per CTA and CTAs per SM. */
+/* Shape `shape` (0 ..< count): particles per CTA, CTAs per SM, block edge in cells. */
 uint32_t tmpm_launch_shape_count(void);
-TmpmStatus tmpm_launch_shape_info(uint32_t shape, uint32_t *threads_per_cta, uint32_t *ctas_per_sm);
+TmpmStatus tmpm_launch_shape_info(uint32_t shape, uint32_t *threads_per_cta, uint32_t *ctas_per_sm,
+                                  uint32_t *block_edge);
 
 /* The shape in use: -1 while trials are outstanding, else its index.  When
  * `ms_per_unit` is non-NULL, it receives (up to `count` entries) the best

@@ -147,7 +147,7 @@ def lib():
     L.tmpm_batch_last_error_message.restype = C.c_char_p
     L.tmpm_launch_shape_count.argtypes = []
     L.tmpm_launch_shape_count.restype = U32
-    L.tmpm_launch_shape_info.argtypes = [U32, C.POINTER(U32), C.POINTER(U32)]
+    L.tmpm_launch_shape_info.argtypes = [U32, C.POINTER(U32), C.POINTER(U32), C.POINTER(U32)]
     L.tmpm_launch_shape_info.restype = S
     L.tmpm_session_launch_shape.argtypes = [P, P, C.c_size_t]
     L.tmpm_session_launch_shape.restype = C.c_int32
@@ -161,15 +161,15 @@ def version() -> str:
     return lib().tmpm_version().decode()
 
 
-def launch_shapes() -> list[tuple[int, int]]:
-    """(particles per CTA, CTAs per SM) of each transfer launch shape, by index."""
+def launch_shapes() -> list[tuple[int, int, int]]:
+    """(particles per CTA, CTAs per SM, grid block edge in cells) of each launch shape, by index."""
     L = lib()
     out = []
     for k in range(int(L.tmpm_launch_shape_count())):
-        t, b = C.c_uint32(0), C.c_uint32(0)
-        if L.tmpm_launch_shape_info(k, C.byref(t), C.byref(b)) != 0:
+        t, b, e = C.c_uint32(0), C.c_uint32(0), C.c_uint32(0)
+        if L.tmpm_launch_shape_info(k, C.byref(t), C.byref(b), C.byref(e)) != 0:
             raise RuntimeError(f"launch shape {k}: {L.tmpm_last_error().decode()}")
-        out.append((int(t.value), int(b.value)))
+        out.append((int(t.value), int(b.value), int(e.value)))
     return out
 
 

@@ -65,7 +65,8 @@ struct TmpmPreparedScene {
     ClassTable classes;     // local classes (namespace 0)
     HostRows rows;          // packed rows, class ids local
     size_t m = 0;           // enabled particles (device rows)
-    size_t blocks = 0;      // occupied home blocks
+    size_t blocks = 0;      // occupied 4^3 home blocks
+    size_t blocks8 = 0;     // occupied 8^3 home blocks
 };
 
 namespace {
@@ -122,6 +123,7 @@ TmpmStatus prepare_scene(const TmpmParams &params, const TmpmParticleArrays *par
     p.dt = dt;
     p.m = pr.enabled;
     p.blocks = pr.blocks.size();
+    p.blocks8 = big_home_blocks(pr.blocks);
     return TMPM_OK;
 }
 
@@ -135,7 +137,8 @@ struct BatchScene {
     uint64_t substeps = 0;   // substeps completed on the device
     size_t dev_offset = 0;   // first device row
     size_t dev_count = 0;    // enabled particles (device rows)
-    size_t blocks = 0;       // occupied home blocks at admission (pool sizing)
+    size_t blocks = 0;       // occupied 4^3 home blocks at admission (pool sizing)
+    size_t blocks8 = 0;      // occupied 8^3 home blocks at admission
     uint32_t queued = 0;     // substeps in the batch in flight
     std::unique_ptr<TmpmPreparedScene> staged;  // admitted, rows not yet on the device
     size_t prev_offset = 0;  // first row in the buffer the batch in flight reads
@@ -187,7 +190,8 @@ struct TmpmBatch {
     uint64_t epoch = 1;  // bumps whenever a device pointer a graph holds changes
     bool pending = false;
     double last_ms = 0.0;
-    LaunchTuner tuner;  // transfer launch shape (tuned on the first batches unless fixed)
+    LaunchTuner tuner;  // transfer launch configuration (tuned on the first batches unless fixed)
+    bool big_blocks_ok = false;  // the node pools hold the live scenes in 8^3 blocks too
 
     struct GraphKey {
         uint32_t steps;
@@ -254,6 +258,8 @@ struct TmpmBatch {
         sp.apply_force = 0;
         sp.resident_checks = 1;
         sp.has_plastic = classes.plastic() ? 1 : 0;
+        sp.shape = 0;
+        sp.block_shift = kBlockShift;
         return sp;
     }
 
@@ -261,6 +267,12 @@ struct TmpmBatch {
         size_t b = 0;
         for (const BatchScene &s : scenes)
             if (s.live || s.draining) b += s.blocks;
+        return b;
+    }
+    size_t total_blocks8() const {
+        size_t b = 0;
+        for (const BatchScene &s : scenes)
+            if (s.live || s.draining) b += s.blocks8;
         return b;
     }
 
@@ -318,14 +330,16 @@ struct TmpmBatch {
     }
 
     TmpmStatus ensure_grid() {
-        uint64_t want = options.max_blocks ? options.max_blocks : 16 * total_blocks() + 4096;
-        if (want > (1u << 27)) want = 1u << 27;
-        if (grids[0].max_blocks >= want) return TMPM_OK;
-        if (!options.max_blocks) want = want + want / 4;  // grow with slack: admissions come one by one
-        if (want > (1u << 27)) want = 1u << 27;
+        const PoolPlan need = pool_plan(total_blocks(), total_blocks8(), options.max_blocks);
+        big_blocks_ok = need.big;
+        if (grids[0].max_blocks >= need.blocks && grids[0].pool_nodes >= need.nodes) return TMPM_OK;
+        // grow with slack: admissions come one by one
+        const PoolPlan grow = pool_plan(total_blocks(), total_blocks8(), options.max_blocks, 1);
+        const size_t nodes = std::max(grow.nodes, need.nodes);
         cudaError_t e;
         for (int g = 0; g < 2; ++g)
-            if ((e = grids[g].alloc(static_cast<uint32_t>(want)))) return cuda_fail(e, "cudaMalloc grid");
+            if ((e = grids[g].alloc(static_cast<uint32_t>(std::max(grow.blocks, need.blocks)), nodes)))
+                return cuda_fail(e, "cudaMalloc grid");
         ++epoch;
         return TMPM_OK;
     }
@@ -535,18 +549,20 @@ struct TmpmBatch {
     }
 
     // The kernels of one batch of `steps` substeps (captured into a graph or launched directly).
-    void launch_batch(uint32_t steps, int shape) {
+    void launch_batch(uint32_t steps, int config) {
         SimParams sp = sim_params();
-        sp.shape = shape;
+        sp.shape = config_shape(config);
+        const int bs = config_block_shift(config);
+        sp.block_shift = bs;
         ParticleSoA src = pbuf[cur].view(nullptr, 1), dst = pbuf[cur ^ 1].view(nullptr, 1);
         SortBuffers sb = sort_buffers();
         launch_resort(src, dst, static_cast<int>(n_phys), static_cast<int>(n_live), dclasses.ptr, sp, sb, stream);
         GridTable g[2];
-        g[0] = grids[0].view();
+        g[0] = grids[0].view(bs);
         g[1] = g[0];
         g[1].pool = grids[1].pool.ptr;
         const int n = static_cast<int>(n_live);
-        launch_clear_table(g[0], stream);
+        launch_clear_table(g[0], g[1], bs, stream);
         SimParams sp0 = sp;
         sp0.step_index = -1;
         launch_transfer(kModeP2G, dst, n, dclasses.ptr, g[1], g[0], sp0, nullptr, nullptr, nullptr, status.ptr,
@@ -573,17 +589,17 @@ struct TmpmBatch {
         if (n_phys > 0) {
             // Plastic classes run the default shape only.
             const bool tunable = !classes.plastic();
-            const int shape = tunable ? tuner.shape() : 0;
+            const int config = tunable ? tuner.config(big_blocks_ok) : 0;
             const double work = static_cast<double>(n_live) * steps;
             if (options.use_graphs) {
-                GraphKey key{steps, n_phys, n_live, cur, epoch, shape};
+                GraphKey key{steps, n_phys, n_live, cur, epoch, config};
                 auto it = graphs.find(key);
                 if (it == graphs.end()) {
                     if (graphs.size() > 16) drop_graphs();
                     cudaGraph_t graph = nullptr;
                     if ((e = cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal)))
                         return cuda_fail(e, "cudaStreamBeginCapture");
-                    launch_batch(steps, shape);
+                    launch_batch(steps, config);
                     if ((e = cudaStreamEndCapture(stream, &graph))) return cuda_fail(e, "cudaStreamEndCapture");
                     cudaGraphExec_t exec = nullptr;
                     e = cudaGraphInstantiate(&exec, graph, 0);
@@ -591,11 +607,11 @@ struct TmpmBatch {
                     if (e) return cuda_fail(e, "cudaGraphInstantiate");
                     it = graphs.emplace(key, exec).first;
                 }
-                if (tunable) tuner.begin(shape, stream);
+                if (tunable) tuner.begin(config, stream);
                 if ((e = cudaGraphLaunch(it->second, stream))) return cuda_fail(e, "cudaGraphLaunch");
             } else {
-                if (tunable) tuner.begin(shape, stream);
-                launch_batch(steps, shape);
+                if (tunable) tuner.begin(config, stream);
+                launch_batch(steps, config);
             }
             if (tunable) tuner.end(work, stream);
             cur ^= 1;
@@ -810,6 +826,7 @@ struct TmpmBatch {
         sc.dt = p->dt;
         sc.dev_count = p->m;
         sc.blocks = p->blocks;
+        sc.blocks8 = p->blocks8;
         sc.world = std::move(p->world);
         sc.staged = std::move(p);
         if (static_cast<size_t>(id) == scenes.size()) scenes.emplace_back();
@@ -952,7 +969,7 @@ struct TmpmBatch {
         for (int k = 0; k < 2; ++k) b += pbuf[k].cap * (27 * 4 + 2 * 4);
         b += (sort_keys[0].count + sort_keys[1].count + sort_vals[0].count + sort_vals[1].count + sort_hist.count) * 4;
         for (int g = 0; g < 2; ++g)
-            b += static_cast<size_t>(grids[g].max_blocks) * (kNodesPerBlock * 16 + 16) +
+            b += grids[g].pool_nodes * 16 + static_cast<size_t>(grids[g].max_blocks) * 16 +
                  static_cast<size_t>(grids[g].capacity) * 12;
         b += cta_cache.count * 4 + dclasses.count * sizeof(DevClass) + kMaxScenes * (sizeof(SceneParams) + 4);
         b += read_unsorted.count * 4;
@@ -981,7 +998,11 @@ void tmpm_scene_prepared_destroy(TmpmPreparedScene *p) { delete p; }
 size_t tmpm_scene_prepared_particle_count(const TmpmPreparedScene *p) { return p ? p->world.n : 0; }
 
 size_t tmpm_scene_prepared_bytes(const TmpmPreparedScene *p) {
-    return p ? p->m * kBytesPerRow + 16 * p->blocks * kBytesPerPoolBlock : 0;
+    if (!p) return 0;
+    // the pool share as pool_plan sizes it: 4^3 blocks, or 8^3 when they fit in twice the nodes
+    const size_t nodes4 = 16 * p->blocks * kNodesPerBlock, nodes8 = 16 * p->blocks8 * kBigNodesPerBlock;
+    const size_t extra = nodes8 <= 2 * nodes4 && nodes8 > nodes4 ? 2 * (nodes8 - nodes4) * 16 : 0;
+    return p->m * kBytesPerRow + 16 * p->blocks * kBytesPerPoolBlock + extra;
 }
 
 TmpmStatus tmpm_batch_create(const TmpmBatchOptions *options, TmpmBatch **out) {
@@ -1151,6 +1172,7 @@ int32_t tmpm_batch_launch_shape(TmpmBatch *b, double *ms_per_unit, size_t count)
     }
     if (ms_per_unit) b->tuner.costs(ms_per_unit, static_cast<uint32_t>(count));
     if (b->classes.plastic()) return 0;  // variants built for the default shape only
+    if (b->tuner.chosen >= 0 && !b->big_blocks_ok) return b->tuner.config(false);  // 8^3 without room: best 4^3
     return b->tuner.chosen;
 }
 

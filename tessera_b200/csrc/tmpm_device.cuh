@@ -631,8 +631,10 @@ __device__ __forceinline__ uint32_t morton_block(int bx, int by, int bz, uint32_
            (spread10(static_cast<uint32_t>(by) & 0x7Fu) << 1) | spread10(static_cast<uint32_t>(bz) & 0x7Fu);
 }
 
-// Find the block id of `key`, allocating (and zero-filling) the block if absent.
-// The allocating thread zeroes the block's 64 nodes and records its
+// Find the block id of `key`, allocating the block if absent.  Ids grow from
+// zero after each table clear and both node pools are zeroed with it, so a
+// new block's nodes are zero already (the grid update zeroes the blocks in use
+// for their next accumulation).  The allocating thread records the block's
 // coordinates before publishing the id with a release store; other threads
 // that find the key wait (bounded) for the id with acquire loads.  Returns -1
 // and sets a status bit on exhaustion or timeout.
@@ -651,10 +653,6 @@ __device__ inline int find_or_insert_block(const GridTable &g, unsigned long lon
                     vref.store(kInvalidId, cuda::memory_order_release);
                     return -1;
                 }
-                float4 *blk = g.pool + static_cast<size_t>(id) * kNodesPerBlock;
-                const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
-#pragma unroll 8
-                for (int i = 0; i < kNodesPerBlock; ++i) blk[i] = z;
                 g.coords[id] = coord;
                 vref.store(id, cuda::memory_order_release);
                 return static_cast<int>(id);

@@ -524,24 +524,30 @@ struct ParticleBuffers {
     }
 };
 
+// Hash table, block coordinates and node pool of one grid.  `max_blocks` counts
+// 4^3 blocks; the pool holds `pool_nodes` nodes, at least max_blocks x 64, so
+// a view for 8^3 blocks has pool_nodes / 512 blocks.
 struct GridBuffers {
     DevBuf<unsigned long long> keys;
     DevBuf<uint32_t> vals, count;
     DevBuf<float4> pool;
     DevBuf<int4> coords;
     uint32_t capacity = 0, max_blocks = 0;
-    cudaError_t alloc(uint32_t blocks) {
+    size_t pool_nodes = 0;
+    cudaError_t alloc(uint32_t blocks, size_t nodes = 0) {
+        nodes = std::max(nodes, static_cast<size_t>(blocks) * kNodesPerBlock);
         uint32_t cap = 1024;
         while (cap < 2u * blocks) cap <<= 1;
         cudaError_t e;
-        if ((e = keys.alloc(cap)) || (e = vals.alloc(cap)) || (e = count.alloc(1)) ||
-            (e = pool.alloc(static_cast<size_t>(blocks) * kNodesPerBlock)) || (e = coords.alloc(blocks)))
+        if ((e = keys.alloc(cap)) || (e = vals.alloc(cap)) || (e = count.alloc(1)) || (e = pool.alloc(nodes)) ||
+            (e = coords.alloc(blocks)))
             return e;
         capacity = cap;
         max_blocks = blocks;
+        pool_nodes = nodes;
         return cudaSuccess;
     }
-    GridTable view() const {
+    GridTable view(int block_shift = kBlockShift) const {
         GridTable g;
         g.keys = keys.ptr;
         g.vals = vals.ptr;
@@ -549,28 +555,75 @@ struct GridBuffers {
         g.pool = pool.ptr;
         g.coords = coords.ptr;
         g.mask = capacity - 1;
-        g.max_blocks = max_blocks;
+        g.max_blocks = static_cast<uint32_t>(std::min<size_t>(max_blocks, pool_nodes >> (3 * block_shift)));
         return g;
     }
 };
 
-// Launch-shape tuner of the transfer kernels.  The first submitted segments
-// (real work, not a rehearsal) run under each candidate shape in turn, `kRounds`
-// times each, timed with CUDA events on the submitting stream; the shape with
-// the least time per particle-substep (best of its rounds, so the first launch
-// of a kernel, which loads its module, does not count against it) is kept once
-// every trial has completed.  Nothing waits for a trial: completed events are
-// read when the next segment asks for its shape.
+// Occupied 8^3 home blocks from the sorted, distinct 4^3 home-block keys
+// (namespace << 48 | biased bx << 32 | biased by << 16 | biased bz).
+inline size_t big_home_blocks(const std::vector<unsigned long long> &blocks4) {
+    std::vector<unsigned long long> big;
+    big.reserve(blocks4.size());
+    auto halve = [](unsigned long long key, int at) {
+        const int c = static_cast<int>((key >> at) & 0xFFFFu) - kBlockBias;
+        return static_cast<unsigned long long>(static_cast<uint32_t>((c >> 1) + kBlockBias) & 0xFFFFu) << at;
+    };
+    for (unsigned long long k : blocks4)
+        big.push_back((k & 0xFFFF000000000000ull) | halve(k, 32) | halve(k, 16) | halve(k, 0));
+    std::sort(big.begin(), big.end());
+    return static_cast<size_t>(std::unique(big.begin(), big.end()) - big.begin());
+}
+
+// Block pool sizing: 16 pool blocks per occupied home block plus slack, in 4^3
+// blocks (or the caller's fixed count).  8^3 blocks are a tuner candidate when
+// the same rule for them needs at most twice the 4^3 pool's nodes (dense
+// scenes); the pool then holds the larger of the two.
+struct PoolPlan {
+    uint64_t blocks = 0;  // 4^3 blocks
+    size_t nodes = 0;
+    bool big = false;
+};
+inline PoolPlan pool_plan(size_t home4, size_t home8, uint64_t fixed_blocks, uint64_t slack_num = 0) {
+    PoolPlan p;
+    uint64_t want = fixed_blocks ? fixed_blocks : std::max<uint64_t>(4096, 16 * home4 + 4096);
+    if (!fixed_blocks) want += want * slack_num / 4;
+    want = std::min<uint64_t>(want, 1u << 27);
+    p.blocks = want;
+    p.nodes = static_cast<size_t>(want) * kNodesPerBlock;
+    if (!fixed_blocks) {
+        uint64_t big_blocks = 16 * static_cast<uint64_t>(home8) + 512;
+        big_blocks += big_blocks * slack_num / 4;
+        const size_t big_nodes = static_cast<size_t>(big_blocks) * kBigNodesPerBlock;
+        if (big_nodes <= 2 * p.nodes && big_blocks <= want) {
+            p.big = true;
+            p.nodes = std::max(p.nodes, big_nodes);
+        }
+    }
+    return p;
+}
+
+// Launch-configuration tuner of the transfer kernels (a configuration is a
+// launch shape and a grid block edge, see config_shape / config_block_shift).
+// The first submitted segments (real work, not a rehearsal) run under each
+// candidate in turn, `kRounds` times each, timed with CUDA events on the
+// submitting stream; the candidate with the least time per particle-substep
+// (best of its rounds, so the first launch of a kernel, which loads its module,
+// does not count against it) is kept once every trial has completed.  Nothing
+// waits for a trial: completed events are read when the next segment asks for
+// its configuration.  Candidates are the 4^3-block configurations, and the
+// 8^3-block ones too when the block pool can hold them (`allow_big` at the
+// first request).
 struct LaunchTuner {
     static constexpr int kRounds = 2;
-    static constexpr int kTrials = kRounds * kNumLaunchShapes;
-    int fixed = -1;   // >= 0: the caller's shape; no tuning
-    int chosen = -1;  // the tuned shape, -1 while trials are outstanding
-    int issued = 0;   // trials started
-    int read = 0;     // trials whose time has been read
-    double best[kNumLaunchShapes];
+    int fixed = -1;       // >= 0: the caller's configuration; no tuning
+    int chosen = -1;      // the tuned configuration, -1 while trials are outstanding
+    int candidates = 0;   // configurations under trial (0: not yet started)
+    int issued = 0;       // trials started
+    int read = 0;         // trials whose time has been read
+    double best[kNumLaunchConfigs];
     struct Trial {
-        int shape = 0;
+        int config = 0;
         double work = 0.0;
         cudaEvent_t a = nullptr, b = nullptr;
     };
@@ -590,15 +643,17 @@ struct LaunchTuner {
         trials.clear();
         open = -1;
     }
-    // `option`: 0 = tune, k > 0 = fixed shape k - 1 (out of range: shape 0).
+    // `option`: 0 = tune, k > 0 = fixed configuration k - 1 (out of range: 0).
     void reset(uint32_t option) {
         release();
-        fixed = option == 0 ? -1 : (option <= static_cast<uint32_t>(kNumLaunchShapes) ? static_cast<int>(option) - 1 : 0);
+        fixed = option == 0 ? -1 : (option <= static_cast<uint32_t>(kNumLaunchConfigs) ? static_cast<int>(option) - 1 : 0);
         chosen = fixed;
+        candidates = 0;
         issued = read = 0;
         for (double &b : best) b = std::numeric_limits<double>::infinity();
     }
     bool tuning() const { return chosen < 0; }
+    int trials_total() const { return kRounds * candidates; }
     void poll() {
         while (read < static_cast<int>(trials.size()) && read != open) {
             Trial &t = trials[read];
@@ -608,30 +663,42 @@ struct LaunchTuner {
             }
             float ms = 0.f;
             if (cudaEventElapsedTime(&ms, t.a, t.b) == cudaSuccess && t.work > 0)
-                best[t.shape] = std::min(best[t.shape], ms / t.work);
+                best[t.config] = std::min(best[t.config], ms / t.work);
             ++read;
         }
-        if (chosen < 0 && issued == kTrials && read == issued) {
+        if (chosen < 0 && candidates > 0 && issued == trials_total() && read == issued) {
             int s = 0;
-            for (int k = 1; k < kNumLaunchShapes; ++k)
+            for (int k = 1; k < candidates; ++k)
                 if (best[k] < best[s]) s = k;
             chosen = s;
             release();
         }
     }
-    // Shape for the next segment.
-    int shape() {
-        if (chosen >= 0) return chosen;
-        poll();
-        if (chosen >= 0) return chosen;
-        return issued < kTrials ? issued % kNumLaunchShapes : 0;
+    // Configuration for the next segment.  Without room for 8^3 blocks
+    // (`allow_big` false) an 8^3 choice falls back to the best 4^3 one.
+    int config(bool allow_big) {
+        if (candidates == 0 && fixed < 0) candidates = allow_big ? kNumLaunchConfigs : kNumLaunchShapes;
+        int c = chosen;
+        if (c < 0) {
+            poll();
+            c = chosen;
+        }
+        if (c < 0) c = issued < trials_total() ? issued % candidates : 0;
+        if (!allow_big && c >= kNumLaunchShapes) {
+            if (fixed >= 0) return config_shape(c);
+            int s = 0;
+            for (int k = 1; k < kNumLaunchShapes; ++k)
+                if (best[k] < best[s]) s = k;
+            return s;
+        }
+        return c;
     }
-    // Brackets one segment of `work` particle-substeps run under shape(); only
-    // trials are recorded.
-    void begin(int shape_used, cudaStream_t stream) {
-        if (chosen >= 0 || issued >= kTrials || shape_used != issued % kNumLaunchShapes) return;
+    // Brackets one segment of `work` particle-substeps run under config();
+    // only trials are recorded.
+    void begin(int config_used, cudaStream_t stream) {
+        if (chosen >= 0 || candidates == 0 || issued >= trials_total() || config_used != issued % candidates) return;
         Trial t;
-        t.shape = shape_used;
+        t.config = config_used;
         if (cudaEventCreate(&t.a) || cudaEventCreate(&t.b) || cudaEventRecord(t.a, stream)) {
             if (t.a) cudaEventDestroy(t.a);
             if (t.b) cudaEventDestroy(t.b);
@@ -648,9 +715,9 @@ struct LaunchTuner {
         cudaEventRecord(trials[open].b, stream);
         open = -1;
     }
-    // Measured ms per particle-substep of each shape (infinity: not measured).
+    // Measured ms per particle-substep of each configuration (infinity: not measured).
     void costs(double *out, uint32_t count) const {
-        for (uint32_t k = 0; k < count && k < static_cast<uint32_t>(kNumLaunchShapes); ++k) out[k] = best[k];
+        for (uint32_t k = 0; k < count && k < static_cast<uint32_t>(kNumLaunchConfigs); ++k) out[k] = best[k];
     }
 };
 

@@ -19,8 +19,10 @@
 
 namespace tmpm {
 
-constexpr int kBlockShift = 2;  // 4^3 cells per grid block
+constexpr int kBlockShift = 2;  // 4^3 cells per grid block (the default block edge)
 constexpr int kNodesPerBlock = 64;
+constexpr int kBigBlockShift = 3;  // 8^3 cells per grid block (a tuner candidate)
+constexpr int kBigNodesPerBlock = 512;
 constexpr unsigned long long kEmptyKey = ~0ull;
 constexpr uint32_t kPendingId = 0xFFFFFFFFu;
 constexpr uint32_t kInvalidId = 0xFFFFFFFEu;
@@ -54,6 +56,12 @@ struct LaunchShape {
 };
 constexpr LaunchShape kLaunchShapes[] = {{256, TMPM_TRANSFER_MIN_BLOCKS}, {128, 8}, {256, 3}};
 constexpr int kNumLaunchShapes = 3;
+// Launch configurations: a shape and a grid block edge.  Configuration c runs
+// shape c % kNumLaunchShapes on 4^3 blocks for c < kNumLaunchShapes, on 8^3
+// blocks above.
+constexpr int kNumLaunchConfigs = 2 * kNumLaunchShapes;
+constexpr int config_shape(int c) { return c % kNumLaunchShapes; }
+constexpr int config_block_shift(int c) { return c < kNumLaunchShapes ? kBlockShift : kBigBlockShift; }
 constexpr int kMinTransferThreads = 128;  // per-CTA records are sized for the smallest shape
 constexpr int kCacheStride = 144;      // per-CTA record: 16-int box header + up to 128 block ids
 
@@ -135,6 +143,7 @@ struct SimParams {
     int has_plastic;      // some particle class is snow, sand or NH sand
     int cpic;             // CPIC on: grid namespace = colour << 8 | side mask of the CPIC groups (< 8)
     int shape;            // transfer launch shape (index into kLaunchShapes)
+    int block_shift;      // log2 of the grid block edge: kBlockShift (4^3) or kBigBlockShift (8^3)
 };
 constexpr int kMaxCpicGroups = 8;
 
@@ -171,7 +180,9 @@ void launch_transfer(int mode, const ParticleSoA &P, int n, const DevClass *clas
 void launch_grid_update(const GridTable &g, const GridTable &next, const SimParams &sp,
                         const DevObstacle *obstacles, const float *planes, double *reactions,
                         uint32_t *status, cudaStream_t stream);
-void launch_clear_table(const GridTable &g, cudaStream_t stream);
+// Empty the hash table of `g` and zero both node pools (g's and other's) over
+// g.max_blocks blocks of edge 2^block_shift.
+void launch_clear_table(const GridTable &g, const GridTable &other, int block_shift, cudaStream_t stream);
 // Re-sort by block key into `dst`; particles of removed scenes sort last and the
 // first `keep` particles are gathered.
 void launch_resort(ParticleSoA &src, ParticleSoA &dst, int n, int keep, const DevClass *classes, const SimParams &sp,
@@ -182,7 +193,7 @@ void launch_bin_keys(const ParticleSoA &P, int n, const DevClass *classes, const
 void launch_bin_keys_values(const float *x, size_t stride, int n, float inv_h, uint32_t *keys, uint32_t *vals,
                             cudaStream_t stream);
 void launch_dump_grid(const GridTable &g, int32_t *cells, float4 *values, uint32_t *count, uint32_t capacity,
-                      cudaStream_t stream);
+                      int block_shift, cudaStream_t stream);
 void launch_snapshot(const ParticleSoA &P, int n, const DevClass *classes, float4 *out, cudaStream_t stream);
 // 27 f32 rows (x, v, C, F, plastic) of the stored particles into world order, `stride` floats per row.
 // Rows in world order: out[c * stride + widx[j]] = component c of stored row j

@@ -44,7 +44,12 @@ struct Box {
     uint32_t color;
 };
 
-__device__ __forceinline__ int node_local(int cx, int cy, int cz) { return ((cx & 3) * 4 + (cy & 3)) * 4 + (cz & 3); }
+// Node index inside its block of edge 2^BS cells (x-major).
+template <int BS>
+__device__ __forceinline__ int node_local(int cx, int cy, int cz) {
+    constexpr int m = (1 << BS) - 1;
+    return ((cx & m) << (2 * BS)) | ((cy & m) << BS) | (cz & m);
+}
 
 // Split a row-major tile index t (dims d0 x d1 x d2, t < 2^20) into (tx, ty, tz)
 // without integer division: (t + 0.5) / d lies at least 1 / (2 d) from an
@@ -63,7 +68,7 @@ struct Split3 {
 };
 
 // Block-wide min/max of base cells and colours; thread 0 fills `box`.
-template <int THREADS>
+template <int THREADS, int BS>
 __device__ __forceinline__ void reduce_box(bool valid, const int b[3], uint32_t color, int (*red)[8], Box &box) {
     int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     int vals[8];
@@ -101,8 +106,8 @@ __device__ __forceinline__ void reduce_box(bool valid, const int b[3], uint32_t 
             for (int a = 0; a < 3; ++a) {
                 box.lo[a] = m[a];
                 box.dim[a] = m[3 + a] - m[a] + 3;
-                box.blo[a] = m[a] >> kBlockShift;
-                box.nb[a] = ((m[3 + a] + 2) >> kBlockShift) - box.blo[a] + 1;
+                box.blo[a] = m[a] >> BS;
+                box.nb[a] = ((m[3 + a] + 2) >> BS) - box.blo[a] + 1;
                 nodes *= box.dim[a];
                 nbt *= box.nb[a];
             }
@@ -119,7 +124,7 @@ __device__ __forceinline__ void reduce_box(bool valid, const int b[3], uint32_t 
 // Box of base cells and colours plus two float sums over the CTA, with one
 // barrier: each warp reduces its lanes and publishes a partial, then every
 // warp combines the partials itself (no second barrier, no shared result).
-template <int THREADS>
+template <int THREADS, int BS>
 __device__ __forceinline__ void reduce_box_sums(bool valid, const int b[3], uint32_t color, float &sum_a, float &sum_b,
                                                 int (*red)[8], float (*redf)[2], Box &box) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -168,8 +173,8 @@ __device__ __forceinline__ void reduce_box_sums(bool valid, const int b[3], uint
         for (int a = 0; a < 3; ++a) {
             box.lo[a] = m[a];
             box.dim[a] = m[3 + a] - m[a] + 3;
-            box.blo[a] = m[a] >> kBlockShift;
-            box.nb[a] = ((m[3 + a] + 2) >> kBlockShift) - box.blo[a] + 1;
+            box.blo[a] = m[a] >> BS;
+            box.nb[a] = ((m[3 + a] + 2) >> BS) - box.blo[a] + 1;
             nodes *= box.dim[a];
             nbt *= box.nb[a];
         }
@@ -187,9 +192,9 @@ __device__ __forceinline__ void quad_weights(float f, float w[3]) {
     w[2] = 0.5f * (f - 0.5f) * (f - 0.5f);
 }
 
+template <int BS>
 __device__ __forceinline__ int tile_block_index(const Box &bx, int cx, int cy, int cz) {
-    return (((cx >> kBlockShift) - bx.blo[0]) * bx.nb[1] + ((cy >> kBlockShift) - bx.blo[1])) * bx.nb[2] +
-           ((cz >> kBlockShift) - bx.blo[2]);
+    return (((cx >> BS) - bx.blo[0]) * bx.nb[1] + ((cy >> BS) - bx.blo[1])) * bx.nb[2] + ((cz >> BS) - bx.blo[2]);
 }
 
 __device__ __forceinline__ M3f load_m3(const float *base, size_t cap, int i) {
@@ -237,7 +242,7 @@ __device__ __forceinline__ float pow2_scale(float total) {
 // substeps its scene advances in this batch) or kCpic (one scene whose grid
 // namespace includes CPIC side masks).  Each costs registers only where used.
 enum Variant { kPlain = 0, kMulti = 1, kCpic = 2 };
-template <int MODE, bool PLASTIC, int VARIANT, int THREADS, int MINB>
+template <int MODE, bool PLASTIC, int VARIANT, int THREADS, int MINB, int BS>
 __global__ void __launch_bounds__(THREADS, MINB)
     k_transfer(ParticleSoA P, int n, const DevClass *__restrict__ classes, GridTable cur, GridTable next,
                SimParams sp, const DevObstacle *__restrict__ obstacles, const float *__restrict__ planes,
@@ -347,7 +352,7 @@ __global__ void __launch_bounds__(THREADS, MINB)
                 bx.nbt = cc[15];
                 bx.ok = 1;
             } else {
-                reduce_box<THREADS>(g2p_on, b, ns, s_red, s_box);
+                reduce_box<THREADS, BS>(g2p_on, b, ns, s_red, s_box);
                 bx = s_box;
                 if (bx.ok) {
                     const Split3 split(bx.nb[1], bx.nb[2]);
@@ -368,11 +373,11 @@ __global__ void __launch_bounds__(THREADS, MINB)
                     int tx, ty, tz;
                     split(t, tx, ty, tz);
                     int cx = bx.lo[0] + tx, cy = bx.lo[1] + ty, cz = bx.lo[2] + tz;
-                    int tb = tile_block_index(bx, cx, cy, cz);
+                    int tb = tile_block_index<BS>(bx, cx, cy, cz);
                     int id = use_cache ? cc[kCacheHeader + tb] : s_blk[tb];
                     if (use_cache) s_blk[tb] = id;
                     float4 val = make_float4(0.f, 0.f, 0.f, 0.f);
-                    if (id >= 0) val = __ldcg(cur.pool + static_cast<size_t>(id) * kNodesPerBlock + node_local(cx, cy, cz));
+                    if (id >= 0) val = __ldcg(cur.pool + static_cast<size_t>(id) * (1 << (3 * BS)) + node_local<BS>(cx, cy, cz));
                     s_gv[t] = val;
                 }
             }
@@ -444,14 +449,14 @@ __global__ void __launch_bounds__(THREADS, MINB)
                         for (int e = 0; e < 3; ++e) {
                             int cx = b[0] + a, cy = b[1] + c, cz = b[2] + e;
                             unsigned long long key =
-                                block_key(cx >> kBlockShift, cy >> kBlockShift, cz >> kBlockShift, ns);
+                                block_key(cx >> BS, cy >> BS, cz >> BS, ns);
                             if (key != last_key) {
                                 last_key = key;
                                 last_id = lookup_block(cur, key);
                             }
                             float4 val = make_float4(0.f, 0.f, 0.f, 0.f);
                             if (last_id >= 0)
-                                val = __ldcg(cur.pool + static_cast<size_t>(last_id) * kNodesPerBlock + node_local(cx, cy, cz));
+                                val = __ldcg(cur.pool + static_cast<size_t>(last_id) * (1 << (3 * BS)) + node_local<BS>(cx, cy, cz));
                             const float w = wx[a] * wy[c] * wz[e];
                             const V3f nv = mk(val.x, val.y, val.z);
                             vel = vel + nv * w;
@@ -572,8 +577,8 @@ __global__ void __launch_bounds__(THREADS, MINB)
     // ----------------------------------------------------------------- P2G
     const int b[3] = {base_cell(x.x, inv_h), base_cell(x.y, inv_h), base_cell(x.z, inv_h)};
     const bool in_range =
-        block_representable(b[0] >> kBlockShift, b[1] >> kBlockShift, b[2] >> kBlockShift) &&
-        block_representable((b[0] + 2) >> kBlockShift, (b[1] + 2) >> kBlockShift, (b[2] + 2) >> kBlockShift);
+        block_representable(b[0] >> BS, b[1] >> BS, b[2] >> BS) &&
+        block_representable((b[0] + 2) >> BS, (b[1] + 2) >> BS, (b[2] + 2) >> BS);
     const bool active = p2g_on && in_range;
     if (p2g_on && !in_range) {
         if (sp.resident_checks) atomicOr(resident_flag, kStatusResident);
@@ -605,7 +610,7 @@ __global__ void __launch_bounds__(THREADS, MINB)
     if (MODE != kModeP2G && CPIC) ns = particle_namespace(k.color, 1, sp.num_obstacles, obstacles, x);
     float tot_m = bound_m, tot_p = bound_p;
     Box bx;
-    reduce_box_sums<THREADS>(active, b, ns, tot_m, tot_p, s_red, s_fred, bx);
+    reduce_box_sums<THREADS, BS>(active, b, ns, tot_m, tot_p, s_red, s_fred, bx);
     if (MODE == kModeP2G && s_abort) return;
     if (bx.ok) {
         // every warp has finished its gather (barrier above): the buffer becomes the scatter tile
@@ -661,9 +666,9 @@ __global__ void __launch_bounds__(THREADS, MINB)
                 }
             }
             // mark the (at most 8) blocks this particle's stencil touches
-            const int bx0 = (b[0] >> kBlockShift) - bx.blo[0], bx1 = ((b[0] + 2) >> kBlockShift) - bx.blo[0];
-            const int by0 = (b[1] >> kBlockShift) - bx.blo[1], by1 = ((b[1] + 2) >> kBlockShift) - bx.blo[1];
-            const int bz0 = (b[2] >> kBlockShift) - bx.blo[2], bz1 = ((b[2] + 2) >> kBlockShift) - bx.blo[2];
+            const int bx0 = (b[0] >> BS) - bx.blo[0], bx1 = ((b[0] + 2) >> BS) - bx.blo[0];
+            const int by0 = (b[1] >> BS) - bx.blo[1], by1 = ((b[1] + 2) >> BS) - bx.blo[1];
+            const int bz0 = (b[2] >> BS) - bx.blo[2], bz1 = ((b[2] + 2) >> BS) - bx.blo[2];
             s_used[(bx0 * bx.nb[1] + by0) * bx.nb[2] + bz0] = 1;
             s_used[(bx0 * bx.nb[1] + by0) * bx.nb[2] + bz1] = 1;
             s_used[(bx0 * bx.nb[1] + by1) * bx.nb[2] + bz0] = 1;
@@ -721,9 +726,9 @@ __global__ void __launch_bounds__(THREADS, MINB)
             int tx, ty, tz;
             split_n(t, tx, ty, tz);
             int cx = bx.lo[0] + tx, cy = bx.lo[1] + ty, cz = bx.lo[2] + tz;
-            int id = s_blk2[tile_block_index(bx, cx, cy, cz)];
+            int id = s_blk2[tile_block_index<BS>(bx, cx, cy, cz)];
             if (id < 0) continue;
-            atomicAdd(next.pool + static_cast<size_t>(id) * kNodesPerBlock + node_local(cx, cy, cz),
+            atomicAdd(next.pool + static_cast<size_t>(id) * (1 << (3 * BS)) + node_local<BS>(cx, cy, cz),
                       make_float4(static_cast<float>(m) * inv_sm, static_cast<float>(px) * inv_sp,
                                   static_cast<float>(py) * inv_sp, static_cast<float>(pz) * inv_sp));
         }
@@ -736,7 +741,7 @@ __global__ void __launch_bounds__(THREADS, MINB)
                 for (int c = 0; c < 3; ++c)
                     for (int e = 0; e < 3; ++e) {
                         int cx = b[0] + a, cy = b[1] + c, cz = b[2] + e;
-                        int gx = cx >> kBlockShift, gy = cy >> kBlockShift, gz = cz >> kBlockShift;
+                        int gx = cx >> BS, gy = cy >> BS, gz = cz >> BS;
                         unsigned long long key = block_key(gx, gy, gz, ns);
                         if (key != last_key) {
                             last_key = key;
@@ -746,7 +751,7 @@ __global__ void __launch_bounds__(THREADS, MINB)
                         float w = wx[a] * wy[c] * wz[e];
                         V3f dpos = mk((a - fx.x) * h, (c - fx.y) * h, (e - fx.z) * h);
                         V3f mom = (mv + mul(A, dpos)) * w;
-                        atomicAdd(next.pool + static_cast<size_t>(last_id) * kNodesPerBlock + node_local(cx, cy, cz),
+                        atomicAdd(next.pool + static_cast<size_t>(last_id) * (1 << (3 * BS)) + node_local<BS>(cx, cy, cz),
                                   make_float4(w * k.mass, mom.x, mom.y, mom.z));
                     }
         }
@@ -756,8 +761,8 @@ __global__ void __launch_bounds__(THREADS, MINB)
 
 // Grid update over all allocated blocks; also zeroes those blocks in the other pool.
 // MULTI: each block takes its scene's parameters from the scene table
-// (scene = block namespace >> kSceneShift).
-template <bool MULTI>
+// (scene = block namespace >> kSceneShift).  Blocks have edge 2^BS cells.
+template <bool MULTI, int BS>
 __global__ void __launch_bounds__(256) k_grid(GridTable g, GridTable nxt, SimParams sp,
                                                const DevObstacle *__restrict__ obstacles,
                                                const float *__restrict__ planes, double *reactions, uint32_t *status) {
@@ -768,7 +773,8 @@ __global__ void __launch_bounds__(256) k_grid(GridTable g, GridTable nxt, SimPar
     const size_t gtid = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     const size_t stride = static_cast<size_t>(gridDim.x) * blockDim.x;
     uint32_t nblocks = min(*g.count, g.max_blocks);
-    const size_t nodes = static_cast<size_t>(nblocks) * kNodesPerBlock;
+    constexpr int kM = (1 << BS) - 1;
+    const size_t nodes = static_cast<size_t>(nblocks) << (3 * BS);
     float4 *next_pool = nxt.pool;
     for (size_t node = gtid; node < nodes; node += stride) {
         float4 mp = g.pool[node];
@@ -778,9 +784,9 @@ __global__ void __launch_bounds__(256) k_grid(GridTable g, GridTable nxt, SimPar
             g.pool[node] = make_float4(0.f, 0.f, 0.f, 0.f);
             continue;
         }
-        int4 c = g.coords[node >> 6];
-        int l = static_cast<int>(node & 63);
-        int cx = c.x * 4 + (l >> 4), cy = c.y * 4 + ((l >> 2) & 3), cz = c.z * 4 + (l & 3);
+        int4 c = g.coords[node >> (3 * BS)];
+        int l = static_cast<int>(node) & ((1 << (3 * BS)) - 1);
+        int cx = (c.x << BS) + (l >> (2 * BS)), cy = (c.y << BS) + ((l >> BS) & kM), cz = (c.z << BS) + (l & kM);
         const SceneParams *const scn = sp.scenes + (MULTI ? (static_cast<uint32_t>(c.w) >> kSceneShift) : 0u);
 #define SCN(f) (MULTI ? scn->f : sp.s0.f)
         const float h = SCN(h), dt = SCN(dt);
@@ -918,20 +924,22 @@ __global__ void k_unsort(ParticleSoA P, int n, float *__restrict__ out, size_t s
     if (nonfinite && !finite) atomicOr(nonfinite, 1u);
 }
 
+template <int BS>
 __global__ void k_dump_grid(GridTable g, int32_t *cells, float4 *values, uint32_t *count, uint32_t capacity) {
     uint32_t nblocks = min(*g.count, g.max_blocks);
-    size_t nodes = static_cast<size_t>(nblocks) * kNodesPerBlock;
+    constexpr int kM = (1 << BS) - 1;
+    size_t nodes = static_cast<size_t>(nblocks) << (3 * BS);
     for (size_t node = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x; node < nodes;
          node += static_cast<size_t>(gridDim.x) * blockDim.x) {
         float4 mp = g.pool[node];
         if (mp.x == 0.0f) continue;
         uint32_t slot = atomicAdd(count, 1u);
         if (slot >= capacity) continue;
-        int4 c = g.coords[node >> 6];
-        int l = static_cast<int>(node & 63);
-        cells[3 * slot] = c.x * 4 + (l >> 4);
-        cells[3 * slot + 1] = c.y * 4 + ((l >> 2) & 3);
-        cells[3 * slot + 2] = c.z * 4 + (l & 3);
+        int4 c = g.coords[node >> (3 * BS)];
+        int l = static_cast<int>(node) & ((1 << (3 * BS)) - 1);
+        cells[3 * slot] = (c.x << BS) + (l >> (2 * BS));
+        cells[3 * slot + 1] = (c.y << BS) + ((l >> BS) & kM);
+        cells[3 * slot + 2] = (c.z << BS) + (l & kM);
         values[slot] = mp;
     }
 }
@@ -962,28 +970,35 @@ void launch_transfer(int mode, const ParticleSoA &P, int n, const DevClass *clas
     // Launch shapes other than the default exist for the variants the tuner
     // picks among (no plastic state; one scene or a batch).
     const bool pl = sp.has_plastic != 0;
+    // plastic and CPIC variants: default shape and 4^3 blocks only
     const int shape = (pl || sp.cpic) ? 0 : sp.shape;
-#define TMPM_LAUNCH(M, PL, V, T, B) \
-    k_transfer<M, PL, V, T, B><<<dim3((n + (T) - 1) / (T)), T, 0, stream>>>(P, n, classes, cur, next, sp, obstacles, \
-                                                                           planes, reactions, status, cache)
-#define TMPM_LAUNCH_SHAPES(M, V)                                      \
-    do {                                                              \
-        if (shape == 1) TMPM_LAUNCH(M, false, V, 128, 8);             \
-        else if (shape == 2) TMPM_LAUNCH(M, false, V, 256, 3);        \
-        else TMPM_LAUNCH(M, false, V, 256, TMPM_TRANSFER_MIN_BLOCKS); \
+    const bool big = !(pl || sp.cpic) && sp.block_shift == kBigBlockShift;
+#define TMPM_LAUNCH(M, PL, V, T, B, BS) \
+    k_transfer<M, PL, V, T, B, BS><<<dim3((n + (T) - 1) / (T)), T, 0, stream>>>(P, n, classes, cur, next, sp, \
+                                                                               obstacles, planes, reactions, status, cache)
+#define TMPM_LAUNCH_SHAPES_BS(M, V, BS)                                   \
+    do {                                                                  \
+        if (shape == 1) TMPM_LAUNCH(M, false, V, 128, 8, BS);             \
+        else if (shape == 2) TMPM_LAUNCH(M, false, V, 256, 3, BS);        \
+        else TMPM_LAUNCH(M, false, V, 256, TMPM_TRANSFER_MIN_BLOCKS, BS); \
     } while (0)
-#define TMPM_LAUNCH_MODE(M)                                                      \
-    do {                                                                         \
-        if (sp.multi) {                                                          \
-            if (pl) TMPM_LAUNCH(M, true, kMulti, 256, TMPM_TRANSFER_MIN_BLOCKS); \
-            else TMPM_LAUNCH_SHAPES(M, kMulti);                                  \
-        } else if (sp.cpic) {                                                    \
-            if (pl) TMPM_LAUNCH(M, true, kCpic, 256, TMPM_TRANSFER_MIN_BLOCKS);  \
-            else TMPM_LAUNCH(M, false, kCpic, 256, TMPM_TRANSFER_MIN_BLOCKS);    \
-        } else {                                                                 \
-            if (pl) TMPM_LAUNCH(M, true, kPlain, 256, TMPM_TRANSFER_MIN_BLOCKS); \
-            else TMPM_LAUNCH_SHAPES(M, kPlain);                                  \
-        }                                                                        \
+#define TMPM_LAUNCH_SHAPES(M, V)                                \
+    do {                                                        \
+        if (big) TMPM_LAUNCH_SHAPES_BS(M, V, kBigBlockShift);   \
+        else TMPM_LAUNCH_SHAPES_BS(M, V, kBlockShift);          \
+    } while (0)
+#define TMPM_LAUNCH_MODE(M)                                                                   \
+    do {                                                                                      \
+        if (sp.multi) {                                                                       \
+            if (pl) TMPM_LAUNCH(M, true, kMulti, 256, TMPM_TRANSFER_MIN_BLOCKS, kBlockShift); \
+            else TMPM_LAUNCH_SHAPES(M, kMulti);                                               \
+        } else if (sp.cpic) {                                                                 \
+            if (pl) TMPM_LAUNCH(M, true, kCpic, 256, TMPM_TRANSFER_MIN_BLOCKS, kBlockShift);  \
+            else TMPM_LAUNCH(M, false, kCpic, 256, TMPM_TRANSFER_MIN_BLOCKS, kBlockShift);    \
+        } else {                                                                              \
+            if (pl) TMPM_LAUNCH(M, true, kPlain, 256, TMPM_TRANSFER_MIN_BLOCKS, kBlockShift); \
+            else TMPM_LAUNCH_SHAPES(M, kPlain);                                               \
+        }                                                                                     \
     } while (0)
     switch (mode) {
     case kModeP2G: TMPM_LAUNCH_MODE(kModeP2G); break;
@@ -992,19 +1007,29 @@ void launch_transfer(int mode, const ParticleSoA &P, int n, const DevClass *clas
     }
 #undef TMPM_LAUNCH_MODE
 #undef TMPM_LAUNCH_SHAPES
+#undef TMPM_LAUNCH_SHAPES_BS
 #undef TMPM_LAUNCH
 }
 
 void launch_grid_update(const GridTable &g, const GridTable &next, const SimParams &sp, const DevObstacle *obstacles,
                         const float *planes, double *reactions, uint32_t *status, cudaStream_t stream) {
     int blocks = device_sm_count() * 8;
-    if (sp.multi) k_grid<true><<<blocks, 256, 0, stream>>>(g, next, sp, obstacles, planes, reactions, status);
-    else k_grid<false><<<blocks, 256, 0, stream>>>(g, next, sp, obstacles, planes, reactions, status);
+    if (sp.block_shift == kBigBlockShift) {
+        if (sp.multi) k_grid<true, kBigBlockShift><<<blocks, 256, 0, stream>>>(g, next, sp, obstacles, planes, reactions, status);
+        else k_grid<false, kBigBlockShift><<<blocks, 256, 0, stream>>>(g, next, sp, obstacles, planes, reactions, status);
+    } else {
+        if (sp.multi) k_grid<true, kBlockShift><<<blocks, 256, 0, stream>>>(g, next, sp, obstacles, planes, reactions, status);
+        else k_grid<false, kBlockShift><<<blocks, 256, 0, stream>>>(g, next, sp, obstacles, planes, reactions, status);
+    }
 }
 
-void launch_clear_table(const GridTable &g, cudaStream_t stream) {
+void launch_clear_table(const GridTable &g, const GridTable &other, int block_shift, cudaStream_t stream) {
     int blocks = device_sm_count() * 4;
     k_clear_table<<<blocks, 256, 0, stream>>>(g);
+    // new block ids start from zero again: both pools start zero-filled
+    const size_t bytes = (static_cast<size_t>(g.max_blocks) << (3 * block_shift)) * sizeof(float4);
+    cudaMemsetAsync(g.pool, 0, bytes, stream);
+    if (other.pool != g.pool) cudaMemsetAsync(other.pool, 0, bytes, stream);
 }
 
 void launch_bin_keys(const ParticleSoA &P, int n, const DevClass *classes, const SimParams &sp, int32_t *cells,
@@ -1032,8 +1057,11 @@ void launch_resort(ParticleSoA &src, ParticleSoA &dst, int n, int keep, const De
 }
 
 void launch_dump_grid(const GridTable &g, int32_t *cells, float4 *values, uint32_t *count, uint32_t capacity,
-                      cudaStream_t stream) {
-    k_dump_grid<<<device_sm_count() * 4, 256, 0, stream>>>(g, cells, values, count, capacity);
+                      int block_shift, cudaStream_t stream) {
+    if (block_shift == kBigBlockShift)
+        k_dump_grid<kBigBlockShift><<<device_sm_count() * 4, 256, 0, stream>>>(g, cells, values, count, capacity);
+    else
+        k_dump_grid<kBlockShift><<<device_sm_count() * 4, 256, 0, stream>>>(g, cells, values, count, capacity);
 }
 
 void launch_unsort(const ParticleSoA &P, int n, float *out, size_t stride, cudaStream_t stream, uint32_t *nonfinite) {

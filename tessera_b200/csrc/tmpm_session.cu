@@ -67,8 +67,9 @@ struct TmpmSession {
     bool force_dirty = false;
     bool has_plastic = false;  // class table holds a snow, sand or NH sand class
     uint64_t since_resort = 0;
-    LaunchTuner tuner;       // transfer launch shape (tuned on the first segments unless fixed)
+    LaunchTuner tuner;       // transfer launch configuration (tuned on the first segments unless fixed)
     int stored_shape = -1;   // launch shape whose per-CTA interleave the device rows hold
+    bool big_blocks_ok = false;  // the node pools hold the scene in 8^3 blocks too
 
     ~TmpmSession() {
         if (stream) {
@@ -102,6 +103,8 @@ struct TmpmSession {
         sp.resident_checks = resident ? 1 : 0;
         sp.has_plastic = has_plastic ? 1 : 0;
         sp.cpic = cpic_active() ? 1 : 0;
+        sp.shape = 0;
+        sp.block_shift = kBlockShift;
         return sp;
     }
 
@@ -214,9 +217,8 @@ struct TmpmSession {
         cudaError_t e;
         if ((e = cudaSetDevice(device))) return cuda_fail(e, "cudaSetDevice");
         // block pool sizing from the number of occupied home blocks
-        size_t unique_blocks = pr.blocks.size();
-        uint64_t want_blocks = options.max_blocks ? options.max_blocks : std::max<uint64_t>(4096, 16 * unique_blocks + 4096);
-        if (want_blocks > (1u << 27)) want_blocks = 1u << 27;
+        const PoolPlan plan = pool_plan(pr.blocks.size(), big_home_blocks(pr.blocks), options.max_blocks);
+        big_blocks_ok = plan.big;
         for (int b = 0; b < 2; ++b)
             if (pbuf[b].cap != cap)
                 if ((e = pbuf[b].alloc(cap))) return cuda_fail(e, "cudaMalloc particles");
@@ -229,8 +231,8 @@ struct TmpmSession {
         }
         if (force_dirty) cudaMemsetAsync(force.ptr, 0, sizeof(float) * force.count, stream);
         for (int g = 0; g < 2; ++g)
-            if (grids[g].max_blocks != want_blocks)
-                if ((e = grids[g].alloc(static_cast<uint32_t>(want_blocks)))) return cuda_fail(e, "cudaMalloc grid");
+            if (grids[g].max_blocks != plan.blocks || grids[g].pool_nodes != plan.nodes)
+                if ((e = grids[g].alloc(static_cast<uint32_t>(plan.blocks), plan.nodes))) return cuda_fail(e, "cudaMalloc grid");
         size_t sort_cap = pbuf[0].cap;
         size_t tiles = (sort_cap + 4095) / 4096;
         if (sort_keys[0].count < sort_cap) {
@@ -296,8 +298,8 @@ struct TmpmSession {
 
     // Grid views for one batch: both share grids[0]'s hash table and block
     // metadata (ids stay stable for the whole batch); they differ in the pool.
-    void grid_views(GridTable g[2]) const {
-        g[0] = grids[0].view();
+    void grid_views(GridTable g[2], int block_shift) const {
+        g[0] = grids[0].view(block_shift);
         g[1] = g[0];
         g[1].pool = grids[1].pool.ptr;
     }
@@ -335,8 +337,10 @@ struct TmpmSession {
         // Plastic and CPIC variants run the default shape only.
         const bool tunable = !has_plastic && !sp.cpic;
         while (done < steps) {
-        const int shape = tunable ? tuner.shape() : 0;
+        const int config = tunable ? tuner.config(big_blocks_ok) : 0;
+        const int shape = config_shape(config), bs = config_block_shift(config);
         sp.shape = shape;
+        sp.block_shift = bs;
         // the rows are re-sorted (and re-interleaved) when the shape changes
         const bool resort_now = since_resort >= interval || shape != stored_shape;
         const uint32_t seg = std::min<uint32_t>(steps - done, resort_now ? interval : interval - since_resort);
@@ -358,12 +362,12 @@ struct TmpmSession {
             stored_shape = shape;
             tock(4);
         }
-        if (tunable) tuner.begin(shape, stream);
+        if (tunable) tuner.begin(config, stream);
         GridTable g[2];
-        grid_views(g);
+        grid_views(g, bs);
         ParticleSoA P = soa();
         tick(0);
-        launch_clear_table(g[0], stream);
+        launch_clear_table(g[0], g[1], bs, stream);
         launch_transfer(kModeP2G, P, n_dev, classes.ptr, g[1], g[0], sp, dev_obstacles.ptr, dev_planes.ptr,
                         reactions.ptr, status.ptr, cta_cache.ptr, stream);
         tock(0);
@@ -848,10 +852,10 @@ TmpmStatus tmpm_debug_p2g(TmpmSession *s, int32_t *cells_out, float *mm_out, siz
     cudaSetDevice(s->device);
     SimParams sp = s->sim_params(s->substep_dt, true);
     GridTable gv[2];
-    s->grid_views(gv);
+    s->grid_views(gv, kBlockShift);
     GridTable g0 = gv[0], g1 = gv[1];
     cudaMemsetAsync(s->status.ptr, 0, sizeof(uint32_t), s->stream);
-    launch_clear_table(g0, s->stream);
+    launch_clear_table(g0, g1, kBlockShift, s->stream);
     launch_transfer(kModeP2G, s->soa(), s->n_dev, s->classes.ptr, g1, g0, sp, s->dev_obstacles.ptr, s->dev_planes.ptr,
                     s->reactions.ptr, s->status.ptr, s->cta_cache.ptr, s->stream);
     DevBuf<int32_t> cells;
@@ -861,7 +865,7 @@ TmpmStatus tmpm_debug_p2g(TmpmSession *s, int32_t *cells_out, float *mm_out, siz
     cudaError_t e;
     if ((e = cells.alloc(3 * cap)) || (e = vals.alloc(cap)) || (e = cnt.alloc(1))) return s->cuda_fail(e, "cudaMalloc");
     cudaMemsetAsync(cnt.ptr, 0, sizeof(uint32_t), s->stream);
-    launch_dump_grid(g0, cells.ptr, vals.ptr, cnt.ptr, static_cast<uint32_t>(cap), s->stream);
+    launch_dump_grid(g0, cells.ptr, vals.ptr, cnt.ptr, static_cast<uint32_t>(cap), kBlockShift, s->stream);
     uint32_t total = 0, stw = 0;
     cudaMemcpyAsync(&total, cnt.ptr, sizeof(uint32_t), cudaMemcpyDeviceToHost, s->stream);
     cudaMemcpyAsync(&stw, s->status.ptr, sizeof(uint32_t), cudaMemcpyDeviceToHost, s->stream);
@@ -908,15 +912,18 @@ TmpmStatus tmpm_bench_substeps(TmpmSession *s, uint32_t steps, double *ms, doubl
 
 }  // extern "C"
 
-uint32_t tmpm_launch_shape_count(void) { return static_cast<uint32_t>(kNumLaunchShapes); }
+uint32_t tmpm_launch_shape_count(void) { return static_cast<uint32_t>(kNumLaunchConfigs); }
 
-TmpmStatus tmpm_launch_shape_info(uint32_t shape, uint32_t *threads_per_cta, uint32_t *ctas_per_sm) {
-    if (shape >= static_cast<uint32_t>(kNumLaunchShapes)) {
+TmpmStatus tmpm_launch_shape_info(uint32_t shape, uint32_t *threads_per_cta, uint32_t *ctas_per_sm,
+                                  uint32_t *block_edge) {
+    if (shape >= static_cast<uint32_t>(kNumLaunchConfigs)) {
         g_last_error = "launch shape out of range";
         return TMPM_ERR_INVALID_INPUT;
     }
-    if (threads_per_cta) *threads_per_cta = static_cast<uint32_t>(kLaunchShapes[shape].threads);
-    if (ctas_per_sm) *ctas_per_sm = static_cast<uint32_t>(kLaunchShapes[shape].min_blocks);
+    const int c = static_cast<int>(shape);
+    if (threads_per_cta) *threads_per_cta = static_cast<uint32_t>(kLaunchShapes[config_shape(c)].threads);
+    if (ctas_per_sm) *ctas_per_sm = static_cast<uint32_t>(kLaunchShapes[config_shape(c)].min_blocks);
+    if (block_edge) *block_edge = 1u << config_block_shift(c);
     return TMPM_OK;
 }
 
@@ -928,5 +935,6 @@ int32_t tmpm_session_launch_shape(TmpmSession *s, double *ms_per_unit, size_t co
     }
     if (ms_per_unit) s->tuner.costs(ms_per_unit, static_cast<uint32_t>(count));
     if (s->has_plastic || s->cpic_active()) return 0;  // variants built for the default shape only
+    if (s->tuner.chosen >= 0 && !s->big_blocks_ok) return s->tuner.config(false);  // 8^3 without room: best 4^3
     return s->tuner.chosen;
 }

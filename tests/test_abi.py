@@ -55,12 +55,14 @@ def test_launch_shapes_are_listed_without_a_device():
     from tessera_b200 import _native
 
     shapes = _native.launch_shapes()
-    assert shapes[0] == (256, 4)  # the default shape: 256 particles per CTA, 4 CTAs per SM
-    assert len(shapes) == 3 and len(set(shapes)) == 3
-    for threads, ctas in shapes:
+    assert shapes[0] == (256, 4, 4)  # the default: 256 particles per CTA, 4 CTAs per SM, 4^3-cell blocks
+    assert len(shapes) == 6 and len(set(shapes)) == 6
+    for threads, ctas, edge in shapes:
         assert threads % 32 == 0 and threads * ctas <= 2048  # whole warps; within an SM's thread slots
+        assert edge in (4, 8)
+    assert [s[:2] for s in shapes[:3]] == [s[:2] for s in shapes[3:]]  # each CTA shape with both block edges
     t = C.c_uint32(0)
-    assert _native.lib().tmpm_launch_shape_info(len(shapes), C.byref(t), None) != 0
+    assert _native.lib().tmpm_launch_shape_info(len(shapes), C.byref(t), None, None) != 0
 
 
 def _one_particle(material=MAT_ELASTIC, params=(2000.0, 0.2)):
