@@ -589,7 +589,7 @@ struct TmpmBatch {
         if (n_phys > 0) {
             // Plastic classes run the default shape only.
             const bool tunable = !classes.plastic();
-            const int config = tunable ? tuner.config(big_blocks_ok) : 0;
+            const int config = tunable ? tuner.config(big_blocks_ok, true) : 0;
             const double work = static_cast<double>(n_live) * steps;
             if (options.use_graphs) {
                 GraphKey key{steps, n_phys, n_live, cur, epoch, config};
@@ -1172,7 +1172,7 @@ int32_t tmpm_batch_launch_shape(TmpmBatch *b, double *ms_per_unit, size_t count)
     }
     if (ms_per_unit) b->tuner.costs(ms_per_unit, static_cast<uint32_t>(count));
     if (b->classes.plastic()) return 0;  // variants built for the default shape only
-    if (b->tuner.chosen >= 0 && !b->big_blocks_ok) return b->tuner.config(false);  // 8^3 without room: best 4^3
+    if (b->tuner.chosen >= 0 && !b->big_blocks_ok) return b->tuner.config(false, true);  // 8^3 without room: best 4^3
     return b->tuner.chosen;
 }
 

@@ -606,12 +606,14 @@ inline PoolPlan pool_plan(size_t home4, size_t home8, uint64_t fixed_blocks, uin
 // Launch-configuration tuner of the transfer kernels (a configuration is a
 // launch shape and a grid block edge, see config_shape / config_block_shift).
 // The first submitted segments (real work, not a rehearsal) run under each
-// candidate in turn, `kRounds` times each, timed with CUDA events on the
-// submitting stream; the candidate with the least time per particle-substep
-// (best of its rounds, so the first launch of a kernel, which loads its module,
-// does not count against it) is kept once every trial has completed.  Nothing
-// waits for a trial: completed events are read when the next segment asks for
-// its configuration.  Candidates are the 4^3-block configurations, and the
+// candidate in turn, timed with CUDA events on the submitting stream: one
+// round in order and one in reverse order, so that a workload that gets
+// slower or faster as the scene evolves weighs on every candidate alike, and
+// the candidate with the least mean time per particle-substep is kept once
+// every trial has completed.  The candidates' kernels are loaded before the
+// first trial, so none pays a lazy module load.  Nothing waits for a trial:
+// completed events are read when the next segment asks for its
+// configuration.  Candidates are the 4^3-block configurations, and the
 // 8^3-block ones too when the block pool can hold them (`allow_big` at the
 // first request).
 struct LaunchTuner {
@@ -621,7 +623,8 @@ struct LaunchTuner {
     int candidates = 0;   // configurations under trial (0: not yet started)
     int issued = 0;       // trials started
     int read = 0;         // trials whose time has been read
-    double best[kNumLaunchConfigs];
+    double best[kNumLaunchConfigs];  // mean ms per particle-substep of the trials read
+    int rounds_read[kNumLaunchConfigs];
     struct Trial {
         int config = 0;
         double work = 0.0;
@@ -651,6 +654,12 @@ struct LaunchTuner {
         candidates = 0;
         issued = read = 0;
         for (double &b : best) b = std::numeric_limits<double>::infinity();
+        for (int &r : rounds_read) r = 0;
+    }
+    // Candidate of trial t: rounds alternate forward and reverse order.
+    int trial_config(int t) const {
+        const int pos = t % candidates;
+        return (t / candidates) % 2 == 0 ? pos : candidates - 1 - pos;
     }
     bool tuning() const { return chosen < 0; }
     int trials_total() const { return kRounds * candidates; }
@@ -662,8 +671,10 @@ struct LaunchTuner {
                 return;
             }
             float ms = 0.f;
-            if (cudaEventElapsedTime(&ms, t.a, t.b) == cudaSuccess && t.work > 0)
-                best[t.config] = std::min(best[t.config], ms / t.work);
+            if (cudaEventElapsedTime(&ms, t.a, t.b) == cudaSuccess && t.work > 0) {
+                const int c = t.config, r = rounds_read[c]++;
+                best[c] = r == 0 ? ms / t.work : (best[c] * r + ms / t.work) / (r + 1);
+            }
             ++read;
         }
         if (chosen < 0 && candidates > 0 && issued == trials_total() && read == issued) {
@@ -676,14 +687,17 @@ struct LaunchTuner {
     }
     // Configuration for the next segment.  Without room for 8^3 blocks
     // (`allow_big` false) an 8^3 choice falls back to the best 4^3 one.
-    int config(bool allow_big) {
-        if (candidates == 0 && fixed < 0) candidates = allow_big ? kNumLaunchConfigs : kNumLaunchShapes;
+    int config(bool allow_big, bool multi) {
+        if (candidates == 0 && fixed < 0) {
+            candidates = allow_big ? kNumLaunchConfigs : kNumLaunchShapes;
+            preload_launch_shapes(multi);
+        }
         int c = chosen;
         if (c < 0) {
             poll();
             c = chosen;
         }
-        if (c < 0) c = issued < trials_total() ? issued % candidates : 0;
+        if (c < 0) c = issued < trials_total() ? trial_config(issued) : 0;
         if (!allow_big && c >= kNumLaunchShapes) {
             if (fixed >= 0) return config_shape(c);
             int s = 0;
@@ -696,7 +710,7 @@ struct LaunchTuner {
     // Brackets one segment of `work` particle-substeps run under config();
     // only trials are recorded.
     void begin(int config_used, cudaStream_t stream) {
-        if (chosen >= 0 || candidates == 0 || issued >= trials_total() || config_used != issued % candidates) return;
+        if (chosen >= 0 || candidates == 0 || issued >= trials_total() || config_used != trial_config(issued)) return;
         Trial t;
         t.config = config_used;
         if (cudaEventCreate(&t.a) || cudaEventCreate(&t.b) || cudaEventRecord(t.a, stream)) {

@@ -180,6 +180,11 @@ void launch_transfer(int mode, const ParticleSoA &P, int n, const DevClass *clas
 void launch_grid_update(const GridTable &g, const GridTable &next, const SimParams &sp,
                         const DevObstacle *obstacles, const float *planes, double *reactions,
                         uint32_t *status, cudaStream_t stream);
+// Load the kernels of every tuner candidate (transfer modes x launch shapes x
+// block edges, grid update) for the single-scene or the multi-scene variant,
+// so that no trial pays a kernel's lazy module load.
+void preload_launch_shapes(bool multi);
+
 // Empty the hash table of `g` and zero both node pools (g's and other's) over
 // g.max_blocks blocks of edge 2^block_shift.
 void launch_clear_table(const GridTable &g, const GridTable &other, int block_shift, cudaStream_t stream);

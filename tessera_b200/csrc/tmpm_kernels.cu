@@ -1023,6 +1023,39 @@ void launch_grid_update(const GridTable &g, const GridTable &next, const SimPara
     }
 }
 
+namespace {
+template <int M, int V, int T, int B, int BS>
+void touch_transfer() {
+    cudaFuncAttributes a;
+    cudaFuncGetAttributes(&a, k_transfer<M, false, V, T, B, BS>);
+}
+template <int V, int BS>
+void touch_shapes() {
+    touch_transfer<kModeP2G, V, 256, TMPM_TRANSFER_MIN_BLOCKS, BS>();
+    touch_transfer<kModeG2P2G, V, 256, TMPM_TRANSFER_MIN_BLOCKS, BS>();
+    touch_transfer<kModeG2P, V, 256, TMPM_TRANSFER_MIN_BLOCKS, BS>();
+    touch_transfer<kModeP2G, V, 128, 8, BS>();
+    touch_transfer<kModeG2P2G, V, 128, 8, BS>();
+    touch_transfer<kModeG2P, V, 128, 8, BS>();
+    touch_transfer<kModeP2G, V, 256, 3, BS>();
+    touch_transfer<kModeG2P2G, V, 256, 3, BS>();
+    touch_transfer<kModeG2P, V, 256, 3, BS>();
+    cudaFuncAttributes a;
+    cudaFuncGetAttributes(&a, k_grid<V == kMulti, BS>);
+}
+}  // namespace
+
+void preload_launch_shapes(bool multi) {
+    if (multi) {
+        touch_shapes<kMulti, kBlockShift>();
+        touch_shapes<kMulti, kBigBlockShift>();
+    } else {
+        touch_shapes<kPlain, kBlockShift>();
+        touch_shapes<kPlain, kBigBlockShift>();
+    }
+    cudaGetLastError();
+}
+
 void launch_clear_table(const GridTable &g, const GridTable &other, int block_shift, cudaStream_t stream) {
     int blocks = device_sm_count() * 4;
     k_clear_table<<<blocks, 256, 0, stream>>>(g);

@@ -337,7 +337,7 @@ struct TmpmSession {
         // Plastic and CPIC variants run the default shape only.
         const bool tunable = !has_plastic && !sp.cpic;
         while (done < steps) {
-        const int config = tunable ? tuner.config(big_blocks_ok) : 0;
+        const int config = tunable ? tuner.config(big_blocks_ok, false) : 0;
         const int shape = config_shape(config), bs = config_block_shift(config);
         sp.shape = shape;
         sp.block_shift = bs;
@@ -935,6 +935,6 @@ int32_t tmpm_session_launch_shape(TmpmSession *s, double *ms_per_unit, size_t co
     }
     if (ms_per_unit) s->tuner.costs(ms_per_unit, static_cast<uint32_t>(count));
     if (s->has_plastic || s->cpic_active()) return 0;  // variants built for the default shape only
-    if (s->tuner.chosen >= 0 && !s->big_blocks_ok) return s->tuner.config(false);  // 8^3 without room: best 4^3
+    if (s->tuner.chosen >= 0 && !s->big_blocks_ok) return s->tuner.config(false, false);  // 8^3 without room: best 4^3
     return s->tuner.chosen;
 }
