@@ -66,6 +66,8 @@ def parse():
     ap.add_argument("--serve-rates", default="200", help="comma-separated arrival rates (requests/s)")
     ap.add_argument("--serve-requests", type=int, default=12)
     ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--launch-shape", type=int, default=None,
+                    help="fix the single-scene launch shape (index of _native.launch_shapes()) instead of tuning it")
     ap.add_argument("--only", choices=["batched", "serving", "adjoint"],
                     help="run one section alone and print its result (profiling; not the benchmark line)")
     return ap.parse_args()
@@ -378,7 +380,7 @@ def run_tessera(args, world, rank, local):
     torch.cuda.set_device(local)
     sc = scenes.dam_break(seed=2 + rank, scale=args.scale)
     n = sc.particles.count
-    session = Session(sc.params, sc.particles, sc.dt, device=local)
+    session = Session(sc.params, sc.particles, sc.dt, device=local, launch_shape=args.launch_shape)
     # active grid nodes G (nodes with mass after P2G) for the algorithmic bytes
     _, mm = session.debug_p2g()
     grid_nodes = int(mm.shape[0])
