@@ -229,6 +229,48 @@ TmpmStatus tmpm_set_substep_dt(TmpmSession *session, double substep_dt);
  * of total duration dt; each substep validated and synchronized. */
 TmpmStatus tmpm_step_cfl(TmpmSession *session, double dt);
 
+/* ---------------- two-way rigid coupling, MPM-owned ----------------
+ * GpuRigidMpmCoupler (crates/tessera-mpm/src/gpu_rigid_sync.rs:62-500) in its
+ * MPM-owned form (submit_mpm_owned_step / step_mpm_owned, gpu_rigid_sync.rs:
+ * 187-214): rigid bodies live on the device beside the session; each coupled
+ * substep sets every mapped obstacle's pose and velocity from its body
+ * (gpu_rigid_sync.wgsl:46-61), runs one MPM substep accumulating the
+ * per-obstacle impulses, and applies them to the bodies: velocity and
+ * angular velocity, then gravity, an optional speed limit and the pose
+ * integration (gpu_rigid_reaction.wgsl:71-150).  The rigid solver itself
+ * (contacts, joints, sleep) belongs to tessera-physics and is not here.  The
+ * session's host obstacle list keeps the poses it was given. */
+typedef struct TmpmRigidBody {
+    double position[3];
+    double inverse_mass;       /* <= 0: not moved by impulses */
+    double orientation[4];     /* unit quaternion x, y, z, w */
+    double linear_velocity[3];
+    double angular_velocity[3];
+    double inverse_inertia[3]; /* body-frame principal inverse inertia */
+} TmpmRigidBody;
+
+typedef struct TmpmRigidMapping {
+    int32_t body;              /* body index, or -1: the obstacle keeps its pose */
+    int32_t reserved;
+    double local_center[3];    /* obstacle centre in the body frame */
+    double local_orientation[4];
+} TmpmRigidMapping;
+
+/* GpuRigidMpmCoupler::new (gpu_rigid_sync.rs:230-343): bodies and one mapping
+ * per session obstacle, in obstacle order.  Replaces an earlier attachment. */
+TmpmStatus tmpm_rigid_attach(TmpmSession *session, const TmpmRigidBody *bodies, size_t body_count,
+                             const TmpmRigidMapping *mappings, size_t mapping_count);
+/* `substeps` (1..64) coupled substeps of the session's substep, then a
+ * synchronize (step_mpm_owned, gpu_rigid_sync.rs:202-214, for each substep).
+ * gravity: the rigid bodies' gravity; max_linear_speed <= 0: no limit.
+ * Needs no pending steps; not with CPIC obstacles (their side masks would use
+ * the pose of the substep before). */
+TmpmStatus tmpm_rigid_step(TmpmSession *session, uint32_t substeps, const double gravity[3],
+                           double max_linear_speed);
+/* The bodies' current state. */
+TmpmStatus tmpm_rigid_read(TmpmSession *session, TmpmRigidBody *bodies, size_t body_count);
+void tmpm_rigid_detach(TmpmSession *session);
+
 /* MpmWorld::step_with_gpu_obstacle_reactions (gpu.rs:2247-2293): as
  * tmpm_step_cfl, also returning per-obstacle impulses, 6 doubles each
  * (linear xyz, angular xyz about the obstacle centre), in obstacle order. */

@@ -316,3 +316,103 @@ def storage_order(perm: np.ndarray, chunk: int = 256, group: int = 8) -> np.ndar
     kk = np.arange(full) % chunk
     src[:full] = (np.arange(full) // chunk) * chunk + (kk % 32) * group + kk // 32
     return perm[src]
+
+
+# -------------------------------------------------------- rigid coupling (f64)
+# Restatement of the MPM-owned two-way rigid coupling: obstacle pose from its
+# body (crates/tessera-mpm/src/gpu_rigid_sync.wgsl:46-61) and obstacle impulses
+# applied to the bodies (gpu_rigid_reaction.wgsl:71-150), in f64.  Bodies are
+# dicts with numpy arrays: position, inverse_mass, orientation (x, y, z, w),
+# linear_velocity, angular_velocity, inverse_inertia (body frame).  Mappings
+# are (body, local_center, local_orientation) with body -1 for a fixed obstacle.
+
+def quat_rotate(q, v):
+    """v rotated by the unit quaternion q (gpu_rigid_sync.wgsl:32-35)."""
+    q = np.asarray(q, dtype=np.float64)
+    v = np.asarray(v, dtype=np.float64)
+    t = 2.0 * np.cross(q[:3], v)
+    return v + q[3] * t + np.cross(q[:3], t)
+
+
+def quat_mul(a, b):
+    """Hamilton product (gpu_rigid_sync.wgsl:37-42)."""
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    v = a[3] * b[:3] + b[3] * a[:3] + np.cross(a[:3], b[:3])
+    return np.array([v[0], v[1], v[2], a[3] * b[3] - np.dot(a[:3], b[:3])])
+
+
+def quat_from_rotation(r):
+    """Rotation by vector r; first order below 1e-5 rad (gpu_rigid_reaction.wgsl:62-69)."""
+    r = np.asarray(r, dtype=np.float64)
+    angle = float(np.linalg.norm(r))
+    if angle < 1e-5:
+        q = np.array([0.5 * r[0], 0.5 * r[1], 0.5 * r[2], 1.0])
+        return q / np.linalg.norm(q)
+    s = np.sin(0.5 * angle) / angle
+    return np.array([r[0] * s, r[1] * s, r[2] * s, np.cos(0.5 * angle)])
+
+
+def rigid_sync(bodies, mappings, obstacles):
+    """Obstacles with the pose and velocity of their bodies (gpu_rigid_sync.wgsl:46-61)."""
+    import dataclasses
+
+    out = []
+    for (body, local_center, local_q), o in zip(mappings, obstacles):
+        if body < 0:
+            out.append(o)
+            continue
+        b = bodies[body]
+        offset = quat_rotate(b["orientation"], local_center)
+        center = b["position"] + offset
+        out.append(dataclasses.replace(
+            o, center=tuple(center), orientation=tuple(quat_mul(b["orientation"], local_q)),
+            linear_velocity=tuple(b["linear_velocity"] + np.cross(b["angular_velocity"], offset)),
+            angular_velocity=tuple(b["angular_velocity"])))
+    return out
+
+
+def rigid_apply(bodies, mappings, obstacles, reactions, dt, gravity=(0.0, 0.0, 0.0), max_speed=0.0,
+                integrate_pose=True):
+    """Bodies after the obstacle impulses of one substep (gpu_rigid_reaction.wgsl:71-150):
+    reactions[i] = (linear impulse, angular impulse about obstacle i's centre)."""
+    out = []
+    for bi, b in enumerate(bodies):
+        b = {k: (np.array(v, dtype=np.float64) if not np.isscalar(v) else v) for k, v in b.items()}
+        if b["inverse_mass"] <= 0.0:
+            out.append(b)
+            continue
+        lin = np.zeros(3)
+        ang = np.zeros(3)
+        mapped = False
+        for oi, (body, _, _) in enumerate(mappings):
+            if body != bi:
+                continue
+            mapped = True
+            imp = np.asarray(reactions[oi][:3], dtype=np.float64)
+            lin += imp
+            ang += np.asarray(reactions[oi][3:6], dtype=np.float64) + np.cross(
+                np.asarray(obstacles[oi].center) - b["position"], imp)
+        finite = np.all(np.abs(lin) < 1e30) and np.all(np.abs(ang) < 1e30)
+        if not finite or not mapped or (not lin.any() and not ang.any() and not integrate_pose):
+            out.append(b)
+            continue
+        q = b["orientation"]
+        conj = np.array([-q[0], -q[1], -q[2], q[3]])
+        dw = quat_rotate(q, quat_rotate(conj, ang) * b["inverse_inertia"])
+        v = b["linear_velocity"] + lin * b["inverse_mass"]
+        w = b["angular_velocity"] + dw
+        if integrate_pose:
+            v = v + np.asarray(gravity, dtype=np.float64) * dt
+        if max_speed > 0.0:
+            speed = float(np.linalg.norm(v))
+            if speed > max_speed:
+                v = v * (max_speed / speed)
+        b["linear_velocity"] = v
+        b["angular_velocity"] = w
+        if integrate_pose:
+            b["position"] = b["position"] + v * dt
+            nq = quat_mul(quat_from_rotation(w * dt), q)
+            b["orientation"] = nq / np.linalg.norm(nq)
+        out.append(b)
+    return out

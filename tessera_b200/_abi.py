@@ -130,6 +130,52 @@ class TmpmSessionOptions(C.Structure):
     ]
 
 
+class TmpmRigidBody(C.Structure):
+    """include/tmpm.h TmpmRigidBody: a rigid body of the two-way coupling."""
+    _fields_ = [
+        ("position", C.c_double * 3),
+        ("inverse_mass", C.c_double),
+        ("orientation", C.c_double * 4),  # x, y, z, w
+        ("linear_velocity", C.c_double * 3),
+        ("angular_velocity", C.c_double * 3),
+        ("inverse_inertia", C.c_double * 3),  # body frame, principal
+    ]
+
+    @staticmethod
+    def make(position, inverse_mass, orientation=(0.0, 0.0, 0.0, 1.0), linear_velocity=(0.0, 0.0, 0.0),
+             angular_velocity=(0.0, 0.0, 0.0), inverse_inertia=(0.0, 0.0, 0.0)) -> "TmpmRigidBody":
+        b = TmpmRigidBody()
+        b.position[:] = [float(v) for v in position]
+        b.inverse_mass = float(inverse_mass)
+        b.orientation[:] = [float(v) for v in orientation]
+        b.linear_velocity[:] = [float(v) for v in linear_velocity]
+        b.angular_velocity[:] = [float(v) for v in angular_velocity]
+        b.inverse_inertia[:] = [float(v) for v in inverse_inertia]
+        return b
+
+    def as_dict(self) -> dict:
+        return {f: (float(getattr(self, f)) if f == "inverse_mass" else np.array(getattr(self, f)[:]))
+                for f, _ in self._fields_}
+
+
+class TmpmRigidMapping(C.Structure):
+    """include/tmpm.h TmpmRigidMapping: obstacle -> body (-1: the obstacle keeps its pose)."""
+    _fields_ = [
+        ("body", C.c_int32),
+        ("reserved", C.c_int32),
+        ("local_center", C.c_double * 3),
+        ("local_orientation", C.c_double * 4),
+    ]
+
+    @staticmethod
+    def make(body, local_center=(0.0, 0.0, 0.0), local_orientation=(0.0, 0.0, 0.0, 1.0)) -> "TmpmRigidMapping":
+        m = TmpmRigidMapping()
+        m.body = int(body)
+        m.local_center[:] = [float(v) for v in local_center]
+        m.local_orientation[:] = [float(v) for v in local_orientation]
+        return m
+
+
 class TmpmBatchOptions(C.Structure):
     _fields_ = [
         ("device", C.c_int32),

@@ -10,7 +10,10 @@ import ctypes as C
 import os
 import subprocess
 
-from ._abi import TmpmBatchOptions, TmpmObstacle, TmpmParams, TmpmParticleArrays, TmpmSessionOptions
+from ._abi import (
+    TmpmBatchOptions, TmpmObstacle, TmpmParams, TmpmParticleArrays, TmpmRigidBody, TmpmRigidMapping,
+    TmpmSessionOptions,
+)
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.environ.get("TMPM_LIB_PATH") or os.path.join(_HERE, "libtmpm.so")
@@ -145,6 +148,14 @@ def lib():
     L.tmpm_adjoint_last_error_message.restype = C.c_char_p
     L.tmpm_batch_last_error_message.argtypes = [P]
     L.tmpm_batch_last_error_message.restype = C.c_char_p
+    L.tmpm_rigid_attach.argtypes = [P, C.POINTER(TmpmRigidBody), C.c_size_t, C.POINTER(TmpmRigidMapping), C.c_size_t]
+    L.tmpm_rigid_attach.restype = S
+    L.tmpm_rigid_step.argtypes = [P, C.c_uint32, C.POINTER(C.c_double), C.c_double]
+    L.tmpm_rigid_step.restype = S
+    L.tmpm_rigid_read.argtypes = [P, C.POINTER(TmpmRigidBody), C.c_size_t]
+    L.tmpm_rigid_read.restype = S
+    L.tmpm_rigid_detach.argtypes = [P]
+    L.tmpm_rigid_detach.restype = None
     L.tmpm_launch_shape_count.argtypes = []
     L.tmpm_launch_shape_count.restype = U32
     L.tmpm_launch_shape_info.argtypes = [U32, C.POINTER(U32), C.POINTER(U32), C.POINTER(U32)]

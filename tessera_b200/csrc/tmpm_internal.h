@@ -108,6 +108,34 @@ struct DevObstacle {
     float verts[12];    // a, b, c (xyz + pad)
 };
 
+// Rigid body of the two-way coupling (the reference's RigidState layout,
+// gpu_rigid_reaction.wgsl:1-7): position | inverse mass, orientation (x, y, z,
+// w), linear and angular velocity, body-frame inverse inertia | awake flag.
+struct DevRigid {
+    float4 pos_inv_mass;
+    float4 q;
+    float4 lin;
+    float4 ang;
+    float4 inv_inertia;
+};
+static_assert(sizeof(DevRigid) == 80, "DevRigid layout");
+
+// Obstacle -> body mapping (gpu_rigid_sync.wgsl:21-25): body index (< 0: the
+// obstacle keeps its pose), the obstacle's centre and orientation in the body frame.
+struct DevRigidMap {
+    int body;
+    int pad[3];
+    float4 local_center;
+    float4 local_q;
+};
+
+struct RigidParams {
+    float dt;
+    float gravity[3];
+    float max_speed;  // <= 0: no limit
+    int integrate_pose;
+};
+
 struct GridTable {
     unsigned long long *keys;  // [capacity]
     uint32_t *vals;            // [capacity]
@@ -180,6 +208,14 @@ void launch_transfer(int mode, const ParticleSoA &P, int n, const DevClass *clas
 void launch_grid_update(const GridTable &g, const GridTable &next, const SimParams &sp,
                         const DevObstacle *obstacles, const float *planes, double *reactions,
                         uint32_t *status, cudaStream_t stream);
+// Two-way rigid coupling: obstacle poses from their bodies; obstacle impulses
+// (6 doubles per obstacle) applied to the bodies.
+void launch_rigid_sync(const DevRigid *bodies, const DevRigidMap *maps, int obstacle_count, DevObstacle *obstacles,
+                       cudaStream_t stream);
+void launch_rigid_apply(DevRigid *bodies, int body_count, const DevRigidMap *maps, int obstacle_count,
+                        const DevObstacle *obstacles, const double *reactions, const RigidParams &p,
+                        cudaStream_t stream);
+
 // Load the kernels of every tuner candidate (transfer modes x launch shapes x
 // block edges, grid update) for the single-scene or the multi-scene variant,
 // so that no trial pays a kernel's lazy module load.

@@ -59,6 +59,9 @@ struct TmpmSession {
     DevBuf<float> dev_planes;
     DevBuf<uint32_t> status;
     DevBuf<double> reactions;
+    DevBuf<DevRigid> rigid_bodies;  // two-way rigid coupling (tmpm_rigid_*)
+    DevBuf<DevRigidMap> rigid_maps;
+    size_t rigid_body_count = 0, rigid_map_count = 0;
     DevBuf<int> cta_cache;  // kCacheStride ints per transfer CTA
     DevBuf<uint32_t> sort_keys[2], sort_vals[2], sort_hist, sort_totals;
     PinnedBuf staging;         // readback
@@ -937,4 +940,127 @@ int32_t tmpm_session_launch_shape(TmpmSession *s, double *ms_per_unit, size_t co
     if (s->has_plastic || s->cpic_active()) return 0;  // variants built for the default shape only
     if (s->tuner.chosen >= 0 && !s->big_blocks_ok) return s->tuner.config(false, false);  // 8^3 without room: best 4^3
     return s->tuner.chosen;
+}
+
+// ---------------------------------------------------------------- rigid coupling
+
+TmpmStatus tmpm_rigid_attach(TmpmSession *s, const TmpmRigidBody *bodies, size_t body_count,
+                             const TmpmRigidMapping *mappings, size_t mapping_count) {
+    TmpmStatus st = session_guard(s, true);
+    if (st != TMPM_OK) return st;
+    if ((body_count && !bodies) || (mapping_count && !mappings))
+        return s->fail(TMPM_ERR_INVALID_INPUT, "null rigid body or mapping array");
+    if (mapping_count != s->obstacles.size())
+        return s->fail(TMPM_ERR_INVALID_INPUT, "one rigid mapping per session obstacle is needed");
+    if (body_count > (1u << 20)) return s->fail(TMPM_ERR_CAPACITY, "too many rigid bodies");
+    std::vector<DevRigid> db(body_count);
+    for (size_t i = 0; i < body_count; ++i) {
+        const TmpmRigidBody &b = bodies[i];
+        float v[16], im = 0.f;
+        const double *src[5] = {b.position, b.orientation, b.linear_velocity, b.angular_velocity, b.inverse_inertia};
+        const int width[5] = {3, 4, 3, 3, 3};
+        bool ok = f32_ok(b.inverse_mass, im);
+        int k = 0;
+        for (int f = 0; f < 5; ++f)
+            for (int c = 0; c < width[f]; ++c) ok = ok && f32_ok(src[f][c], v[k++]);
+        const double qn = b.orientation[0] * b.orientation[0] + b.orientation[1] * b.orientation[1] +
+                          b.orientation[2] * b.orientation[2] + b.orientation[3] * b.orientation[3];
+        if (!ok || !(std::fabs(qn - 1.0) < 1e-3))
+            return s->fail(TMPM_ERR_INVALID_INPUT, "rigid body not finite in f32 or orientation not a unit quaternion");
+        db[i].pos_inv_mass = make_float4(v[0], v[1], v[2], im);
+        db[i].q = make_float4(v[3], v[4], v[5], v[6]);
+        db[i].lin = make_float4(v[7], v[8], v[9], 0.f);
+        db[i].ang = make_float4(v[10], v[11], v[12], 0.f);
+        db[i].inv_inertia = make_float4(v[13], v[14], v[15], 1.f);
+    }
+    std::vector<DevRigidMap> dm(mapping_count);
+    for (size_t i = 0; i < mapping_count; ++i) {
+        const TmpmRigidMapping &m = mappings[i];
+        if (m.body >= 0 && static_cast<size_t>(m.body) >= body_count)
+            return s->fail(TMPM_ERR_INVALID_INPUT, "rigid mapping names a body that does not exist");
+        float c[7];
+        bool ok = true;
+        for (int k = 0; k < 3; ++k) ok = ok && f32_ok(m.local_center[k], c[k]);
+        for (int k = 0; k < 4; ++k) ok = ok && f32_ok(m.local_orientation[k], c[3 + k]);
+        if (!ok) return s->fail(TMPM_ERR_INVALID_INPUT, "rigid mapping not finite in f32");
+        dm[i].body = m.body < 0 ? -1 : m.body;
+        dm[i].local_center = make_float4(c[0], c[1], c[2], 0.f);
+        dm[i].local_q = make_float4(c[3], c[4], c[5], c[6]);
+    }
+    cudaSetDevice(s->device);
+    cudaError_t e;
+    if ((e = s->rigid_bodies.alloc(std::max<size_t>(body_count, 1))) ||
+        (e = s->rigid_maps.alloc(std::max<size_t>(mapping_count, 1))))
+        return s->cuda_fail(e, "cudaMalloc rigid");
+    if ((body_count && (e = cudaMemcpy(s->rigid_bodies.ptr, db.data(), sizeof(DevRigid) * body_count,
+                                       cudaMemcpyHostToDevice))) ||
+        (mapping_count && (e = cudaMemcpy(s->rigid_maps.ptr, dm.data(), sizeof(DevRigidMap) * mapping_count,
+                                          cudaMemcpyHostToDevice))))
+        return s->cuda_fail(e, "rigid upload");
+    s->rigid_body_count = body_count;
+    s->rigid_map_count = mapping_count;
+    return TMPM_OK;
+}
+
+TmpmStatus tmpm_rigid_step(TmpmSession *s, uint32_t substeps, const double gravity[3], double max_linear_speed) {
+    TmpmStatus st = session_guard(s, true);
+    if (st != TMPM_OK) return st;
+    if (substeps == 0 || substeps > 64) return s->fail(TMPM_ERR_INVALID_INPUT, "substeps per submit must be 1..64");
+    if (s->rigid_map_count != s->obstacles.size() || (!s->rigid_body_count && s->rigid_map_count))
+        return s->fail(TMPM_ERR_INVALID_INPUT, "rigid coupling not attached for the current obstacle set");
+    if (s->cpic_active())
+        return s->fail(TMPM_ERR_RESIDENT_UNAVAILABLE, "rigid coupling with CPIC obstacles is not supported");
+    RigidParams p{};
+    bool ok = f32_ok(s->substep_dt, p.dt) && f32_ok(std::isfinite(max_linear_speed) ? max_linear_speed : -1.0, p.max_speed);
+    for (int k = 0; k < 3; ++k) ok = ok && gravity && f32_ok(gravity[k], p.gravity[k]);
+    if (!ok) return s->fail(TMPM_ERR_INVALID_INPUT, "rigid gravity or speed limit not finite in f32");
+    p.integrate_pose = 1;
+    st = s->validate_resident(s->substep_dt);
+    if (st != TMPM_OK) return st;
+    cudaSetDevice(s->device);
+    const int nobs = static_cast<int>(s->obstacles.size());
+    for (uint32_t k = 0; k < substeps; ++k) {
+        if (nobs) {
+            cudaMemsetAsync(s->reactions.ptr, 0, sizeof(double) * 6 * nobs, s->stream);
+            launch_rigid_sync(s->rigid_bodies.ptr, s->rigid_maps.ptr, nobs, s->dev_obstacles.ptr, s->stream);
+        }
+        st = s->enqueue(1, s->substep_dt, true, nobs > 0, nullptr);
+        if (st != TMPM_OK) return st;
+        launch_rigid_apply(s->rigid_bodies.ptr, static_cast<int>(s->rigid_body_count), s->rigid_maps.ptr, nobs,
+                           s->dev_obstacles.ptr, s->reactions.ptr, p, s->stream);
+        s->pending += 1;
+    }
+    cudaError_t e = cudaGetLastError();
+    if (e) return s->cuda_fail(e, "rigid coupling launch");
+    return s->synchronize();
+}
+
+TmpmStatus tmpm_rigid_read(TmpmSession *s, TmpmRigidBody *bodies, size_t body_count) {
+    if (!s || (body_count && !bodies)) return TMPM_ERR_INVALID_INPUT;
+    if (body_count != s->rigid_body_count) return s->fail(TMPM_ERR_INVALID_INPUT, "body count does not match the attachment");
+    if (!body_count) return TMPM_OK;
+    std::vector<DevRigid> db(body_count);
+    cudaSetDevice(s->device);
+    cudaError_t e;
+    if ((e = cudaStreamSynchronize(s->stream)) ||
+        (e = cudaMemcpy(db.data(), s->rigid_bodies.ptr, sizeof(DevRigid) * body_count, cudaMemcpyDeviceToHost)))
+        return s->cuda_fail(e, "rigid readback");
+    for (size_t i = 0; i < body_count; ++i) {
+        const DevRigid &d = db[i];
+        TmpmRigidBody &b = bodies[i];
+        const float4 *f[5] = {&d.pos_inv_mass, &d.q, &d.lin, &d.ang, &d.inv_inertia};
+        double *dst[5] = {b.position, b.orientation, b.linear_velocity, b.angular_velocity, b.inverse_inertia};
+        const int width[5] = {3, 4, 3, 3, 3};
+        for (int k = 0; k < 5; ++k) {
+            const float c[4] = {f[k]->x, f[k]->y, f[k]->z, f[k]->w};
+            for (int j = 0; j < width[k]; ++j) dst[k][j] = c[j];
+        }
+        b.inverse_mass = d.pos_inv_mass.w;
+    }
+    return TMPM_OK;
+}
+
+void tmpm_rigid_detach(TmpmSession *s) {
+    if (!s) return;
+    s->rigid_body_count = s->rigid_map_count = 0;
 }

@@ -186,6 +186,31 @@ class Session:
         n = min(int(count.value), capacity)
         return cells[:n], vals[:n]
 
+    # ------------------------------------------------------- rigid coupling
+    def rigid_attach(self, bodies, mappings) -> None:
+        """Rigid bodies (TmpmRigidBody) and one mapping (TmpmRigidMapping) per
+        obstacle, in obstacle order, for MPM-owned two-way coupling."""
+        from ._abi import TmpmRigidBody, TmpmRigidMapping
+
+        b = (TmpmRigidBody * max(len(bodies), 1))(*bodies)
+        m = (TmpmRigidMapping * max(len(mappings), 1))(*mappings)
+        self._rigid_count = len(bodies)
+        _check(_native.lib().tmpm_rigid_attach(self._h, b, len(bodies), m, len(mappings)), self._h)
+
+    def rigid_step(self, substeps: int, gravity=(0.0, 0.0, 0.0), max_linear_speed: float = 0.0) -> None:
+        """`substeps` coupled substeps (obstacles follow their bodies; impulses
+        move the bodies), then a synchronize."""
+        g = (C.c_double * 3)(*[float(v) for v in gravity])
+        _check(_native.lib().tmpm_rigid_step(self._h, int(substeps), g, float(max_linear_speed)), self._h)
+
+    def rigid_bodies(self) -> list:
+        from ._abi import TmpmRigidBody
+
+        n = getattr(self, "_rigid_count", 0)
+        out = (TmpmRigidBody * max(n, 1))()
+        _check(_native.lib().tmpm_rigid_read(self._h, out, n), self._h)
+        return [out[i] for i in range(n)]
+
     def launch_shape(self) -> dict:
         """Transfer launch shape in use (None while trials are outstanding) and
         the measured cost of each shape."""
