@@ -197,6 +197,40 @@ def cpu_baseline(scene_fn, target_seconds=15.0):
                       f"materials) x {substeps} substeps, {threads} independent copies in parallel, {el:.1f} s"}
 
 
+def bench_small_configs(target_seconds=5.0) -> dict:
+    """The CPU-runnable configurations beside the GPU: the corotated block of
+    configuration 1 (h = 1/64, [0.3, 0.6]^3 at 8 per cell; dt = 5e-5, since
+    1e-4 is above its CFL bound) through a single-scene session, and both it
+    and the 64k-particle block of configuration 5 through the oracle, one
+    independent copy per host core."""
+    from oracle import oracle as O
+    from tessera_b200 import scenes
+    from tessera_b200.session import Session
+
+    out = {}
+    threads = os.cpu_count() or 1
+    for name, sc in (("config1-corotated-block", scenes.elastic_block()), ("config5-corotated-block",
+                                                                         scenes.adjoint_block())):
+        n = sc.particles.count
+        entry = {"particles": n, "dt": sc.dt, "unit": METRIC}
+        ses = Session(sc.params, sc.particles, sc.dt)
+        for _ in range(3):
+            ses.bench_substeps(64)
+        ses.synchronize()
+        ms, _ = ses.bench_substeps(64 * 8)
+        ses.synchronize()
+        ses.close()
+        entry["gpu"] = n * 64 * 8 / (ms / 1e3)
+        world = O.OracleWorld(sc.params, sc.particles)
+        el = world.bench(threads, 1, sc.dt)
+        substeps = max(1, int(target_seconds / max(el, 1e-3)))
+        el = world.bench(threads, substeps, sc.dt)
+        entry["cpu"] = {"value": threads * n * substeps / el, "cores": threads, "kind": "port",
+                        "sample": f"{substeps} substeps, {threads} independent copies in parallel, {el:.1f} s"}
+        out[name] = entry
+    return out
+
+
 def shape_summary(info: dict) -> dict:
     """The tuned transfer launch shape and what each candidate measured."""
     k = info["shape"]
@@ -454,11 +488,13 @@ def run_tessera(args, world, rank, local):
                "h2d_bytes_per_step": 4 * 24 * cap + 8 * cap + 12 * n + 4,
                "d2h_bytes_per_step": 4 * 24 * n + 4 * n + 4, "seconds_per_step": e2e_s}
 
-    cpu = None
+    cpu = small = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(scenes.dam_break)
     clk = clocks.summary()
     session.close()
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        small = bench_small_configs()
     batched = serving = None
     if rank == 0 and world == 1 and not args.no_batched:
         batched = bench_batched(args.batched_scenes)
@@ -485,6 +521,7 @@ def run_tessera(args, world, rank, local):
             "batched": batched,
             "serving": serving,
             "adjoint": adjoint,
+            "small_configs": small,
         }
         print(json.dumps(line), flush=True)
 
