@@ -66,6 +66,9 @@ struct TmpmSession {
     DevBuf<uint32_t> sort_keys[2], sort_vals[2], sort_hist, sort_totals;
     PinnedBuf staging;         // readback
     DevBuf<float> unsorted;    // readback rows in world order
+    DevBuf<uint32_t> readback_flag;  // non-finite flag of a readback
+    static constexpr int kReadChunks = 8;
+    cudaEvent_t read_events[kReadChunks] = {};  // pipelined readback: copy chunk k+1 while chunk k is applied
     PinnedBuf upload_staging;  // packed f32 state for uploads
     bool force_dirty = false;
     bool has_plastic = false;  // class table holds a snow, sand or NH sand class
@@ -79,6 +82,8 @@ struct TmpmSession {
             cudaStreamSynchronize(stream);
         }
         if (done) cudaEventDestroy(done);
+        for (cudaEvent_t &ev : read_events)
+            if (ev) cudaEventDestroy(ev);
         if (stream) cudaStreamDestroy(stream);
     }
 
@@ -449,29 +454,40 @@ struct TmpmSession {
             // rows back in world order on the device, one copy, then sequential host passes
             const size_t N = world.n, floats = 27 * N;
             if (unsorted.count < floats && (e = unsorted.alloc(floats))) return cuda_fail(e, "cudaMalloc readback");
+            if (!readback_flag.count && (e = readback_flag.alloc(1))) return cuda_fail(e, "cudaMalloc readback");
             if (!staging.ensure(floats * sizeof(float))) return fail(TMPM_ERR_DEVICE, "cudaMallocHost staging failed");
+            for (cudaEvent_t &ev : read_events)
+                if (!ev && (e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming))) return cuda_fail(e, "cudaEventCreate");
             float *h = static_cast<float *>(staging.ptr);
-            launch_unsort(soa(), n, unsorted.ptr, N, stream);
-            if ((e = cudaMemcpyAsync(h, unsorted.ptr, sizeof(float) * floats, cudaMemcpyDeviceToHost, stream)) ||
+            // collect_prepared: non-finite transfers are an error before anything is
+            // applied; the un-sort kernel checks every component on the device
+            uint32_t nonfinite = 0;
+            if ((e = cudaMemsetAsync(readback_flag.ptr, 0, sizeof(uint32_t), stream))) return cuda_fail(e, "readback");
+            launch_unsort(soa(), n, unsorted.ptr, N, stream, readback_flag.ptr);
+            if ((e = cudaMemcpyAsync(&nonfinite, readback_flag.ptr, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream)) ||
                 (e = cudaStreamSynchronize(stream)))
                 return cuda_fail(e, "readback");
-            // collect_prepared: non-finite transfers are an error before anything is applied
-            std::atomic<bool> bad{false};
-            parallel_for(N, [&](size_t a, size_t b) {
-                for (size_t c = 0; c < 27 && !bad.load(std::memory_order_relaxed); ++c)
-                    for (size_t w = a; w < b; ++w)
-                        if (world.enabled[w] && !std::isfinite(h[c * N + w])) {
-                            bad = true;
-                            break;
-                        }
-            });
-            if (bad) {
+            if (nonfinite) {
                 valid = false;
                 return fail(TMPM_ERR_NON_FINITE_STATE, "MPM integration produced a non-finite state");
             }
+            // world-index chunks: the copy of chunk k + 1 runs while chunk k is applied
+            const size_t per = (N + kReadChunks - 1) / kReadChunks;
+            int chunks = 0;
+            for (size_t a = 0; a < N; a += per, ++chunks) {
+                const size_t w = std::min(per, N - a) * sizeof(float);
+                if ((e = cudaMemcpy2DAsync(h + a, N * sizeof(float), unsorted.ptr + a, N * sizeof(float), w, 27,
+                                           cudaMemcpyDeviceToHost, stream)) ||
+                    (e = cudaEventRecord(read_events[chunks], stream)))
+                    return cuda_fail(e, "readback");
+            }
             ++world.version;
-            parallel_for(N, [&](size_t a, size_t b) {
-                for (size_t w = a; w < b; ++w) {
+            for (int k = 0; k < chunks; ++k) {
+                if ((e = cudaEventSynchronize(read_events[k]))) return cuda_fail(e, "readback");
+                const size_t lo = k * per, hi = std::min(N, lo + per);
+                parallel_for(hi - lo, [&](size_t a, size_t b) {
+                for (size_t w = lo + a; w < lo + b; ++w) {
+                    for (int c = 0; c < 3; ++c) world.force[3 * w + c] = 0.0;
                     if (!world.enabled[w]) continue;
                     if (world.fixed[w]) {
                         for (int k = 0; k < 3; ++k) world.vel[3 * w + k] = 0.0;
@@ -488,9 +504,11 @@ struct TmpmSession {
                     }
                     const int mat = world.material[w];
                     if (mat == TMPM_MAT_SAND || mat == TMPM_MAT_SNOW || mat == TMPM_MAT_SAND_NEO_HOOKEAN)
-                        for (int k = 0; k < 3; ++k) world.plastic[3 * w + k] = h[(24 + k) * N + w];
+                        for (int q = 0; q < 3; ++q) world.plastic[3 * w + q] = h[(24 + q) * N + w];
                 }
-            });
+                });
+            }
+            return TMPM_OK;
         }
         std::fill(world.force.begin(), world.force.end(), 0.0);
         return TMPM_OK;
