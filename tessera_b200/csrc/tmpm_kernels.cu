@@ -376,10 +376,16 @@ __global__ void __launch_bounds__(THREADS, MINB)
                     int tb = tile_block_index<BS>(bx, cx, cy, cz);
                     int id = use_cache ? cc[kCacheHeader + tb] : s_blk[tb];
                     if (use_cache) s_blk[tb] = id;
-                    float4 val = make_float4(0.f, 0.f, 0.f, 0.f);
-                    if (id >= 0) val = __ldcg(cur.pool + static_cast<size_t>(id) * (1 << (3 * BS)) + node_local<BS>(cx, cy, cz));
-                    s_gv[t] = val;
+                    if (id >= 0) {
+                        // asynchronous 16-byte copy global -> shared (L2 only), no register staging
+                        const float4 *src = cur.pool + static_cast<size_t>(id) * (1 << (3 * BS)) + node_local<BS>(cx, cy, cz);
+                        const unsigned dst = static_cast<unsigned>(__cvta_generic_to_shared(s_gv + t));
+                        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src) : "memory");
+                    } else {
+                        s_gv[t] = make_float4(0.f, 0.f, 0.f, 0.f);
+                    }
                 }
+                asm volatile("cp.async.wait_all;" ::: "memory");
             }
             bad = __syncthreads_or(bad) != 0;
             if (!bad) break;
