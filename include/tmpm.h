@@ -261,12 +261,16 @@ typedef struct TmpmRigidMapping {
 TmpmStatus tmpm_rigid_attach(TmpmSession *session, const TmpmRigidBody *bodies, size_t body_count,
                              const TmpmRigidMapping *mappings, size_t mapping_count);
 /* `substeps` (1..64) coupled substeps of the session's substep, then a
- * synchronize (step_mpm_owned, gpu_rigid_sync.rs:202-214, for each substep).
- * gravity: the rigid bodies' gravity; max_linear_speed <= 0: no limit.
- * Needs no pending steps; not with CPIC obstacles (their side masks would use
- * the pose of the substep before). */
+ * synchronize.  integrate_pose != 0: step_mpm_owned (gpu_rigid_sync.rs:
+ * 202-214), the impulses, gravity and the speed limit change the velocities
+ * and the poses advance; 0: step_two_way (gpu_rigid_sync.rs:216-228), only
+ * the impulses (and the speed limit) change the velocities, for a rigid
+ * solver that integrates the bodies itself.  gravity: the rigid bodies'
+ * gravity; max_linear_speed <= 0: no limit.  Needs no pending steps; not
+ * with CPIC obstacles (their side masks would use the pose of the substep
+ * before). */
 TmpmStatus tmpm_rigid_step(TmpmSession *session, uint32_t substeps, const double gravity[3],
-                           double max_linear_speed);
+                           double max_linear_speed, int32_t integrate_pose);
 /* The bodies' current state. */
 TmpmStatus tmpm_rigid_read(TmpmSession *session, TmpmRigidBody *bodies, size_t body_count);
 void tmpm_rigid_detach(TmpmSession *session);

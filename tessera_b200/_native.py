@@ -150,7 +150,7 @@ def lib():
     L.tmpm_batch_last_error_message.restype = C.c_char_p
     L.tmpm_rigid_attach.argtypes = [P, C.POINTER(TmpmRigidBody), C.c_size_t, C.POINTER(TmpmRigidMapping), C.c_size_t]
     L.tmpm_rigid_attach.restype = S
-    L.tmpm_rigid_step.argtypes = [P, C.c_uint32, C.POINTER(C.c_double), C.c_double]
+    L.tmpm_rigid_step.argtypes = [P, C.c_uint32, C.POINTER(C.c_double), C.c_double, C.c_int32]
     L.tmpm_rigid_step.restype = S
     L.tmpm_rigid_read.argtypes = [P, C.POINTER(TmpmRigidBody), C.c_size_t]
     L.tmpm_rigid_read.restype = S

@@ -1020,7 +1020,8 @@ TmpmStatus tmpm_rigid_attach(TmpmSession *s, const TmpmRigidBody *bodies, size_t
     return TMPM_OK;
 }
 
-TmpmStatus tmpm_rigid_step(TmpmSession *s, uint32_t substeps, const double gravity[3], double max_linear_speed) {
+TmpmStatus tmpm_rigid_step(TmpmSession *s, uint32_t substeps, const double gravity[3], double max_linear_speed,
+                           int32_t integrate_pose) {
     TmpmStatus st = session_guard(s, true);
     if (st != TMPM_OK) return st;
     if (substeps == 0 || substeps > 64) return s->fail(TMPM_ERR_INVALID_INPUT, "substeps per submit must be 1..64");
@@ -1032,7 +1033,7 @@ TmpmStatus tmpm_rigid_step(TmpmSession *s, uint32_t substeps, const double gravi
     bool ok = f32_ok(s->substep_dt, p.dt) && f32_ok(std::isfinite(max_linear_speed) ? max_linear_speed : -1.0, p.max_speed);
     for (int k = 0; k < 3; ++k) ok = ok && gravity && f32_ok(gravity[k], p.gravity[k]);
     if (!ok) return s->fail(TMPM_ERR_INVALID_INPUT, "rigid gravity or speed limit not finite in f32");
-    p.integrate_pose = 1;
+    p.integrate_pose = integrate_pose ? 1 : 0;
     st = s->validate_resident(s->substep_dt);
     if (st != TMPM_OK) return st;
     cudaSetDevice(s->device);

@@ -197,11 +197,14 @@ class Session:
         self._rigid_count = len(bodies)
         _check(_native.lib().tmpm_rigid_attach(self._h, b, len(bodies), m, len(mappings)), self._h)
 
-    def rigid_step(self, substeps: int, gravity=(0.0, 0.0, 0.0), max_linear_speed: float = 0.0) -> None:
+    def rigid_step(self, substeps: int, gravity=(0.0, 0.0, 0.0), max_linear_speed: float = 0.0,
+                   integrate_pose: bool = True) -> None:
         """`substeps` coupled substeps (obstacles follow their bodies; impulses
-        move the bodies), then a synchronize."""
+        change the bodies' velocities and, with integrate_pose, gravity acts and
+        the poses advance), then a synchronize."""
         g = (C.c_double * 3)(*[float(v) for v in gravity])
-        _check(_native.lib().tmpm_rigid_step(self._h, int(substeps), g, float(max_linear_speed)), self._h)
+        _check(_native.lib().tmpm_rigid_step(self._h, int(substeps), g, float(max_linear_speed),
+                                             1 if integrate_pose else 0), self._h)
 
     def rigid_bodies(self) -> list:
         from ._abi import TmpmRigidBody

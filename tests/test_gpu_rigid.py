@@ -110,3 +110,60 @@ def test_attach_rejects_inconsistent_input():
     with pytest.raises(TesseraError) as e:
         s.rigid_step(1)  # nothing attached for this obstacle set
     assert e.value.status == TMPM_ERR_INVALID_INPUT
+
+
+def one_particle(x, vx=0.0):
+    p = density_particles([x], 0.04, 1000.0, MAT_ELASTIC, (1000.0, 0.2))
+    p.velocity[0, 0] = vx
+    return p
+
+
+def unit_sphere_bodies(xs, **kw):
+    bodies = [TmpmRigidBody.make((x, 0.0, 0.0), 1.0, inverse_inertia=(1.0, 1.0, 1.0), **kw) for x in xs]
+    obstacles = [Obstacle.sphere((x, 0.0, 0.0), 1.0) for x in xs]
+    maps = [TmpmRigidMapping.make(i) for i in range(len(xs))]
+    return bodies, obstacles, maps
+
+
+def test_mpm_owned_step_integrates_rigid_pose():  # gpu_rigid_sync.rs:607-668
+    params = make_params(0.1, gravity=(0.0, 0.0, 0.0))
+    bodies, obstacles, maps = unit_sphere_bodies([0.0], linear_velocity=(1.0, 0.0, 0.0),
+                                                 angular_velocity=(0.0, 0.0, 1.0))
+    s = Session(params, one_particle((3.0, 0.0, 0.0)), 0.001, obstacles=obstacles)
+    s.rigid_attach(bodies, maps)
+    s.rigid_step(1, gravity=(0.0, 0.0, -9.81))
+    first = s.rigid_bodies()[0].as_dict()
+    assert abs(first["position"][0] - 0.001) < 1e-6
+    assert abs(first["position"][2] + 9.81e-6) < 1e-7
+    assert abs(first["orientation"][2] - 0.0005) < 1e-6
+    s.rigid_step(1, gravity=(0.0, 0.0, -9.81))
+    second = s.rigid_bodies()[0].as_dict()
+    assert second["position"][0] > first["position"][0] and second["orientation"][2] > first["orientation"][2]
+
+
+def test_mpm_owned_step_caps_speed_before_pose_integration():  # gpu_rigid_sync.rs:671-724
+    params = make_params(0.1, gravity=(0.0, 0.0, 0.0))
+    bodies, obstacles, maps = unit_sphere_bodies([0.0], linear_velocity=(2.0, 0.0, 0.0))
+    s = Session(params, one_particle((3.0, 0.0, 0.0)), 0.001, obstacles=obstacles)
+    s.rigid_attach(bodies, maps)
+    s.rigid_step(1, max_linear_speed=0.5)
+    b = s.rigid_bodies()[0].as_dict()
+    assert abs(b["linear_velocity"][0] - 0.5) < 1e-5 and abs(b["position"][0] - 0.0005) < 1e-6
+
+
+@pytest.mark.parametrize("count", [1, 17, 70])
+def test_two_way_reaction_reaches_its_body(count):  # gpu_rigid_sync.rs:727-858
+    """A particle moving into the last of `count` unit spheres (the others far
+    away): only that body takes the impulse; the particle slows down."""
+    params = make_params(0.1, gravity=(0.0, 0.0, 0.0))
+    xs = [10.0 + 3.0 * k for k in range(count - 1)] + [0.0]
+    bodies, obstacles, maps = unit_sphere_bodies(xs)
+    s = Session(params, one_particle((1.02, 0.0, 0.0), vx=-1.0), 0.001, obstacles=obstacles)
+    s.rigid_attach(bodies, maps)
+    s.rigid_step(1, integrate_pose=False)
+    states = [b.as_dict() for b in s.rigid_bodies()]
+    assert all(abs(b["linear_velocity"][0]) < 1e-6 for b in states[:-1])
+    assert states[-1]["linear_velocity"][0] < -0.01, states[-1]
+    assert states[-1]["position"][0] == 0.0  # velocities only: the rigid solver integrates
+    assert s.particles().velocity[0, 0] > -1.0
+    assert s.substeps() == 1
