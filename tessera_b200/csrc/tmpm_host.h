@@ -877,8 +877,14 @@ struct PackResult {
 // `alloc(n_enabled)` supplies the PackTarget and pass 2 writes the f32 rows
 // at compacted positions.  Results equal a serial pass in world order.
 // `ns_high` is OR-ed into every class's grid namespace (multi-scene batches).
-template <typename Alloc>
-PackResult pack_world(const HostWorld &world, float inv_h, uint32_t ns_high, ClassTable &ct, Alloc alloc) {
+// No work before a block of pass 1 (see pack_world's `before`).
+struct PackNoHook {
+    bool operator()(size_t, size_t, size_t) const { return true; }
+};
+
+template <typename Alloc, typename Before = PackNoHook>
+PackResult pack_world(const HostWorld &world, float inv_h, uint32_t ns_high, ClassTable &ct, Alloc alloc,
+                      Before before = Before()) {
     PackResult res;
     const size_t N = world.n;
     struct ChunkOut {
@@ -886,6 +892,7 @@ PackResult pack_world(const HostWorld &world, float inv_h, uint32_t ns_high, Cla
         TmpmStatus st = TMPM_OK;
         const char *msg = "";
         size_t enabled = 0;
+        bool aborted = false;  // `before` rejected a block
         std::vector<DevClass> classes;
         std::vector<unsigned long long> blocks;
     };
@@ -903,7 +910,8 @@ PackResult pack_world(const HostWorld &world, float inv_h, uint32_t ns_high, Cla
             o.st = st;
             o.msg = msg;
         };
-        for (size_t i = lo; i < hi; ++i) {
+        // one particle; `return bad(...)` records the chunk's first error
+        auto one = [&](size_t i) {
             float f4[4];
             for (int k = 0; k < 3; ++k)
                 if (!f32_ok(world.pos[3 * i + k], f4[k]) || !f32_ok(world.vel[3 * i + k], f4[3]) ||
@@ -922,7 +930,7 @@ PackResult pack_world(const HostWorld &world, float inv_h, uint32_t ns_high, Cla
                 if (!f32_ok(world.F[9 * i + k], t) || !f32_ok(world.C[9 * i + k], t))
                     return bad(i, TMPM_ERR_INVALID_INPUT, "particle matrices not representable in f32");
             }
-            if (!world.enabled[i]) continue;
+            if (!world.enabled[i]) return;
             int base[3];
             for (int k = 0; k < 3; ++k) {
                 float xk = static_cast<float>(world.pos[3 * i + k]);
@@ -1009,10 +1017,29 @@ PackResult pack_world(const HostWorld &world, float inv_h, uint32_t ns_high, Cla
                 last_block = hb;
             }
             ++o.enabled;
+        };
+        // blocks of 256: `before` (e.g. the load of these particles into `world`)
+        // runs first, so the particles are checked and packed while in cache;
+        // after an error of this pass the rest of the chunk still goes through
+        // `before`, whose own errors come first
+        constexpr size_t kBlock = 256;
+        for (size_t a0 = lo; a0 < hi; a0 += kBlock) {
+            const size_t b0 = std::min(hi, a0 + kBlock);
+            if (!before(c, a0, b0)) {
+                o.aborted = true;
+                return;
+            }
+            for (size_t i = a0; i < b0 && o.first_bad == std::numeric_limits<size_t>::max(); ++i) one(i);
         }
         std::sort(o.blocks.begin(), o.blocks.end());
         o.blocks.erase(std::unique(o.blocks.begin(), o.blocks.end()), o.blocks.end());
     });
+    for (const ChunkOut &o : co)
+        if (o.aborted) {
+            res.st = TMPM_ERR_MPM_INVALID_INPUT;
+            res.msg = "invalid MPM input";
+            return res;
+        }
     size_t worst = std::numeric_limits<size_t>::max();
     for (const ChunkOut &o : co)
         if (o.first_bad < worst) {

@@ -13,6 +13,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <functional>
 #include <limits>
 #include <mutex>
 #include <string>
@@ -136,7 +137,10 @@ struct TmpmSession {
 
     // Pack and upload the world (the device half of GpuMpmTransfers::prepare,
     // gpu.rs:1091-1600).  Device buffers are reused when large enough.
-    TmpmStatus upload(double dt) {
+    // `before`, when given, runs on each block of particles just before the
+    // packing pass validates and packs it (tmpm_write_particles loads the
+    // particles into the world there, so they are checked and packed in cache).
+    TmpmStatus upload(double dt, const std::function<bool(size_t, size_t, size_t)> *before = nullptr) {
         float h32, dt32, inv_d32;
         if (!f32_ok(params.cell_width, h32) || !f32_ok(dt, dt32) ||
             !f32_ok(4.0 / (params.cell_width * params.cell_width), inv_d32) || h32 <= 0.0f || dt32 <= 0.0f)
@@ -158,17 +162,20 @@ struct TmpmSession {
         // Validate and pack the world straight into pinned staging (stride `cap`).
         ClassTable ct;
         size_t cap = 256;
-        PackResult pr = pack_world(world, inv_h, 0u, ct, [&](size_t n_enabled) {
-            PackTarget tg;
-            cap = std::max<size_t>(256, (n_enabled + 255) / 256 * 256);
-            if (n_enabled > static_cast<size_t>(std::numeric_limits<int>::max() / 2)) return tg;
-            if (!upload_staging.ensure((27 * cap + 2 * cap) * sizeof(float))) return tg;
-            tg.base = static_cast<float *>(upload_staging.ptr);
-            tg.cls = reinterpret_cast<uint32_t *>(tg.base + 27 * cap);
-            tg.widx = tg.cls + cap;
-            tg.stride = cap;
-            return tg;
-        });
+        PackResult pr = pack_world(
+            world, inv_h, 0u, ct,
+            [&](size_t n_enabled) {
+                PackTarget tg;
+                cap = std::max<size_t>(256, (n_enabled + 255) / 256 * 256);
+                if (n_enabled > static_cast<size_t>(std::numeric_limits<int>::max() / 2)) return tg;
+                if (!upload_staging.ensure((27 * cap + 2 * cap) * sizeof(float))) return tg;
+                tg.base = static_cast<float *>(upload_staging.ptr);
+                tg.cls = reinterpret_cast<uint32_t *>(tg.base + 27 * cap);
+                tg.widx = tg.cls + cap;
+                tg.stride = cap;
+                return tg;
+            },
+            [&](size_t c, size_t a, size_t b) { return !before || (*before)(c, a, b); });
         if (pr.st != TMPM_OK) {
             if (pr.st == TMPM_ERR_DEVICE && pr.enabled > static_cast<size_t>(std::numeric_limits<int>::max() / 2))
                 return fail(TMPM_ERR_CAPACITY, "too many particles for one session");
@@ -758,6 +765,61 @@ TmpmStatus tmpm_remove_chunk(TmpmSession *s, uint64_t chunk, size_t *removed_out
 TmpmStatus tmpm_write_particles(TmpmSession *s, const TmpmParticleArrays *particles) {
     TmpmStatus st = session_guard(s, true);
     if (st != TMPM_OK) return st;
+    const bool fused = particles && particles->count > 0 && !s->cpic_active() && particles->position &&
+                       particles->velocity && particles->mass && particles->rest_volume && particles->radius &&
+                       particles->material && particles->material_params;
+    if (fused) {
+        // The particles are loaded into the world inside the packing pass, one
+        // block at a time, so each is copied, validated (world.rs:492-503),
+        // bounded for the CFL step and packed for upload while in cache.  The
+        // errors keep the order of the two-pass path below: invalid input, then
+        // the CFL bound, then what packing rejects.
+        std::swap(s->world, s->spare);  // spare: the previous world, restored on failure
+        HostWorld &nw = s->world;
+        const HostWorld &old = s->spare;
+        nw.resize(particles->count);
+        const double max_substep = s->params.max_substep, h = s->params.cell_width;
+        std::vector<double> part(host_threads() + 1, max_substep);
+        std::atomic<bool> bad{false};
+        const bool keep_chunks = !particles->chunk_id;
+        std::function<bool(size_t, size_t, size_t)> load = [&](size_t c, size_t a, size_t b) {
+            if (bad.load(std::memory_order_relaxed)) return false;
+            nw.load_range(*particles, a, b);
+            double dt = part[c];
+            for (size_t i = a; i < b; ++i) {
+                if (!valid_particle(nw, i)) {
+                    bad = true;
+                    return false;
+                }
+                if (nw.enabled[i] && !nw.fixed[i])
+                    dt = std::min(dt, timestep_bound(nw.material[i], &nw.mparams[5 * i], nw.mass[i] / nw.vol[i],
+                                                     &nw.vel[3 * i], h, det9(&nw.F[9 * i])));
+                if (keep_chunks && i < old.n) nw.chunk[i] = old.chunk[i];
+            }
+            part[c] = dt;
+            return true;
+        };
+        cudaSetDevice(s->device);
+        st = s->upload(s->substep_dt, &load);
+        if (bad) {
+            st = s->fail(TMPM_ERR_MPM_INVALID_INPUT, "invalid MPM input");
+        } else {
+            double dt = max_substep;  // the CFL bound stable_timestep() would compute
+            for (double d : part) dt = std::min(dt, d);
+            nw.cfl_version = nw.version;
+            nw.cfl_h = h;
+            nw.cfl_max = max_substep;
+            nw.cfl_value = std::min(dt, max_substep);
+            const TmpmStatus v = s->validate_resident(s->substep_dt);
+            if (v != TMPM_OK) st = v;
+        }
+        if (st != TMPM_OK) {
+            std::swap(s->world, s->spare);
+            if (s->valid) s->upload(s->substep_dt);
+            return st;
+        }
+        return TMPM_OK;
+    }
     // Load into the session's spare world (its storage is reused across calls)
     // and swap it in; the previous world comes back on any failure.
     HostWorld &nw = s->spare;

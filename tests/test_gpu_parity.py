@@ -338,3 +338,48 @@ def test_snapshot_matches_synchronized_state():  # gpu.rs:2964-3161
     assert np.abs(snap[:, :3] - got.position).max() < 1e-6
     assert np.abs(snap[:, 4:7] - got.velocity).max() < 1e-6
     assert np.allclose(snap[:, 3], got.mass, rtol=1e-6) and np.allclose(snap[:, 7], got.rest_volume, rtol=1e-6)
+
+
+def test_write_particles_replaces_the_world_and_bad_input_leaves_it():
+    """tmpm_write_particles (load, validation, CFL bound and packing in one pass):
+    the written world is what the session then advances, like the oracle; an
+    invalid particle, a step above the CFL bound or a state f32 cannot hold is
+    rejected with the previous world and device state intact."""
+    from tessera_b200._abi import TMPM_ERR_MPM_INVALID_INPUT
+
+    sc = scenes.sphere_drop()
+    s = Session(sc.params, sc.particles, sc.dt, obstacles=sc.obstacles)
+    s.step(4)
+    moved = sc.particles.copy()
+    moved.position[:, 0] += 0.02
+    moved.velocity[:, 1] = 0.3
+    moved.chunk_id[:] = 7
+    s.write_particles(moved)
+    got = s.particles()
+    assert np.array_equal(got.position, moved.position) and np.array_equal(got.velocity, moved.velocity)
+    assert np.all(got.chunk_id == 7)
+    s.step(8)
+    w = O.OracleWorld(sc.params, moved)
+    w.set_obstacles(sc.obstacles)
+    for _ in range(8):
+        w.substep_fixed(sc.dt)
+    assert_close(w.particles(), s.particles(), 2e-5, 2e-4)
+    keep = s.particles()
+    bad_mass = moved.copy()
+    bad_mass.mass[5] = -1.0
+    too_fast = moved.copy()
+    too_fast.velocity[9, 2] = 1e4
+    no_f32 = moved.copy()
+    no_f32.position[3, 0] = 1e39  # finite in f64, beyond f32
+    for bad, status in ((bad_mass, TMPM_ERR_MPM_INVALID_INPUT), (too_fast, TMPM_ERR_INVALID_INPUT),
+                        (no_f32, TMPM_ERR_INVALID_INPUT)):
+        with pytest.raises(TesseraError) as e:
+            s.write_particles(bad)
+        assert e.value.status == status
+        now = s.particles()
+        assert np.array_equal(now.position, keep.position) and np.array_equal(now.velocity, keep.velocity)
+    # the session still advances the kept world like the oracle
+    s.step(2)
+    for _ in range(2):
+        w.substep_fixed(sc.dt)
+    assert_close(w.particles(), s.particles(), 2e-5, 2e-4)
