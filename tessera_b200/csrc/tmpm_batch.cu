@@ -114,7 +114,7 @@ TmpmStatus prepare_scene(const TmpmParams &params, const TmpmParticleArrays *par
         tg.widx = row_widx(p.rows, stride);
         tg.stride = stride;
         return tg;
-    });
+    }, PackNoHook(), true);
     if (pr.st != TMPM_OK) {
         g_last_error = pr.msg;
         return pr.st;

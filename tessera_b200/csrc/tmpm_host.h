@@ -882,11 +882,19 @@ struct PackNoHook {
     bool operator()(size_t, size_t, size_t) const { return true; }
 };
 
+// With `eager_rows`, the f32 rows are written in the first pass, at each
+// particle's world index, while its values are in cache (the target comes from
+// alloc(world.n)); when every particle is enabled those are the final
+// positions and the second pass writes only the class and index rows.
 template <typename Alloc, typename Before = PackNoHook>
 PackResult pack_world(const HostWorld &world, float inv_h, uint32_t ns_high, ClassTable &ct, Alloc alloc,
-                      Before before = Before()) {
+                      Before before = Before(), bool eager_rows = false) {
     PackResult res;
     const size_t N = world.n;
+    PackTarget tg0;
+    if (eager_rows && N > 0) tg0 = alloc(N);
+    const bool eager = tg0.base != nullptr;
+    const size_t S0 = tg0.stride;
     struct ChunkOut {
         size_t first_bad = std::numeric_limits<size_t>::max();
         TmpmStatus st = TMPM_OK;
@@ -1016,6 +1024,18 @@ PackResult pack_world(const HostWorld &world, float inv_h, uint32_t ns_high, Cla
                 o.blocks.push_back(hb);
                 last_block = hb;
             }
+            if (eager) {
+                float *r = tg0.base;
+                for (int k3 = 0; k3 < 3; ++k3) {
+                    r[k3 * S0 + i] = static_cast<float>(world.pos[3 * i + k3]);
+                    r[(3 + k3) * S0 + i] = static_cast<float>(world.vel[3 * i + k3]);
+                    r[(24 + k3) * S0 + i] = static_cast<float>(world.plastic[3 * i + k3]);
+                }
+                for (int k9 = 0; k9 < 9; ++k9) {
+                    r[(6 + k9) * S0 + i] = static_cast<float>(world.C[9 * i + k9]);
+                    r[(15 + k9) * S0 + i] = static_cast<float>(world.F[9 * i + k9]);
+                }
+            }
             ++o.enabled;
         };
         // blocks of 256: `before` (e.g. the load of these particles into `world`)
@@ -1066,7 +1086,9 @@ PackResult pack_world(const HostWorld &world, float inv_h, uint32_t ns_high, Cla
         return res;
     }
     res.enabled = n_enabled;
-    PackTarget tg = alloc(n_enabled);
+    // every particle enabled: the rows of the first pass are in place
+    const bool rows_done = eager && n_enabled == N;
+    PackTarget tg = rows_done ? tg0 : alloc(n_enabled);
     if (!tg.base) {
         res.st = TMPM_ERR_DEVICE;
         res.msg = "pinned staging allocation failed";
@@ -1079,6 +1101,12 @@ PackResult pack_world(const HostWorld &world, float inv_h, uint32_t ns_high, Cla
         const std::vector<uint32_t> &rm = remap[c];
         for (size_t i = lo; i < hi; ++i) {
             if (!world.enabled[i]) continue;
+            if (rows_done) {
+                tg.cls[j] = rm[lcls[i]] | (world.fixed[i] ? kFixedBit : 0u);
+                tg.widx[j] = static_cast<uint32_t>(i);
+                ++j;
+                continue;
+            }
             for (int k3 = 0; k3 < 3; ++k3) {
                 hx[k3 * S + j] = static_cast<float>(world.pos[3 * i + k3]);
                 hv[k3 * S + j] = static_cast<float>(world.vel[3 * i + k3]);

@@ -175,7 +175,7 @@ struct TmpmSession {
                 tg.stride = cap;
                 return tg;
             },
-            [&](size_t c, size_t a, size_t b) { return !before || (*before)(c, a, b); });
+            [&](size_t c, size_t a, size_t b) { return !before || (*before)(c, a, b); }, true);
         if (pr.st != TMPM_OK) {
             if (pr.st == TMPM_ERR_DEVICE && pr.enabled > static_cast<size_t>(std::numeric_limits<int>::max() / 2))
                 return fail(TMPM_ERR_CAPACITY, "too many particles for one session");
