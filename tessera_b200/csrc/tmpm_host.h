@@ -117,67 +117,90 @@ struct HostWorld {
         parallel_for(n, [&](size_t lo, size_t hi) { load_range(a, lo, hi); });
     }
 
+    // Field by field (contiguous copies of [lo, hi) in the same layout), with the
+    // defaults of absent optional arrays: F = I, C = 0, force 0, damping 0, the
+    // plastic state (1, 1 for sand kinds else 0, 0), enabled, not fixed.
     void load_range(const TmpmParticleArrays &a, size_t lo, size_t hi) {
-        for (size_t i = lo; i < hi; ++i) {
-            for (int k = 0; k < 3; ++k) {
-                pos[3 * i + k] = a.position[3 * i + k];
-                vel[3 * i + k] = a.velocity[3 * i + k];
-                force[3 * i + k] = a.force ? a.force[3 * i + k] : 0.0;
-            }
-            for (int k = 0; k < 9; ++k) {
-                F[9 * i + k] = a.deformation ? a.deformation[9 * i + k] : ((k % 4 == 0) ? 1.0 : 0.0);
-                C[9 * i + k] = a.affine ? a.affine[9 * i + k] : 0.0;
-            }
-            mass[i] = a.mass[i];
-            vol[i] = a.rest_volume[i];
-            radius[i] = a.radius[i];
-            damping[i] = a.damping ? a.damping[i] : 0.0;
-            material[i] = a.material[i];
-            for (int k = 0; k < 5; ++k) mparams[5 * i + k] = a.material_params[5 * i + k];
-            if (a.plastic) {
-                for (int k = 0; k < 3; ++k) plastic[3 * i + k] = a.plastic[3 * i + k];
-            } else {
+        const size_t m = hi - lo;
+        auto copy = [&](auto *dst, const auto *src, int width) {
+            std::memcpy(dst + width * lo, src + width * lo, sizeof(*dst) * width * m);
+        };
+        copy(pos.data(), a.position, 3);
+        copy(vel.data(), a.velocity, 3);
+        if (a.force) copy(force.data(), a.force, 3);
+        else std::fill(force.begin() + 3 * lo, force.begin() + 3 * hi, 0.0);
+        if (a.deformation) {
+            copy(F.data(), a.deformation, 9);
+        } else {
+            for (size_t i = lo; i < hi; ++i)
+                for (int k = 0; k < 9; ++k) F[9 * i + k] = (k % 4 == 0) ? 1.0 : 0.0;
+        }
+        if (a.affine) copy(C.data(), a.affine, 9);
+        else std::fill(C.begin() + 9 * lo, C.begin() + 9 * hi, 0.0);
+        copy(mass.data(), a.mass, 1);
+        copy(vol.data(), a.rest_volume, 1);
+        copy(radius.data(), a.radius, 1);
+        if (a.damping) copy(damping.data(), a.damping, 1);
+        else std::fill(damping.begin() + lo, damping.begin() + hi, 0.0);
+        copy(material.data(), a.material, 1);
+        copy(mparams.data(), a.material_params, 5);
+        if (a.plastic) {
+            copy(plastic.data(), a.plastic, 3);
+        } else {
+            for (size_t i = lo; i < hi; ++i) {
                 plastic[3 * i] = 1.0;
-                plastic[3 * i + 1] = (material[i] == TMPM_MAT_SAND || material[i] == TMPM_MAT_SAND_NEO_HOOKEAN) ? 1.0 : 0.0;
+                plastic[3 * i + 1] =
+                    (material[i] == TMPM_MAT_SAND || material[i] == TMPM_MAT_SAND_NEO_HOOKEAN) ? 1.0 : 0.0;
                 plastic[3 * i + 2] = 0.0;
             }
-            enabled[i] = a.enabled ? (a.enabled[i] != 0) : 1;
-            fixed[i] = a.fixed ? (a.fixed[i] != 0) : 0;
-            color[i] = a.transfer_color ? a.transfer_color[i] : 0;
-            group[i] = a.group_id ? a.group_id[i] : 0;
-            chunk[i] = a.chunk_id ? a.chunk_id[i] : 0;
         }
+        if (a.enabled) {
+            for (size_t i = lo; i < hi; ++i) enabled[i] = a.enabled[i] != 0;
+        } else {
+            std::fill(enabled.begin() + lo, enabled.begin() + hi, uint8_t(1));
+        }
+        if (a.fixed) {
+            for (size_t i = lo; i < hi; ++i) fixed[i] = a.fixed[i] != 0;
+        } else {
+            std::fill(fixed.begin() + lo, fixed.begin() + hi, uint8_t(0));
+        }
+        if (a.transfer_color) copy(color.data(), a.transfer_color, 1);
+        else std::fill(color.begin() + lo, color.begin() + hi, uint16_t(0));
+        if (a.group_id) copy(group.data(), a.group_id, 1);
+        else std::fill(group.begin() + lo, group.begin() + hi, 0u);
+        if (a.chunk_id) copy(chunk.data(), a.chunk_id, 1);
+        else std::fill(chunk.begin() + lo, chunk.begin() + hi, uint64_t(0));
     }
 
     void store(TmpmParticleArrays &a) const {
         parallel_for(n, [&](size_t lo, size_t hi) { store_range(a, lo, hi); });
     }
 
+    // Field by field, only the fields `a` asks for.
     void store_range(TmpmParticleArrays &a, size_t lo, size_t hi) const {
-        for (size_t i = lo; i < hi; ++i) {
-            for (int k = 0; k < 3; ++k) {
-                if (a.position) a.position[3 * i + k] = pos[3 * i + k];
-                if (a.velocity) a.velocity[3 * i + k] = vel[3 * i + k];
-                if (a.force) a.force[3 * i + k] = force[3 * i + k];
-                if (a.plastic) a.plastic[3 * i + k] = plastic[3 * i + k];
-            }
-            for (int k = 0; k < 9; ++k) {
-                if (a.deformation) a.deformation[9 * i + k] = F[9 * i + k];
-                if (a.affine) a.affine[9 * i + k] = C[9 * i + k];
-            }
-            if (a.mass) a.mass[i] = mass[i];
-            if (a.rest_volume) a.rest_volume[i] = vol[i];
-            if (a.radius) a.radius[i] = radius[i];
-            if (a.damping) a.damping[i] = damping[i];
-            if (a.material) a.material[i] = material[i];
-            if (a.material_params)
-                for (int k = 0; k < 5; ++k) a.material_params[5 * i + k] = mparams[5 * i + k];
-            if (a.enabled) a.enabled[i] = enabled[i];
-            if (a.fixed) a.fixed[i] = fixed[i];
-            if (a.transfer_color) a.transfer_color[i] = color[i];
-            if (a.group_id) a.group_id[i] = group[i];
-            if (a.chunk_id) a.chunk_id[i] = chunk[i];
-        }
+        const size_t m = hi - lo;
+        auto copy = [&](auto *dst, const auto *src, int width) {
+            if (dst) std::memcpy(dst + width * lo, src + width * lo, sizeof(*dst) * width * m);
+        };
+        copy(a.position, pos.data(), 3);
+        copy(a.velocity, vel.data(), 3);
+        copy(a.force, force.data(), 3);
+        copy(a.plastic, plastic.data(), 3);
+        copy(a.deformation, F.data(), 9);
+        copy(a.affine, C.data(), 9);
+        copy(a.mass, mass.data(), 1);
+        copy(a.rest_volume, vol.data(), 1);
+        copy(a.radius, radius.data(), 1);
+        copy(a.damping, damping.data(), 1);
+        copy(a.material, material.data(), 1);
+        copy(a.material_params, mparams.data(), 5);
+        copy(a.transfer_color, color.data(), 1);
+        copy(a.group_id, group.data(), 1);
+        copy(a.chunk_id, chunk.data(), 1);
+        if (a.enabled)
+            for (size_t i = lo; i < hi; ++i) a.enabled[i] = enabled[i];
+        if (a.fixed)
+            for (size_t i = lo; i < hi; ++i) a.fixed[i] = fixed[i];
     }
 
     void append(const HostWorld &o) {
