@@ -8,8 +8,10 @@
 // A batch opens with a P2G-only transfer and closes with a G2P-only transfer,
 // which alone writes velocity and the affine matrix back to HBM.
 //
-// Each CTA owns 256 consecutive particles in storage order (sorted by 4^3
-// block).  It stages the grid nodes its particles touch in a shared-memory
+// Each CTA owns a chunk of consecutive particles in storage order (sorted by
+// block and cell; 256 or 128 per chunk, the launch shape's CTA size, see
+// kLaunchShapes; grid blocks of 4^3 or 8^3 cells, the template parameter BS).
+// It stages the grid nodes its particles touch in a shared-memory
 // box ("tile"): the gather tile holds step-n velocities, the scatter tile
 // accumulates step-(n+1) mass and momentum with shared atomics and is flushed
 // to the block pool with one float4 atomic per touched node.  Chunks whose box
