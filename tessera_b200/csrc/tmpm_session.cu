@@ -15,6 +15,7 @@
 #include <cstring>
 #include <functional>
 #include <limits>
+#include <map>
 #include <mutex>
 #include <string>
 #include <thread>
@@ -29,6 +30,11 @@ using namespace tmpm;
 
 
 void tmpm::set_last_error(const std::string &msg) { g_last_error = msg; }
+
+// Segments of at least this many substeps are captured and replayed as CUDA
+// graphs (shorter ones, e.g. the single substeps of tmpm_step_cfl, are
+// launched: a capture costs more than it saves when not repeated).
+constexpr uint32_t kGraphMinSubsteps = 8;
 
 struct TmpmSession {
     // host world (last synchronized state)
@@ -75,6 +81,9 @@ struct TmpmSession {
     bool has_plastic = false;  // class table holds a snow, sand or NH sand class
     uint64_t since_resort = 0;
     LaunchTuner tuner;       // transfer launch configuration (tuned on the first segments unless fixed)
+    // Segments captured as CUDA graphs, keyed by everything their kernels bake
+    // in (parameters, buffer pointers, sizes); replayed when a segment repeats.
+    std::map<std::string, cudaGraphExec_t> seg_graphs;
     int stored_shape = -1;   // launch shape whose per-CTA interleave the device rows hold
     bool big_blocks_ok = false;  // the node pools hold the scene in 8^3 blocks too
 
@@ -82,6 +91,7 @@ struct TmpmSession {
         if (stream) {
             cudaStreamSynchronize(stream);
         }
+        drop_graphs();
         if (done) cudaEventDestroy(done);
         for (cudaEvent_t &ev : read_events)
             if (ev) cudaEventDestroy(ev);
@@ -319,6 +329,82 @@ struct TmpmSession {
         g[1].pool = grids[1].pool.ptr;
     }
 
+    void drop_graphs() {
+        for (auto &kv : seg_graphs) cudaGraphExecDestroy(kv.second);
+        seg_graphs.clear();
+    }
+
+    SortBuffers sort_buffers() const {
+        SortBuffers sb{};
+        sb.keys[0] = sort_keys[0].ptr;
+        sb.keys[1] = sort_keys[1].ptr;
+        sb.vals[0] = sort_vals[0].ptr;
+        sb.vals[1] = sort_vals[1].ptr;
+        sb.hist = sort_hist.ptr;
+        sb.totals = sort_totals.ptr;
+        sb.cap = sort_keys[0].count;
+        return sb;
+    }
+
+    // The kernels of one segment in stream order: re-sort from row buffer
+    // `from` into the other (when `resort`), table clear, P2G, `seg` x (grid
+    // update, transfer) with the last transfer G2P-only; the one-shot forces
+    // act in the first substep and are cleared after it when `apply_force`.
+    void launch_segment(const SimParams &sp, int from, bool resort, uint32_t seg, bool apply_force) {
+        const int bs = sp.block_shift;
+        const int rows = resort ? from ^ 1 : from;
+        if (resort) {
+            ParticleSoA src = pbuf[from].view(force.ptr, std::max<size_t>(world.n, 1));
+            ParticleSoA dst = pbuf[rows].view(force.ptr, std::max<size_t>(world.n, 1));
+            SortBuffers sb = sort_buffers();
+            launch_resort(src, dst, n_dev, n_dev, classes.ptr, sp, sb, stream);
+        }
+        GridTable g[2];
+        grid_views(g, bs);
+        const ParticleSoA P = pbuf[rows].view(force.ptr, std::max<size_t>(world.n, 1));
+        launch_clear_table(g[0], g[1], bs, stream);
+        launch_transfer(kModeP2G, P, n_dev, classes.ptr, g[1], g[0], sp, dev_obstacles.ptr, dev_planes.ptr,
+                        reactions.ptr, status.ptr, cta_cache.ptr, stream);
+        for (uint32_t k = 0; k < seg; ++k) {
+            const GridTable &gc = g[k & 1], &gn = g[(k + 1) & 1];
+            launch_grid_update(gc, gn, sp, dev_obstacles.ptr, dev_planes.ptr, reactions.ptr, status.ptr, stream);
+            SimParams spk = sp;
+            spk.apply_force = (apply_force && k == 0) ? 1 : 0;
+            launch_transfer(k + 1 == seg ? kModeG2P : kModeG2P2G, P, n_dev, classes.ptr, gc, gn, spk,
+                            dev_obstacles.ptr, dev_planes.ptr, reactions.ptr, status.ptr, cta_cache.ptr, stream);
+            if (apply_force && k == 0) cudaMemsetAsync(force.ptr, 0, sizeof(float) * force.count, stream);
+        }
+    }
+
+    // Everything launch_segment's kernels bake in, as a byte string.
+    std::string segment_key(const SimParams &sp, int from, bool resort, uint32_t seg, bool apply_force) const {
+        struct {
+            SimParams sp;
+            ParticleSoA rows[2];
+            GridTable g[2];
+            SortBuffers sb;
+            const void *ptr[7];
+            size_t force_count, n_world;
+            int64_t from, resort, seg, n_dev, apply_force;
+        } k;
+        std::memset(&k, 0, sizeof k);
+        k.sp = sp;
+        for (int b = 0; b < 2; ++b) k.rows[b] = pbuf[b].view(force.ptr, std::max<size_t>(world.n, 1));
+        grid_views(k.g, sp.block_shift);
+        k.sb = sort_buffers();
+        const void *ptrs[7] = {classes.ptr, dev_obstacles.ptr, dev_planes.ptr, reactions.ptr, status.ptr,
+                               cta_cache.ptr, force.ptr};
+        for (int i = 0; i < 7; ++i) k.ptr[i] = ptrs[i];
+        k.force_count = force.count;
+        k.n_world = world.n;
+        k.from = from;
+        k.resort = resort;
+        k.seg = seg;
+        k.n_dev = n_dev;
+        k.apply_force = apply_force;
+        return std::string(reinterpret_cast<const char *>(&k), sizeof k);
+    }
+
     // Queue `steps` resident substeps on the stream (encode_prepared, gpu.rs:1729-1777).
     TmpmStatus enqueue(uint32_t steps, double dt, bool resident, bool with_reactions, std::vector<float> *kernel_ms) {
         if (n_dev == 0) return TMPM_OK;
@@ -359,18 +445,40 @@ struct TmpmSession {
         // the rows are re-sorted (and re-interleaved) when the shape changes
         const bool resort_now = since_resort >= interval || shape != stored_shape;
         const uint32_t seg = std::min<uint32_t>(steps - done, resort_now ? interval : interval - since_resort);
+        const bool apply_force = done == 0 && force_dirty;
+        // Replay a captured graph for a segment long enough to be worth it,
+        // outside per-kernel timing and tuning trials; otherwise launch.
+        const bool graph = kernel_ms == nullptr && !(tunable && tuner.tuning()) && seg >= kGraphMinSubsteps;
+        if (graph) {
+            const std::string key = segment_key(sp, cur, resort_now, seg, apply_force);
+            auto it = seg_graphs.find(key);
+            if (it == seg_graphs.end()) {
+                if (seg_graphs.size() >= 16) drop_graphs();
+                cudaGraph_t g = nullptr;
+                cudaError_t e;
+                if ((e = cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal)))
+                    return cuda_fail(e, "cudaStreamBeginCapture");
+                launch_segment(sp, cur, resort_now, seg, apply_force);
+                if ((e = cudaStreamEndCapture(stream, &g))) return cuda_fail(e, "cudaStreamEndCapture");
+                cudaGraphExec_t exec = nullptr;
+                e = cudaGraphInstantiate(&exec, g, 0);
+                cudaGraphDestroy(g);
+                if (e) return cuda_fail(e, "cudaGraphInstantiate");
+                it = seg_graphs.emplace(key, exec).first;
+            }
+            cudaError_t e = cudaGraphLaunch(it->second, stream);
+            if (e) return cuda_fail(e, "cudaGraphLaunch");
+            if (resort_now) {
+                cur ^= 1;
+                since_resort = 0;
+                stored_shape = shape;
+            }
+        } else {
         if (resort_now) {
             tick(0);
             ParticleSoA src = soa();
             ParticleSoA dst = pbuf[cur ^ 1].view(force.ptr, std::max<size_t>(world.n, 1));
-            SortBuffers sb{};
-            sb.keys[0] = sort_keys[0].ptr;
-            sb.keys[1] = sort_keys[1].ptr;
-            sb.vals[0] = sort_vals[0].ptr;
-            sb.vals[1] = sort_vals[1].ptr;
-            sb.hist = sort_hist.ptr;
-            sb.totals = sort_totals.ptr;
-            sb.cap = sort_keys[0].count;
+            SortBuffers sb = sort_buffers();
             launch_resort(src, dst, n_dev, n_dev, classes.ptr, sp, sb, stream);
             cur ^= 1;
             since_resort = 0;
@@ -392,18 +500,17 @@ struct TmpmSession {
             launch_grid_update(gc, gn, sp, dev_obstacles.ptr, dev_planes.ptr, reactions.ptr, status.ptr, stream);
             tock(1);
             SimParams spk = sp;
-            const bool first = done == 0 && s == 0;
-            spk.apply_force = (first && force_dirty) ? 1 : 0;
+            const bool first = s == 0;
+            spk.apply_force = (first && apply_force) ? 1 : 0;
             bool last = s + 1 == seg;
             tick(0);
             launch_transfer(last ? kModeG2P : kModeG2P2G, P, n_dev, classes.ptr, gc, gn, spk, dev_obstacles.ptr,
                             dev_planes.ptr, reactions.ptr, status.ptr, cta_cache.ptr, stream);
             tock(last ? 3 : 2);
-            if (first && force_dirty) {
-                cudaMemsetAsync(force.ptr, 0, sizeof(float) * force.count, stream);
-                force_dirty = false;
-            }
+            if (first && apply_force) cudaMemsetAsync(force.ptr, 0, sizeof(float) * force.count, stream);
         }
+        }
+        if (apply_force) force_dirty = false;
         if (tunable) tuner.end(static_cast<double>(n_dev) * seg, stream);
         since_resort += seg;
         done += seg;
