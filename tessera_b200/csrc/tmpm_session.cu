@@ -405,7 +405,30 @@ struct TmpmSession {
         return std::string(reinterpret_cast<const char *>(&k), sizeof k);
     }
 
+    // One segment replayed from its captured graph (captured now if new).
+    TmpmStatus run_segment_graph(const SimParams &sp, bool resort, uint32_t seg, bool apply_force) {
+        const std::string key = segment_key(sp, cur, resort, seg, apply_force);
+        auto it = seg_graphs.find(key);
+        cudaError_t e;
+        if (it == seg_graphs.end()) {
+            if (seg_graphs.size() >= 16) drop_graphs();
+            cudaGraph_t g = nullptr;
+            if ((e = cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal)))
+                return cuda_fail(e, "cudaStreamBeginCapture");
+            launch_segment(sp, cur, resort, seg, apply_force);
+            if ((e = cudaStreamEndCapture(stream, &g))) return cuda_fail(e, "cudaStreamEndCapture");
+            cudaGraphExec_t exec = nullptr;
+            e = cudaGraphInstantiate(&exec, g, 0);
+            cudaGraphDestroy(g);
+            if (e) return cuda_fail(e, "cudaGraphInstantiate");
+            it = seg_graphs.emplace(key, exec).first;
+        }
+        if ((e = cudaGraphLaunch(it->second, stream))) return cuda_fail(e, "cudaGraphLaunch");
+        return TMPM_OK;
+    }
+
     // Queue `steps` resident substeps on the stream (encode_prepared, gpu.rs:1729-1777).
+    // With `kernel_ms`, each kernel is timed with CUDA events (bench hook).
     TmpmStatus enqueue(uint32_t steps, double dt, bool resident, bool with_reactions, std::vector<float> *kernel_ms) {
         if (n_dev == 0) return TMPM_OK;
         SimParams sp = sim_params(dt, resident);
@@ -434,91 +457,73 @@ struct TmpmSession {
         // with a G2P-only transfer (the fused one keeps v and C in registers)
         // and the next opens with re-sort, table clear and P2G.
         const uint32_t interval = options.resort_interval ? options.resort_interval : kResortSubsteps;
-        uint32_t done = 0;
         // Plastic and CPIC variants run the default shape only.
         const bool tunable = !has_plastic && !sp.cpic;
-        while (done < steps) {
-        const int config = tunable ? tuner.config(big_blocks_ok, false) : 0;
-        const int shape = config_shape(config), bs = config_block_shift(config);
-        sp.shape = shape;
-        sp.block_shift = bs;
-        // the rows are re-sorted (and re-interleaved) when the shape changes
-        const bool resort_now = since_resort >= interval || shape != stored_shape;
-        const uint32_t seg = std::min<uint32_t>(steps - done, resort_now ? interval : interval - since_resort);
-        const bool apply_force = done == 0 && force_dirty;
-        // Replay a captured graph for a segment long enough to be worth it,
-        // outside per-kernel timing and tuning trials; otherwise launch.
-        const bool graph = kernel_ms == nullptr && !(tunable && tuner.tuning()) && seg >= kGraphMinSubsteps;
-        if (graph) {
-            const std::string key = segment_key(sp, cur, resort_now, seg, apply_force);
-            auto it = seg_graphs.find(key);
-            if (it == seg_graphs.end()) {
-                if (seg_graphs.size() >= 16) drop_graphs();
-                cudaGraph_t g = nullptr;
-                cudaError_t e;
-                if ((e = cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal)))
-                    return cuda_fail(e, "cudaStreamBeginCapture");
-                launch_segment(sp, cur, resort_now, seg, apply_force);
-                if ((e = cudaStreamEndCapture(stream, &g))) return cuda_fail(e, "cudaStreamEndCapture");
-                cudaGraphExec_t exec = nullptr;
-                e = cudaGraphInstantiate(&exec, g, 0);
-                cudaGraphDestroy(g);
-                if (e) return cuda_fail(e, "cudaGraphInstantiate");
-                it = seg_graphs.emplace(key, exec).first;
+        TmpmStatus st = TMPM_OK;
+        for (uint32_t done = 0; done < steps && st == TMPM_OK;) {
+            const int config = tunable ? tuner.config(big_blocks_ok, false) : 0;
+            const int shape = config_shape(config), bs = config_block_shift(config);
+            sp.shape = shape;
+            sp.block_shift = bs;
+            // the rows are re-sorted (and re-interleaved) when the shape changes
+            const bool resort = since_resort >= interval || shape != stored_shape;
+            const uint32_t seg = std::min<uint32_t>(steps - done, resort ? interval : interval - since_resort);
+            const bool apply_force = done == 0 && force_dirty;
+            // Replay a captured graph for a segment long enough to be worth it,
+            // outside per-kernel timing and tuning trials; otherwise launch.
+            if (kernel_ms == nullptr && !(tunable && tuner.tuning()) && seg >= kGraphMinSubsteps) {
+                st = run_segment_graph(sp, resort, seg, apply_force);
+            } else {
+                // launch_segment's kernels one by one, timed with `kernel_ms`
+                if (resort) {
+                    tick(0);
+                    ParticleSoA src = soa();
+                    ParticleSoA dst = pbuf[cur ^ 1].view(force.ptr, std::max<size_t>(world.n, 1));
+                    SortBuffers sb = sort_buffers();
+                    launch_resort(src, dst, n_dev, n_dev, classes.ptr, sp, sb, stream);
+                    tock(4);
+                }
+                if (tunable) tuner.begin(config, stream);
+                GridTable g[2];
+                grid_views(g, bs);
+                const ParticleSoA P = pbuf[resort ? cur ^ 1 : cur].view(force.ptr, std::max<size_t>(world.n, 1));
+                tick(0);
+                launch_clear_table(g[0], g[1], bs, stream);
+                launch_transfer(kModeP2G, P, n_dev, classes.ptr, g[1], g[0], sp, dev_obstacles.ptr, dev_planes.ptr,
+                                reactions.ptr, status.ptr, cta_cache.ptr, stream);
+                tock(0);
+                for (uint32_t k = 0; k < seg; ++k) {
+                    const GridTable &gc = g[k & 1], &gn = g[(k + 1) & 1];
+                    tick(0);
+                    launch_grid_update(gc, gn, sp, dev_obstacles.ptr, dev_planes.ptr, reactions.ptr, status.ptr,
+                                       stream);
+                    tock(1);
+                    SimParams spk = sp;
+                    spk.apply_force = (apply_force && k == 0) ? 1 : 0;
+                    const bool last = k + 1 == seg;
+                    tick(0);
+                    launch_transfer(last ? kModeG2P : kModeG2P2G, P, n_dev, classes.ptr, gc, gn, spk,
+                                    dev_obstacles.ptr, dev_planes.ptr, reactions.ptr, status.ptr, cta_cache.ptr,
+                                    stream);
+                    tock(last ? 3 : 2);
+                    if (apply_force && k == 0) cudaMemsetAsync(force.ptr, 0, sizeof(float) * force.count, stream);
+                }
+                if (tunable) tuner.end(static_cast<double>(n_dev) * seg, stream);
             }
-            cudaError_t e = cudaGraphLaunch(it->second, stream);
-            if (e) return cuda_fail(e, "cudaGraphLaunch");
-            if (resort_now) {
+            if (resort) {
                 cur ^= 1;
                 since_resort = 0;
                 stored_shape = shape;
             }
-        } else {
-        if (resort_now) {
-            tick(0);
-            ParticleSoA src = soa();
-            ParticleSoA dst = pbuf[cur ^ 1].view(force.ptr, std::max<size_t>(world.n, 1));
-            SortBuffers sb = sort_buffers();
-            launch_resort(src, dst, n_dev, n_dev, classes.ptr, sp, sb, stream);
-            cur ^= 1;
-            since_resort = 0;
-            stored_shape = shape;
-            tock(4);
-        }
-        if (tunable) tuner.begin(config, stream);
-        GridTable g[2];
-        grid_views(g, bs);
-        ParticleSoA P = soa();
-        tick(0);
-        launch_clear_table(g[0], g[1], bs, stream);
-        launch_transfer(kModeP2G, P, n_dev, classes.ptr, g[1], g[0], sp, dev_obstacles.ptr, dev_planes.ptr,
-                        reactions.ptr, status.ptr, cta_cache.ptr, stream);
-        tock(0);
-        for (uint32_t s = 0; s < seg; ++s) {
-            const GridTable &gc = g[s & 1], &gn = g[(s + 1) & 1];
-            tick(0);
-            launch_grid_update(gc, gn, sp, dev_obstacles.ptr, dev_planes.ptr, reactions.ptr, status.ptr, stream);
-            tock(1);
-            SimParams spk = sp;
-            const bool first = s == 0;
-            spk.apply_force = (first && apply_force) ? 1 : 0;
-            bool last = s + 1 == seg;
-            tick(0);
-            launch_transfer(last ? kModeG2P : kModeG2P2G, P, n_dev, classes.ptr, gc, gn, spk, dev_obstacles.ptr,
-                            dev_planes.ptr, reactions.ptr, status.ptr, cta_cache.ptr, stream);
-            tock(last ? 3 : 2);
-            if (first && apply_force) cudaMemsetAsync(force.ptr, 0, sizeof(float) * force.count, stream);
-        }
-        }
-        if (apply_force) force_dirty = false;
-        if (tunable) tuner.end(static_cast<double>(n_dev) * seg, stream);
-        since_resort += seg;
-        done += seg;
+            if (apply_force) force_dirty = false;
+            since_resort += seg;
+            done += seg;
         }
         if (kernel_ms) {
             cudaEventDestroy(ev[0]);
             cudaEventDestroy(ev[1]);
         }
+        if (st != TMPM_OK) return st;
         cudaError_t e = cudaGetLastError();
         if (e) return cuda_fail(e, "kernel launch");
         return TMPM_OK;
