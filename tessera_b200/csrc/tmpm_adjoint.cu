@@ -446,11 +446,74 @@ struct TmpmAdjoint {
     DevBuf<uint32_t> err;
     bool have_forward = false;
     std::string last_error;
+    // The forward and adjoint sweeps (fixed launches over fixed buffers) are
+    // captured as CUDA graphs on first use and replayed afterwards.
+    cudaGraphExec_t fwd_exec = nullptr, bwd_exec = nullptr;
 
     ~TmpmAdjoint() {
         if (stream) {
             cudaStreamSynchronize(stream);
             cudaStreamDestroy(stream);
+        }
+        if (fwd_exec) cudaGraphExecDestroy(fwd_exec);
+        if (bwd_exec) cudaGraphExecDestroy(bwd_exec);
+    }
+
+    // Capture `launch` (stream work only) into *exec once, then launch it.
+    template <typename Fn>
+    cudaError_t replay(cudaGraphExec_t *exec, Fn launch) {
+        cudaError_t e;
+        if (!*exec) {
+            cudaGraph_t g = nullptr;
+            if ((e = cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal))) return e;
+            launch();
+            if ((e = cudaStreamEndCapture(stream, &g))) return e;
+            e = cudaGraphInstantiate(exec, g, 0);
+            cudaGraphDestroy(g);
+            if (e) {
+                *exec = nullptr;
+                return e;
+            }
+        }
+        return cudaGraphLaunch(*exec, stream);
+    }
+
+    // The forward sweep: `substeps` substeps from seg[0] ping-ponging with
+    // seg[1], a checkpoint every `every`.
+    void forward_sweep() {
+        float *cur = seg.ptr, *nxt = seg.ptr + state_floats();
+        for (uint32_t s = 0; s < substeps; ++s) {
+            if (s % every == 0)
+                cudaMemcpyAsync(ckpt.ptr + (s / every) * state_floats(), cur, sizeof(float) * state_floats(),
+                                cudaMemcpyDeviceToDevice, stream);
+            substep(cur, nxt);
+            std::swap(cur, nxt);
+        }
+    }
+
+    // The adjoint sweep from adj[0] (the loss gradient of the final state),
+    // segment by segment from the last checkpoint back; the initial-state
+    // adjoint ends in adj[substeps & 1].
+    void backward_sweep() {
+        int a = 0;
+        const uint32_t segments = (substeps + every - 1) / every;
+        for (int sg = static_cast<int>(segments) - 1; sg >= 0; --sg) {
+            const uint32_t s0 = sg * every, s1 = std::min(substeps, s0 + every);
+            // replay the segment: seg[j] = state at substep s0 + j
+            cudaMemcpyAsync(seg.ptr, ckpt.ptr + sg * state_floats(), sizeof(float) * state_floats(),
+                            cudaMemcpyDeviceToDevice, stream);
+            for (uint32_t s = s0; s + 1 < s1; ++s)
+                substep(seg.ptr + (s - s0) * state_floats(), seg.ptr + (s - s0 + 1) * state_floats());
+            for (int s = static_cast<int>(s1) - 1; s >= static_cast<int>(s0); --s) {
+                const float *S = seg.ptr + (s - s0) * state_floats();
+                p2g_grid(S);
+                cudaMemsetAsync(gvb.ptr, 0, sizeof(float4) * nodes, stream);
+                k_g2p_back<<<blocks_n(), 256, 0, stream>>>(P, consts(), S, gv.ptr, adj[a].ptr, part.ptr, gvb.ptr);
+                k_grid_back<<<blocks_nodes(), 256, 0, stream>>>(P, grid.ptr, gv.ptr, gvb.ptr, nodes);
+                k_p2g_back<<<blocks_n(), 256, 0, stream>>>(P, consts(), S, E.ptr, gvb.ptr, part.ptr, adj[a ^ 1].ptr,
+                                                           Ebar.ptr);
+                a ^= 1;
+            }
         }
     }
     TmpmStatus fail(TmpmStatus st, const std::string &msg) {
@@ -517,15 +580,10 @@ struct TmpmAdjoint {
             (e = cudaMemcpyAsync(seg.ptr, S0.data(), sizeof(float) * state_floats(), cudaMemcpyHostToDevice, stream)) ||
             (e = cudaMemsetAsync(err.ptr, 0, sizeof(uint32_t), stream)))
             return cuda_fail(e, "adjoint upload");
-        // seg holds two ping-pong states during the forward
-        float *cur = seg.ptr, *nxt = seg.ptr + state_floats();
-        for (uint32_t s = 0; s < substeps; ++s) {
-            if (s % every == 0)
-                cudaMemcpyAsync(ckpt.ptr + (s / every) * state_floats(), cur, sizeof(float) * state_floats(),
-                                cudaMemcpyDeviceToDevice, stream);
-            substep(cur, nxt);
-            std::swap(cur, nxt);
-        }
+        // seg holds two ping-pong states during the forward; the final state is
+        // in the first of them after an even number of substeps
+        if ((e = replay(&fwd_exec, [&]() { forward_sweep(); }))) return cuda_fail(e, "adjoint forward");
+        const float *cur = (substeps % 2 == 0) ? seg.ptr : seg.ptr + state_floats();
         std::vector<float> out(6 * n);
         if ((e = cudaMemcpyAsync(out.data(), cur, sizeof(float) * 6 * n, cudaMemcpyDeviceToHost, stream)) ||
             (e = cudaStreamSynchronize(stream)))
@@ -557,26 +615,9 @@ struct TmpmAdjoint {
             (e = cudaMemsetAsync(Ebar.ptr, 0, sizeof(float) * n, stream)) ||
             (e = cudaMemsetAsync(err.ptr, 0, sizeof(uint32_t), stream)))
             return cuda_fail(e, "adjoint upload");
-        int a = 0;
-        const uint32_t segments = (substeps + every - 1) / every;
-        for (int sg = static_cast<int>(segments) - 1; sg >= 0; --sg) {
-            const uint32_t s0 = sg * every, s1 = std::min(substeps, s0 + every);
-            // replay the segment: seg[j] = state at substep s0 + j
-            cudaMemcpyAsync(seg.ptr, ckpt.ptr + sg * state_floats(), sizeof(float) * state_floats(),
-                            cudaMemcpyDeviceToDevice, stream);
-            for (uint32_t s = s0; s + 1 < s1; ++s)
-                substep(seg.ptr + (s - s0) * state_floats(), seg.ptr + (s - s0 + 1) * state_floats());
-            for (int s = static_cast<int>(s1) - 1; s >= static_cast<int>(s0); --s) {
-                const float *S = seg.ptr + (s - s0) * state_floats();
-                p2g_grid(S);
-                cudaMemsetAsync(gvb.ptr, 0, sizeof(float4) * nodes, stream);
-                k_g2p_back<<<blocks_n(), 256, 0, stream>>>(P, consts(), S, gv.ptr, adj[a].ptr, part.ptr, gvb.ptr);
-                k_grid_back<<<blocks_nodes(), 256, 0, stream>>>(P, grid.ptr, gv.ptr, gvb.ptr, nodes);
-                k_p2g_back<<<blocks_n(), 256, 0, stream>>>(P, consts(), S, E.ptr, gvb.ptr, part.ptr, adj[a ^ 1].ptr,
-                                                           Ebar.ptr);
-                a ^= 1;
-            }
-        }
+        // the parity of the final adj buffer: one flip per substep
+        const int a = static_cast<int>(substeps & 1u);
+        if ((e = replay(&bwd_exec, [&]() { backward_sweep(); }))) return cuda_fail(e, "adjoint backward");
         std::vector<float> vb(3 * n), eb(n);
         if ((e = cudaMemcpyAsync(vb.data(), adj[a].ptr + 3 * n, sizeof(float) * 3 * n, cudaMemcpyDeviceToHost, stream)) ||
             (e = cudaMemcpyAsync(eb.data(), Ebar.ptr, sizeof(float) * n, cudaMemcpyDeviceToHost, stream)) ||
