@@ -29,7 +29,9 @@
 // through one pinned buffer that the batch keeps and reuses.
 
 #include <chrono>
+#include <condition_variable>
 #include <cstdio>
+#include <deque>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -207,6 +209,14 @@ struct TmpmBatch {
     std::map<GraphKey, cudaGraphExec_t> graphs;
 
     ~TmpmBatch() {
+        if (upload_worker.joinable()) {
+            {
+                std::lock_guard<std::mutex> lk(up_mu);
+                up_stop = true;
+            }
+            up_cv.notify_all();
+            upload_worker.join();
+        }
         if (upload_stream) cudaStreamSynchronize(upload_stream);
         if (stream) cudaStreamSynchronize(stream);
         if (upload_done) cudaEventDestroy(upload_done);
@@ -401,6 +411,47 @@ struct TmpmBatch {
         const void *src;
         size_t bytes;
     };
+    // Admission copies run on a worker thread, so that the thread admitting
+    // scenes returns at once (the copies overlap the batch in flight and the
+    // caller's own work); the next submit waits for them (join_uploads).
+    struct UploadJob {
+        std::vector<CopyPiece> pieces;
+        size_t id;
+    };
+    std::thread upload_worker;
+    std::mutex up_mu;
+    std::condition_variable up_cv;
+    std::deque<UploadJob> up_jobs;
+    bool up_busy = false, up_stop = false;
+    cudaError_t up_error = cudaSuccess;
+
+    void upload_loop() {
+        cudaSetDevice(device);
+        std::unique_lock<std::mutex> lk(up_mu);
+        for (;;) {
+            up_cv.wait(lk, [&] { return up_stop || !up_jobs.empty(); });
+            if (up_jobs.empty()) return;  // stopping with nothing left
+            UploadJob job = std::move(up_jobs.front());
+            up_jobs.pop_front();
+            up_busy = true;
+            lk.unlock();
+            cudaError_t e = copy_h2d(job.pieces, upload_stream);
+            if (e == cudaSuccess) e = cudaMemsetAsync(scene_status.ptr + job.id, 0, sizeof(uint32_t), upload_stream);
+            lk.lock();
+            if (e != cudaSuccess && up_error == cudaSuccess) up_error = e;
+            up_busy = false;
+            up_cv.notify_all();
+        }
+    }
+
+    // Wait until the worker has issued every queued copy; its first error.
+    cudaError_t drain_uploads() {
+        std::unique_lock<std::mutex> lk(up_mu);
+        up_cv.wait(lk, [&] { return up_jobs.empty() && !up_busy; });
+        const cudaError_t e = up_error;
+        up_error = cudaSuccess;
+        return e;
+    }
     cudaError_t copy_h2d(const std::vector<CopyPiece> &pieces, cudaStream_t st) {
         cudaError_t e;
         bool pinned = true;
@@ -466,17 +517,16 @@ struct TmpmBatch {
         return cudaSuccess;
     }
 
-    cudaError_t copy_scene_rows(size_t id, cudaStream_t st) {
+    // The copies that put scene `id`'s staged rows at rows [n_phys, n_phys + m)
+    // of the buffer the next batch re-sorts from; assigns those rows.
+    std::vector<CopyPiece> scene_pieces(size_t id) {
         TmpmPreparedScene &p = *scenes[id].staged;
         const size_t m = p.m, stride = std::max<size_t>(m, 1);
         const size_t pc = pbuf[cur].cap;
         const ParticleBuffers &pb = pbuf[cur];
-        cudaError_t e = cudaSuccess;
+        std::vector<CopyPiece> pieces;
         if (m) {
-            // host rows: 27 f32 component rows, class, world index (stride m);
-            // device rows: the same order across the fields (pitch cap)
             const float *hb = row_base(p.rows);
-            std::vector<CopyPiece> pieces;
             auto rows = [&](float *dst, int first, int count) {
                 for (int r = 0; r < count; ++r)
                     pieces.push_back({dst + r * pc + n_phys, hb + (first + r) * stride, m * 4});
@@ -488,12 +538,17 @@ struct TmpmBatch {
             rows(pb.pl.ptr, 24, 3);
             pieces.push_back({pb.cls.ptr + n_phys, row_cls(p.rows, stride), m * 4});
             pieces.push_back({pb.widx.ptr + n_phys, row_widx(p.rows, stride), m * 4});
-            if ((e = copy_h2d(pieces, st))) return e;
         }
-        if ((e = cudaMemsetAsync(scene_status.ptr + id, 0, sizeof(uint32_t), st))) return e;
         scenes[id].dev_offset = n_phys;
         n_phys += m;
-        return cudaSuccess;
+        return pieces;
+    }
+
+    // Scene `id`'s staged rows to the device on `st` (see scene_pieces).
+    cudaError_t copy_scene_rows(size_t id, cudaStream_t st) {
+        const cudaError_t e = copy_h2d(scene_pieces(id), st);
+        if (e != cudaSuccess) return e;
+        return cudaMemsetAsync(scene_status.ptr + id, 0, sizeof(uint32_t), st);
     }
 
     // Copy an admitted scene's rows now, on the upload stream, if the
@@ -503,9 +558,14 @@ struct TmpmBatch {
     // rows stay staged and the next submit grows the buffers and copies them.
     TmpmStatus upload_early(size_t id) {
         if (n_phys + scenes[id].staged->m > pbuf[cur].cap) return TMPM_OK;
-        cudaError_t e;
-        if ((e = copy_scene_rows(id, upload_stream))) return cuda_fail(e, "scene upload");
-        early_uploads.push_back(std::move(scenes[id].staged));
+        UploadJob job{scene_pieces(id), id};
+        if (!upload_worker.joinable()) upload_worker = std::thread([this] { upload_loop(); });
+        {
+            std::lock_guard<std::mutex> lk(up_mu);
+            up_jobs.push_back(std::move(job));
+        }
+        up_cv.notify_all();
+        early_uploads.push_back(std::move(scenes[id].staged));  // rows stay alive until the copies are done
         uploads_open = true;
         return TMPM_OK;
     }
@@ -514,6 +574,7 @@ struct TmpmBatch {
     TmpmStatus join_uploads() {
         if (!uploads_open) return TMPM_OK;
         cudaError_t e;
+        if ((e = drain_uploads())) return cuda_fail(e, "scene upload");
         if ((e = cudaEventRecord(upload_done, upload_stream)) || (e = cudaStreamWaitEvent(stream, upload_done, 0)))
             return cuda_fail(e, "scene upload");
         for (auto &p : early_uploads) in_flight_uploads.push_back(std::move(p));
@@ -1005,6 +1066,16 @@ size_t tmpm_scene_prepared_bytes(const TmpmPreparedScene *p) {
     return p->m * kBytesPerRow + 16 * p->blocks * kBytesPerPoolBlock + extra;
 }
 
+// Reads of finished scenes run beside the batch in flight; at the highest
+// stream priority their small un-sort kernel is scheduled ahead of the
+// batch's queued CTAs instead of waiting for them.
+static cudaError_t create_read_stream(cudaStream_t *s) {
+    int least = 0, greatest = 0;
+    cudaError_t e = cudaDeviceGetStreamPriorityRange(&least, &greatest);
+    if (e != cudaSuccess) return e;
+    return cudaStreamCreateWithPriority(s, cudaStreamNonBlocking, greatest);
+}
+
 TmpmStatus tmpm_batch_create(const TmpmBatchOptions *options, TmpmBatch **out) {
     if (!out) {
         g_last_error = "null argument";
@@ -1018,7 +1089,7 @@ TmpmStatus tmpm_batch_create(const TmpmBatchOptions *options, TmpmBatch **out) {
     b->tuner.reset(b->options.launch_shape);
     cudaError_t e;
     if ((e = cudaSetDevice(b->device)) || (e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking)) ||
-        (e = cudaStreamCreateWithFlags(&b->read_stream, cudaStreamNonBlocking)) ||
+        (e = create_read_stream(&b->read_stream)) ||
         (e = cudaStreamCreateWithFlags(&b->upload_stream, cudaStreamNonBlocking)) ||
         (e = cudaEventCreateWithFlags(&b->upload_done, cudaEventDisableTiming)) ||
         (e = cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming)) || (e = cudaEventCreate(&b->t_begin)) ||

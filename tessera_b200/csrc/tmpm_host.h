@@ -641,6 +641,10 @@ inline PoolPlan pool_plan(size_t home4, size_t home8, uint64_t fixed_blocks, uin
 // first request).
 struct LaunchTuner {
     static constexpr int kRounds = 2;
+    // Trials this long (particle-substeps; ~0.15 s of device time) are measured
+    // well enough in one round: the second is skipped.
+    static constexpr double kOneRoundWork = 1073741824.0;
+    int rounds = kRounds;
     int fixed = -1;       // >= 0: the caller's configuration; no tuning
     int chosen = -1;      // the tuned configuration, -1 while trials are outstanding
     int candidates = 0;   // configurations under trial (0: not yet started)
@@ -675,6 +679,7 @@ struct LaunchTuner {
         fixed = option == 0 ? -1 : (option <= static_cast<uint32_t>(kNumLaunchConfigs) ? static_cast<int>(option) - 1 : 0);
         chosen = fixed;
         candidates = 0;
+        rounds = kRounds;
         issued = read = 0;
         for (double &b : best) b = std::numeric_limits<double>::infinity();
         for (int &r : rounds_read) r = 0;
@@ -685,7 +690,7 @@ struct LaunchTuner {
         return (t / candidates) % 2 == 0 ? pos : candidates - 1 - pos;
     }
     bool tuning() const { return chosen < 0; }
-    int trials_total() const { return kRounds * candidates; }
+    int trials_total() const { return rounds * candidates; }
     void poll() {
         while (read < static_cast<int>(trials.size()) && read != open) {
             Trial &t = trials[read];
@@ -748,6 +753,7 @@ struct LaunchTuner {
     }
     void end(double work, cudaStream_t stream) {
         if (open < 0) return;
+        if (issued == 1 && work >= kOneRoundWork) rounds = 1;
         trials[open].work = work;
         cudaEventRecord(trials[open].b, stream);
         open = -1;

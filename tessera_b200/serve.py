@@ -98,7 +98,7 @@ class Server:
     `device_bytes()` (tessera_b200.batch.PreparedScene by default)."""
 
     def __init__(self, batch=None, hbm_budget: float = 120e9, chunk: int = 32, lookahead: int = 8,
-                 prepare_workers: int = 4, keep_outputs: bool = False, max_scenes: int = 256, prepare=None,
+                 prepare_workers: int = 1, keep_outputs: bool = False, max_scenes: int = 256, prepare=None,
                  clock=time.perf_counter):
         if batch is None or prepare is None:
             from .batch import Batch, PreparedScene
