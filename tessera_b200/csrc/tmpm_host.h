@@ -4,11 +4,17 @@
 // pinned buffers, and the f32 packing of a world for upload.
 #pragma once
 
+#include <immintrin.h>
+
 #include <algorithm>
 #include <atomic>
 #include <cmath>
+#include <condition_variable>
+#include <cstdlib>
 #include <cstring>
+#include <functional>
 #include <limits>
+#include <mutex>
 #include <string>
 #include <thread>
 #include <unordered_map>
@@ -23,7 +29,152 @@ inline thread_local std::string g_last_error;  // reason reported by tmpm_last_e
 
 inline constexpr double kSyncTimeoutSeconds = 5.0;  // gpu.rs:1853-1862
 
-inline unsigned host_threads() { return std::max(1u, std::min(32u, std::thread::hardware_concurrency())); }
+// Host threads for the parallel host passes: the hardware threads (at most 32),
+// or TMPM_HOST_THREADS (1-32) when set, read once per process.
+inline unsigned host_threads() {
+    static const unsigned t = [] {
+        unsigned n = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+        if (const char *e = std::getenv("TMPM_HOST_THREADS")) {
+            const long v = std::strtol(e, nullptr, 10);
+            if (v >= 1 && v <= 32) n = static_cast<unsigned>(v);
+        }
+        return n;
+    }();
+    return t;
+}
+
+// ------------------------------------------------------ host memory traffic
+
+// Copy with non-temporal stores for the 16-byte-aligned middle: the destination
+// lines are written without first being read into the cache (no
+// read-for-ownership), a third of the traffic of a large state copy, and the
+// copy does not evict the data a pass is working on.  Short copies use memcpy.
+// A thread that stored this way calls stream_fence() before another thread or
+// a DMA engine reads the destination.
+inline void stream_copy(void *dst, const void *src, size_t bytes) {
+    char *d = static_cast<char *>(dst);
+    const char *s = static_cast<const char *>(src);
+    if (bytes < 256) {
+        std::memcpy(d, s, bytes);
+        return;
+    }
+    const size_t head = (16 - (reinterpret_cast<uintptr_t>(d) & 15)) & 15;
+    std::memcpy(d, s, head);
+    d += head;
+    s += head;
+    bytes -= head;
+    const size_t lines = bytes / 64;
+    for (size_t i = 0; i < lines; ++i, d += 64, s += 64) {
+        const __m128i a = _mm_loadu_si128(reinterpret_cast<const __m128i *>(s));
+        const __m128i b = _mm_loadu_si128(reinterpret_cast<const __m128i *>(s + 16));
+        const __m128i c = _mm_loadu_si128(reinterpret_cast<const __m128i *>(s + 32));
+        const __m128i e = _mm_loadu_si128(reinterpret_cast<const __m128i *>(s + 48));
+        _mm_stream_si128(reinterpret_cast<__m128i *>(d), a);
+        _mm_stream_si128(reinterpret_cast<__m128i *>(d + 16), b);
+        _mm_stream_si128(reinterpret_cast<__m128i *>(d + 32), c);
+        _mm_stream_si128(reinterpret_cast<__m128i *>(d + 48), e);
+    }
+    std::memcpy(d, s, bytes - 64 * lines);
+}
+
+// Zero `bytes` with non-temporal stores (see stream_copy).
+inline void stream_zero(void *dst, size_t bytes) {
+    char *d = static_cast<char *>(dst);
+    if (bytes < 256) {
+        std::memset(d, 0, bytes);
+        return;
+    }
+    const size_t head = (16 - (reinterpret_cast<uintptr_t>(d) & 15)) & 15;
+    std::memset(d, 0, head);
+    d += head;
+    bytes -= head;
+    const __m128i z = _mm_setzero_si128();
+    const size_t lines = bytes / 64;
+    for (size_t i = 0; i < lines; ++i, d += 64) {
+        _mm_stream_si128(reinterpret_cast<__m128i *>(d), z);
+        _mm_stream_si128(reinterpret_cast<__m128i *>(d + 16), z);
+        _mm_stream_si128(reinterpret_cast<__m128i *>(d + 32), z);
+        _mm_stream_si128(reinterpret_cast<__m128i *>(d + 48), z);
+    }
+    std::memset(d, 0, bytes - 64 * lines);
+}
+
+inline void stream_fence() { _mm_sfence(); }
+
+// Persistent workers for the parallel host passes (a pass over a few million
+// particles takes milliseconds, and creating and joining 16 threads for each
+// took ~0.23 ms).  One job runs at a time: the caller and the workers claim
+// chunk indices from a shared counter, so the caller alone can finish any job;
+// a caller that finds a job running (another thread, or a pass nested inside a
+// chunk) runs its own job on threads of its own instead of waiting.
+class HostPool {
+  public:
+    static HostPool &get() {
+        static HostPool *pool = new HostPool(host_threads() - 1);  // never destroyed: workers may outlive statics
+        return *pool;
+    }
+
+    // fn(c) for every c in [0, chunks), on the workers and the calling thread;
+    // false (nothing run) when another job holds the pool.
+    bool try_run(size_t chunks, const std::function<void(size_t)> &fn) {
+        std::unique_lock<std::mutex> run(run_mu_, std::try_to_lock);
+        if (!run.owns_lock()) return false;
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            job_ = &fn;
+            count_ = chunks;
+            next_.store(0, std::memory_order_relaxed);
+            completed_ = 0;
+            ++gen_;
+        }
+        cv_.notify_all();
+        const size_t did = drain(fn, chunks);
+        std::unique_lock<std::mutex> lk(mu_);
+        completed_ += did;
+        // every chunk done and no worker still between claiming and leaving
+        done_cv_.wait(lk, [&] { return completed_ == count_ && active_ == 0; });
+        job_ = nullptr;
+        return true;
+    }
+
+  private:
+    explicit HostPool(unsigned workers) {
+        for (unsigned w = 0; w < workers; ++w) std::thread([this] { loop(); }).detach();
+    }
+
+    size_t drain(const std::function<void(size_t)> &fn, size_t chunks) {
+        size_t did = 0;
+        for (size_t c; (c = next_.fetch_add(1, std::memory_order_relaxed)) < chunks; ++did) fn(c);
+        return did;
+    }
+
+    void loop() {
+        uint64_t seen = 0;
+        std::unique_lock<std::mutex> lk(mu_);
+        for (;;) {
+            cv_.wait(lk, [&] { return gen_ != seen; });
+            seen = gen_;
+            if (!job_) continue;
+            const std::function<void(size_t)> *fn = job_;
+            const size_t chunks = count_;
+            ++active_;
+            lk.unlock();
+            const size_t did = drain(*fn, chunks);
+            lk.lock();
+            completed_ += did;
+            --active_;
+            if (completed_ == count_ && active_ == 0) done_cv_.notify_all();
+        }
+    }
+
+    std::mutex run_mu_, mu_;
+    std::condition_variable cv_, done_cv_;
+    const std::function<void(size_t)> *job_ = nullptr;
+    size_t count_ = 0, completed_ = 0;
+    unsigned active_ = 0;
+    uint64_t gen_ = 0;
+    std::atomic<size_t> next_{0};
+};
 
 // Run fn(chunk, begin, end) over [0, n) split into contiguous chunks, one per host thread.
 template <typename Fn>
@@ -33,13 +184,12 @@ inline void parallel_chunks(size_t n, Fn fn, size_t min_per_chunk = 32768) {
         fn(size_t(0), size_t(0), n);
         return;
     }
-    size_t per = (n + chunks - 1) / chunks;
+    const size_t per = (n + chunks - 1) / chunks;
+    chunks = (n + per - 1) / per;
+    const std::function<void(size_t)> job = [&](size_t c) { fn(c, c * per, std::min(n, c * per + per)); };
+    if (HostPool::get().try_run(chunks, job)) return;
     std::vector<std::thread> pool;
-    for (size_t c = 0; c < chunks; ++c) {
-        size_t a = c * per, b = std::min(n, a + per);
-        if (a >= b) break;
-        pool.emplace_back([=]() { fn(c, a, b); });
-    }
+    for (size_t c = 0; c < chunks; ++c) pool.emplace_back([&, c]() { job(c); });
     for (auto &t : pool) t.join();
 }
 
@@ -173,14 +323,19 @@ struct HostWorld {
     }
 
     void store(TmpmParticleArrays &a) const {
-        parallel_for(n, [&](size_t lo, size_t hi) { store_range(a, lo, hi); });
+        parallel_for(n, [&](size_t lo, size_t hi) {
+            store_range(a, lo, hi);
+            stream_fence();
+        });
     }
 
-    // Field by field, only the fields `a` asks for.
+    // Field by field, only the fields `a` asks for, with streaming stores (the
+    // caller's arrays are written, not read: no read-for-ownership traffic);
+    // the caller fences before the arrays are read on another thread.
     void store_range(TmpmParticleArrays &a, size_t lo, size_t hi) const {
         const size_t m = hi - lo;
         auto copy = [&](auto *dst, const auto *src, int width) {
-            if (dst) std::memcpy(dst + width * lo, src + width * lo, sizeof(*dst) * width * m);
+            if (dst) stream_copy(dst + width * lo, src + width * lo, sizeof(*dst) * width * m);
         };
         copy(a.position, pos.data(), 3);
         copy(a.velocity, vel.data(), 3);
@@ -911,13 +1066,22 @@ struct PackNoHook {
     bool operator()(size_t, size_t, size_t) const { return true; }
 };
 
+// Nothing to do when a range of eager rows is complete (see pack_world's `ready`).
+struct PackNoRows {
+    void operator()(size_t, size_t) const {}
+};
+
 // With `eager_rows`, the f32 rows are written in the first pass, at each
 // particle's world index, while its values are in cache (the target comes from
 // alloc(world.n)); when every particle is enabled those are the final
-// positions and the second pass writes only the class and index rows.
-template <typename Alloc, typename Before = PackNoHook>
+// positions and the second pass writes only the class and index rows.  Each
+// pass-1 thread calls `ready(begin, end)` whenever the eager rows of world
+// indices [begin, end) are written (about every 32k particles), so they can be
+// copied on while the pass goes on; they are final only if every particle
+// turns out enabled and the pack succeeds.
+template <typename Alloc, typename Before = PackNoHook, typename Ready = PackNoRows>
 PackResult pack_world(const HostWorld &world, float inv_h, uint32_t ns_high, ClassTable &ct, Alloc alloc,
-                      Before before = Before(), bool eager_rows = false) {
+                      Before before = Before(), bool eager_rows = false, Ready ready = Ready()) {
     PackResult res;
     const size_t N = world.n;
     PackTarget tg0;
@@ -1071,7 +1235,8 @@ PackResult pack_world(const HostWorld &world, float inv_h, uint32_t ns_high, Cla
         // runs first, so the particles are checked and packed while in cache;
         // after an error of this pass the rest of the chunk still goes through
         // `before`, whose own errors come first
-        constexpr size_t kBlock = 256;
+        constexpr size_t kBlock = 256, kReadyRows = 32768;
+        size_t handed = lo;  // eager rows [lo, handed) went to `ready`
         for (size_t a0 = lo; a0 < hi; a0 += kBlock) {
             const size_t b0 = std::min(hi, a0 + kBlock);
             if (!before(c, a0, b0)) {
@@ -1079,6 +1244,10 @@ PackResult pack_world(const HostWorld &world, float inv_h, uint32_t ns_high, Cla
                 return;
             }
             for (size_t i = a0; i < b0 && o.first_bad == std::numeric_limits<size_t>::max(); ++i) one(i);
+            if (eager && o.first_bad == std::numeric_limits<size_t>::max() && (b0 - handed >= kReadyRows || b0 == hi)) {
+                ready(handed, b0);
+                handed = b0;
+            }
         }
         std::sort(o.blocks.begin(), o.blocks.end());
         o.blocks.erase(std::unique(o.blocks.begin(), o.blocks.end()), o.blocks.end());

@@ -170,8 +170,15 @@ struct TmpmSession {
         }
 
         // Validate and pack the world straight into pinned staging (stride `cap`).
+        // When the device rows already have this capacity, each range of rows
+        // the packing completes is copied to the device at once, so the copy
+        // runs while the rest is packed (the rows are final when every
+        // particle is enabled; otherwise, or after a failure, the full copies
+        // below or the re-upload overwrite them in stream order).
         ClassTable ct;
         size_t cap = 256;
+        bool early = false;
+        std::atomic<int> early_err{0};
         PackResult pr = pack_world(
             world, inv_h, 0u, ct,
             [&](size_t n_enabled) {
@@ -183,9 +190,26 @@ struct TmpmSession {
                 tg.cls = reinterpret_cast<uint32_t *>(tg.base + 27 * cap);
                 tg.widx = tg.cls + cap;
                 tg.stride = cap;
+                early = n_enabled == world.n && pbuf[0].cap == cap && pbuf[1].cap == cap;
                 return tg;
             },
-            [&](size_t c, size_t a, size_t b) { return !before || (*before)(c, a, b); }, true);
+            [&](size_t c, size_t a, size_t b) { return !before || (*before)(c, a, b); }, true,
+            [&](size_t lo, size_t hi) {
+                if (!early) return;
+                const float *h = static_cast<const float *>(upload_staging.ptr);
+                const ParticleBuffers &pb = pbuf[0];
+                const size_t pitch = cap * sizeof(float), w = (hi - lo) * sizeof(float);
+                const struct {
+                    float *dst;
+                    int row, rows;
+                } parts[5] = {{pb.x.ptr, 0, 3}, {pb.v.ptr, 3, 3}, {pb.C.ptr, 6, 9}, {pb.F.ptr, 15, 9}, {pb.pl.ptr, 24, 3}};
+                cudaError_t e = cudaSetDevice(device);
+                for (int k = 0; k < 5 && e == cudaSuccess; ++k)
+                    e = cudaMemcpy2DAsync(parts[k].dst + lo, pitch, h + parts[k].row * cap + lo, pitch, w, parts[k].rows,
+                                          cudaMemcpyHostToDevice, stream);
+                if (e != cudaSuccess) early_err = static_cast<int>(e);
+            });
+        if (early_err.load()) return cuda_fail(static_cast<cudaError_t>(early_err.load()), "cudaMemcpy2DAsync rows");
         if (pr.st != TMPM_OK) {
             if (pr.st == TMPM_ERR_DEVICE && pr.enabled > static_cast<size_t>(std::numeric_limits<int>::max() / 2))
                 return fail(TMPM_ERR_CAPACITY, "too many particles for one session");
@@ -277,11 +301,13 @@ struct TmpmSession {
         cur = 0;
         ParticleBuffers &pb = pbuf[0];
         if (n_dev) {
-            cudaMemcpyAsync(pb.x.ptr, hx, sizeof(float) * 3 * cap, cudaMemcpyHostToDevice, stream);
-            cudaMemcpyAsync(pb.v.ptr, hv, sizeof(float) * 3 * cap, cudaMemcpyHostToDevice, stream);
-            cudaMemcpyAsync(pb.C.ptr, hC, sizeof(float) * 9 * cap, cudaMemcpyHostToDevice, stream);
-            cudaMemcpyAsync(pb.F.ptr, hF, sizeof(float) * 9 * cap, cudaMemcpyHostToDevice, stream);
-            cudaMemcpyAsync(pb.pl.ptr, hpl, sizeof(float) * 3 * cap, cudaMemcpyHostToDevice, stream);
+            if (!(early && n_enabled == world.n)) {  // else the rows are on their way already
+                cudaMemcpyAsync(pb.x.ptr, hx, sizeof(float) * 3 * cap, cudaMemcpyHostToDevice, stream);
+                cudaMemcpyAsync(pb.v.ptr, hv, sizeof(float) * 3 * cap, cudaMemcpyHostToDevice, stream);
+                cudaMemcpyAsync(pb.C.ptr, hC, sizeof(float) * 9 * cap, cudaMemcpyHostToDevice, stream);
+                cudaMemcpyAsync(pb.F.ptr, hF, sizeof(float) * 9 * cap, cudaMemcpyHostToDevice, stream);
+                cudaMemcpyAsync(pb.pl.ptr, hpl, sizeof(float) * 3 * cap, cudaMemcpyHostToDevice, stream);
+            }
             cudaMemcpyAsync(pb.cls.ptr, hcls, sizeof(uint32_t) * cap, cudaMemcpyHostToDevice, stream);
             cudaMemcpyAsync(pb.widx.ptr, hwidx, sizeof(uint32_t) * cap, cudaMemcpyHostToDevice, stream);
         }
