@@ -870,10 +870,11 @@ struct LaunchTuner {
     }
     // Configuration for the next segment.  Without room for 8^3 blocks
     // (`allow_big` false) an 8^3 choice falls back to the best 4^3 one.
-    int config(bool allow_big, bool multi) {
+    // `multi` and `obstacles` say which kernel variants the trials run.
+    int config(bool allow_big, bool multi, bool obstacles = false) {
         if (candidates == 0 && fixed < 0) {
             candidates = allow_big ? kNumLaunchConfigs : kNumLaunchShapes;
-            preload_launch_shapes(multi);
+            preload_launch_shapes(multi, obstacles);
         }
         int c = chosen;
         if (c < 0) {

@@ -217,9 +217,9 @@ void launch_rigid_apply(DevRigid *bodies, int body_count, const DevRigidMap *map
                         cudaStream_t stream);
 
 // Load the kernels of every tuner candidate (transfer modes x launch shapes x
-// block edges, grid update) for the single-scene or the multi-scene variant,
-// so that no trial pays a kernel's lazy module load.
-void preload_launch_shapes(bool multi);
+// block edges, grid update) for the multi-scene variant or the single-scene one
+// with or without obstacles, so that no trial pays a kernel's lazy module load.
+void preload_launch_shapes(bool multi, bool obstacles);
 
 // Empty the hash table of `g` and zero both node pools (g's and other's) over
 // g.max_blocks blocks of edge 2^block_shift.

@@ -238,12 +238,18 @@ __device__ __forceinline__ float pow2_scale(float total) {
 
 // PLASTIC selects the variant that carries plastic state (snow, sand, NH sand);
 // scenes without plastic materials run the leaner variant.  VARIANT selects
-// kPlain (one scene, parameters from the kernel parameters), kMulti (a
-// multi-scene batch: each particle reads its scene's parameters from the scene
-// table, scene = class namespace >> kSceneShift, and takes part only in the
-// substeps its scene advances in this batch) or kCpic (one scene whose grid
-// namespace includes CPIC side masks).  Each costs registers only where used.
-enum Variant { kPlain = 0, kMulti = 1, kCpic = 2 };
+// kPlain (one scene without obstacles, parameters from the kernel parameters),
+// kPlainObst (the same with rigid obstacles), kMulti (a multi-scene batch,
+// which has no obstacles: each particle reads its scene's parameters from the
+// scene table, scene = class namespace >> kSceneShift, and takes part only in
+// the substeps its scene advances in this batch) or kCpic (one scene with
+// obstacles whose grid namespace includes CPIC side masks).  Each costs
+// registers only where used: the obstacle contact calls an out-of-line
+// surface function, and with that call in the kernel the register allocator
+// kept ~500 more bytes per thread in local memory on every particle's path
+// (80 registers: 172 bytes of spill stores against 28 without it), which cost
+// the obstacle-free dam break ~10 % of its fused transfer time.
+enum Variant { kPlain = 0, kMulti = 1, kCpic = 2, kPlainObst = 3 };
 template <int MODE, bool PLASTIC, int VARIANT, int THREADS, int MINB, int BS>
 __global__ void __launch_bounds__(THREADS, MINB)
     k_transfer(ParticleSoA P, int n, const DevClass *__restrict__ classes, GridTable cur, GridTable next,
@@ -251,6 +257,7 @@ __global__ void __launch_bounds__(THREADS, MINB)
                double *reactions, uint32_t *status, int *__restrict__ cache) {
     constexpr bool MULTI = VARIANT == kMulti;
     constexpr bool CPIC = VARIANT == kCpic;
+    constexpr bool OBST = VARIANT == kCpic || VARIANT == kPlainObst;
     // One buffer holds the G2P gather tile (float4 per node) and then the P2G
     // scatter tile (4 fixed-point ints per node, component-major).
     constexpr int kTileNodes = tile_nodes(THREADS);
@@ -504,7 +511,7 @@ __global__ void __launch_bounds__(THREADS, MINB)
                     }
                 }
             }
-            for (int oi = 0; oi < sp.num_obstacles; ++oi) {
+            for (int oi = 0; OBST && oi < sp.num_obstacles; ++oi) {
                 const DevObstacle &o = obstacles[oi];
                 if (!obstacle_may_contact(o, pos, radius)) continue;
                 V3f nrm;
@@ -770,7 +777,8 @@ __global__ void __launch_bounds__(THREADS, MINB)
 // Grid update over all allocated blocks; also zeroes those blocks in the other pool.
 // MULTI: each block takes its scene's parameters from the scene table
 // (scene = block namespace >> kSceneShift).  Blocks have edge 2^BS cells.
-template <bool MULTI, int BS>
+// OBST: the scene has rigid obstacles (a batch never has).
+template <bool MULTI, int BS, bool OBST>
 __global__ void __launch_bounds__(256) k_grid(GridTable g, GridTable nxt, SimParams sp,
                                                const DevObstacle *__restrict__ obstacles,
                                                const float *__restrict__ planes, double *reactions, uint32_t *status) {
@@ -815,7 +823,7 @@ __global__ void __launch_bounds__(256) k_grid(GridTable g, GridTable nxt, SimPar
             }
         }
 #undef SCN
-        for (int oi = 0; oi < sp.num_obstacles; ++oi) {
+        for (int oi = 0; OBST && oi < sp.num_obstacles; ++oi) {
             const DevObstacle &o = obstacles[oi];
             if (!obstacle_may_contact(o, pos, h)) continue;
             V3f nrm;
@@ -976,8 +984,10 @@ void launch_transfer(int mode, const ParticleSoA &P, int n, const DevClass *clas
                      double *reactions, uint32_t *status, int *cache, cudaStream_t stream) {
     if (n <= 0) return;
     // Launch shapes other than the default exist for the variants the tuner
-    // picks among (no plastic state; one scene or a batch).
+    // picks among (no plastic state; one scene or a batch).  Plastic state and
+    // CPIC run with the obstacle contact compiled in, with or without obstacles.
     const bool pl = sp.has_plastic != 0;
+    const bool obst = sp.num_obstacles > 0;
     // plastic and CPIC variants: default shape and 4^3 blocks only
     const int shape = (pl || sp.cpic) ? 0 : sp.shape;
     const bool big = !(pl || sp.cpic) && sp.block_shift == kBigBlockShift;
@@ -1004,7 +1014,8 @@ void launch_transfer(int mode, const ParticleSoA &P, int n, const DevClass *clas
             if (pl) TMPM_LAUNCH(M, true, kCpic, 256, TMPM_TRANSFER_MIN_BLOCKS, kBlockShift);  \
             else TMPM_LAUNCH(M, false, kCpic, 256, TMPM_TRANSFER_MIN_BLOCKS, kBlockShift);    \
         } else {                                                                              \
-            if (pl) TMPM_LAUNCH(M, true, kPlain, 256, TMPM_TRANSFER_MIN_BLOCKS, kBlockShift); \
+            if (pl) TMPM_LAUNCH(M, true, kPlainObst, 256, TMPM_TRANSFER_MIN_BLOCKS, kBlockShift); \
+            else if (obst) TMPM_LAUNCH_SHAPES(M, kPlainObst);                                 \
             else TMPM_LAUNCH_SHAPES(M, kPlain);                                               \
         }                                                                                     \
     } while (0)
@@ -1022,13 +1033,18 @@ void launch_transfer(int mode, const ParticleSoA &P, int n, const DevClass *clas
 void launch_grid_update(const GridTable &g, const GridTable &next, const SimParams &sp, const DevObstacle *obstacles,
                         const float *planes, double *reactions, uint32_t *status, cudaStream_t stream) {
     int blocks = device_sm_count() * 8;
+    const bool obst = !sp.multi && sp.num_obstacles > 0;
+#define TMPM_GRID(MU, BS, OB) k_grid<MU, BS, OB><<<blocks, 256, 0, stream>>>(g, next, sp, obstacles, planes, reactions, status)
     if (sp.block_shift == kBigBlockShift) {
-        if (sp.multi) k_grid<true, kBigBlockShift><<<blocks, 256, 0, stream>>>(g, next, sp, obstacles, planes, reactions, status);
-        else k_grid<false, kBigBlockShift><<<blocks, 256, 0, stream>>>(g, next, sp, obstacles, planes, reactions, status);
+        if (sp.multi) TMPM_GRID(true, kBigBlockShift, false);
+        else if (obst) TMPM_GRID(false, kBigBlockShift, true);
+        else TMPM_GRID(false, kBigBlockShift, false);
     } else {
-        if (sp.multi) k_grid<true, kBlockShift><<<blocks, 256, 0, stream>>>(g, next, sp, obstacles, planes, reactions, status);
-        else k_grid<false, kBlockShift><<<blocks, 256, 0, stream>>>(g, next, sp, obstacles, planes, reactions, status);
+        if (sp.multi) TMPM_GRID(true, kBlockShift, false);
+        else if (obst) TMPM_GRID(false, kBlockShift, true);
+        else TMPM_GRID(false, kBlockShift, false);
     }
+#undef TMPM_GRID
 }
 
 namespace {
@@ -1049,14 +1065,17 @@ void touch_shapes() {
     touch_transfer<kModeG2P2G, V, 256, 3, BS>();
     touch_transfer<kModeG2P, V, 256, 3, BS>();
     cudaFuncAttributes a;
-    cudaFuncGetAttributes(&a, k_grid<V == kMulti, BS>);
+    cudaFuncGetAttributes(&a, k_grid<V == kMulti, BS, V == kPlainObst>);
 }
 }  // namespace
 
-void preload_launch_shapes(bool multi) {
+void preload_launch_shapes(bool multi, bool obstacles) {
     if (multi) {
         touch_shapes<kMulti, kBlockShift>();
         touch_shapes<kMulti, kBigBlockShift>();
+    } else if (obstacles) {
+        touch_shapes<kPlainObst, kBlockShift>();
+        touch_shapes<kPlainObst, kBigBlockShift>();
     } else {
         touch_shapes<kPlain, kBlockShift>();
         touch_shapes<kPlain, kBigBlockShift>();

@@ -487,7 +487,7 @@ struct TmpmSession {
         const bool tunable = !has_plastic && !sp.cpic;
         TmpmStatus st = TMPM_OK;
         for (uint32_t done = 0; done < steps && st == TMPM_OK;) {
-            const int config = tunable ? tuner.config(big_blocks_ok, false) : 0;
+            const int config = tunable ? tuner.config(big_blocks_ok, false, !obstacles.empty()) : 0;
             const int shape = config_shape(config), bs = config_block_shift(config);
             sp.shape = shape;
             sp.block_shift = bs;
@@ -619,9 +619,10 @@ struct TmpmSession {
             // world-index chunks: the copy of chunk k + 1 runs while chunk k is applied
             const size_t per = (N + kReadChunks - 1) / kReadChunks;
             int chunks = 0;
+            const size_t rows = has_plastic ? 27 : 24;  // rows 24-26 (plastic state) are read for plastic classes only
             for (size_t a = 0; a < N; a += per, ++chunks) {
                 const size_t w = std::min(per, N - a) * sizeof(float);
-                if ((e = cudaMemcpy2DAsync(h + a, N * sizeof(float), unsorted.ptr + a, N * sizeof(float), w, 27,
+                if ((e = cudaMemcpy2DAsync(h + a, N * sizeof(float), unsorted.ptr + a, N * sizeof(float), w, rows,
                                            cudaMemcpyDeviceToHost, stream)) ||
                     (e = cudaEventRecord(read_events[chunks], stream)))
                     return cuda_fail(e, "readback");
@@ -1156,7 +1157,7 @@ int32_t tmpm_session_launch_shape(TmpmSession *s, double *ms_per_unit, size_t co
     }
     if (ms_per_unit) s->tuner.costs(ms_per_unit, static_cast<uint32_t>(count));
     if (s->has_plastic || s->cpic_active()) return 0;  // variants built for the default shape only
-    if (s->tuner.chosen >= 0 && !s->big_blocks_ok) return s->tuner.config(false, false);  // 8^3 without room: best 4^3
+    if (s->tuner.chosen >= 0 && !s->big_blocks_ok) return s->tuner.config(false, false, !s->obstacles.empty());  // 8^3 without room: best 4^3
     return s->tuner.chosen;
 }
 
