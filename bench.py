@@ -420,7 +420,8 @@ def run_tessera(args, world, rank, local):
     grid_nodes = int(mm.shape[0])
 
     # the launch-shape tuner's trials (two 64-substep segments per shape) come
-    # before the warm-up, so every timed segment runs the chosen shape
+    # before the warm-up, so the timed region starts on the chosen shape (the
+    # session keeps timing its segments and may switch as the scene evolves)
     for _ in range(16):
         if session.launch_shape()["shape"] is not None:
             break
@@ -437,6 +438,7 @@ def run_tessera(args, world, rank, local):
     torch.cuda.synchronize()
     barrier(world)
     session.synchronize()  # validates the device result (raises on any failure flag)
+    shape_end = session.launch_shape()  # the session keeps timing segments and may have switched
     ms_max = allreduce_max(ms, world)
     units = allreduce_sum(float(n) * BATCH * args.steps, world)
     value = units / (ms_max / 1000.0)
@@ -522,6 +524,7 @@ def run_tessera(args, world, rank, local):
                        "active_grid_nodes": grid_nodes, "dt": sc.dt, "substeps_per_step": BATCH,
                        "l2": "inputs larger than L2 (particle state ~0.4 GB per GPU)",
                        "launch_shape": shape_summary(shape_info),
+                       "launch_shape_after_timing": shape_summary(shape_end),
                        "parallelism": f"replicas x{world}"},
             "gpu_launches": (2 * BATCH + 2 + RESORT_LAUNCHES) * args.steps,
             "roofline": roofline,

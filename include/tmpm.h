@@ -467,9 +467,11 @@ TmpmStatus tmpm_debug_p2g(TmpmSession *session, int32_t *cells_out, float *mass_
                           size_t capacity, size_t *count);
 
 /* Kernel timing (bench hook): time `steps` substeps of the resident path on the
- * session stream with CUDA events; returns milliseconds via *ms.  Per-kernel
- * averages (ms per launch) go to kernel_ms[0..n) in the order p2g, grid,
- * g2p2g, g2p, resort when kernel_ms is non-NULL. */
+ * session stream with CUDA events; returns milliseconds via *ms (host waits
+ * between submissions included).  The substeps go in submissions of at most 64,
+ * each waited for before the next, as a caller stepping frame by frame runs
+ * them.  Per-kernel averages (ms per launch) go to kernel_ms[0..n) in the order
+ * p2g, grid, g2p2g, g2p, resort when kernel_ms is non-NULL. */
 TmpmStatus tmpm_bench_substeps(TmpmSession *session, uint32_t steps, double *ms,
                                double *kernel_ms, size_t kernel_count);
 
@@ -483,7 +485,13 @@ TmpmStatus tmpm_bench_substeps(TmpmSession *session, uint32_t steps, double *ms,
  * particle-substep, as CUDA events on its stream measured it.  8-cell blocks
  * are tried when the block pool holds the scene in them at most twice the
  * 4-cell pool's size (dense scenes).  Plastic materials and CPIC run shape 0
- * only. */
+ * only.  A session keeps timing its full segments after the choice, because a
+ * scene's best shape can change as it evolves: every sixth such segment runs
+ * the best other shape by its latest time, which takes over when it beat the
+ * chosen shape's recent mean by more than 1 %.  The times are read when later
+ * segments are submitted, so a caller that submits one frame at a time (and
+ * waits for it) gets the switch within a segment or two; a batch keeps its
+ * first choice. */
 
 /* Shape `shape` (0 ..< count): particles per CTA, CTAs per SM, block edge in cells. */
 uint32_t tmpm_launch_shape_count(void);
@@ -491,7 +499,7 @@ TmpmStatus tmpm_launch_shape_info(uint32_t shape, uint32_t *threads_per_cta, uin
                                   uint32_t *block_edge);
 
 /* The shape in use: -1 while trials are outstanding, else its index.  When
- * `ms_per_unit` is non-NULL, it receives (up to `count` entries) the best
+ * `ms_per_unit` is non-NULL, it receives (up to `count` entries) the latest
  * measured milliseconds per particle-substep of each shape (infinity where no
  * trial has been read). */
 int32_t tmpm_session_launch_shape(TmpmSession *session, double *ms_per_unit, size_t count);

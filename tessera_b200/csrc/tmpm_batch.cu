@@ -1243,8 +1243,7 @@ int32_t tmpm_batch_launch_shape(TmpmBatch *b, double *ms_per_unit, size_t count)
     }
     if (ms_per_unit) b->tuner.costs(ms_per_unit, static_cast<uint32_t>(count));
     if (b->classes.plastic()) return 0;  // variants built for the default shape only
-    if (b->tuner.chosen >= 0 && !b->big_blocks_ok) return b->tuner.config(false, true);  // 8^3 without room: best 4^3
-    return b->tuner.chosen;
+    return b->tuner.current(b->big_blocks_ok);  // 8^3 without room: the best 4^3
 }
 
 size_t tmpm_batch_device_bytes(const TmpmBatch *b) { return b ? b->device_bytes() : 0; }

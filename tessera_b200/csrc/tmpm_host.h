@@ -815,8 +815,35 @@ struct LaunchTuner {
     std::vector<Trial> trials;
     int open = -1;  // index of the trial being recorded
 
+    // After the choice (single scenes, `watch`): a scene's cost per
+    // particle-substep drifts as it evolves (a dam break's CTA boxes widen as
+    // it spreads) and the best configuration can change with it, so every full
+    // segment keeps being timed ("probes") and every kChallengeEvery-th one
+    // runs the best other candidate by its latest time; the challenger takes
+    // over when it beat the mean of the chosen configuration's segments since
+    // the last challenge by more than kSwitchMargin.  Segments open with a
+    // re-sort and a table clear either way, so a switch costs nothing extra.
+    static constexpr int kChallengeEvery = 6;
+    static constexpr double kSwitchMargin = 0.01;
+    bool watch = false;
+    struct Probe {
+        int config = 0;
+        double work = 0.0;
+        cudaEvent_t a = nullptr, b = nullptr;
+    };
+    std::vector<Probe> probes;        // recorded, oldest first; read ones are removed
+    std::vector<cudaEvent_t> spare;   // events of read probes, reused
+    int probe_open = -1;
+    double recent = 0.0;              // mean time of the chosen configuration's probes since the last challenge
+    int recent_n = 0;
+    int since_challenge = 0;          // probes of the chosen configuration since the last challenge
+    bool challenge_pending = false;   // a challenger's probe is recorded but not read
+
     LaunchTuner() { reset(0); }
-    ~LaunchTuner() { release(); }
+    ~LaunchTuner() {
+        release();
+        drop_probes();
+    }
     LaunchTuner(const LaunchTuner &) = delete;
     LaunchTuner &operator=(const LaunchTuner &) = delete;
 
@@ -828,9 +855,23 @@ struct LaunchTuner {
         trials.clear();
         open = -1;
     }
+    void drop_probes() {
+        for (Probe &p : probes) {
+            if (p.a) cudaEventDestroy(p.a);
+            if (p.b) cudaEventDestroy(p.b);
+        }
+        probes.clear();
+        for (cudaEvent_t e : spare) cudaEventDestroy(e);
+        spare.clear();
+        probe_open = -1;
+        recent = 0.0;
+        recent_n = since_challenge = 0;
+        challenge_pending = false;
+    }
     // `option`: 0 = tune, k > 0 = fixed configuration k - 1 (out of range: 0).
     void reset(uint32_t option) {
         release();
+        drop_probes();
         fixed = option == 0 ? -1 : (option <= static_cast<uint32_t>(kNumLaunchConfigs) ? static_cast<int>(option) - 1 : 0);
         chosen = fixed;
         candidates = 0;
@@ -880,8 +921,20 @@ struct LaunchTuner {
         if (c < 0) {
             poll();
             c = chosen;
+        } else if (watching()) {
+            poll_probes();
+            c = chosen;
+            if (!challenge_pending && recent_n >= 2 && since_challenge >= kChallengeEvery) {
+                const int r = challenger(allow_big);
+                if (r >= 0) return r;
+            }
         }
         if (c < 0) c = issued < trials_total() ? trial_config(issued) : 0;
+        return usable(c, allow_big);
+    }
+    // The configuration to report: the choice (or trial), as config() runs it.
+    int current(bool allow_big) const { return chosen < 0 ? chosen : usable(chosen, allow_big); }
+    int usable(int c, bool allow_big) const {
         if (!allow_big && c >= kNumLaunchShapes) {
             if (fixed >= 0) return config_shape(c);
             int s = 0;
@@ -890,6 +943,96 @@ struct LaunchTuner {
             return s;
         }
         return c;
+    }
+    bool watching() const { return watch && chosen >= 0 && fixed < 0 && candidates > 1; }
+    // The best candidate other than the choice by its latest time (-1: none).
+    int challenger(bool allow_big) const {
+        int r = -1;
+        const int limit = allow_big ? candidates : std::min(candidates, kNumLaunchShapes);
+        for (int k = 0; k < limit; ++k)
+            if (k != chosen && (r < 0 || best[k] < best[r])) r = k;
+        return r;
+    }
+    // Brackets a full segment (re-sort included) of `work` particle-substeps
+    // after the choice; no-ops unless watching.
+    void probe_begin(int config_used, cudaStream_t stream) {
+        if (!watching() || probe_open >= 0) return;
+        Probe p;
+        p.config = config_used;
+        p.a = take_event();
+        p.b = take_event();
+        if (!p.a || !p.b || cudaEventRecord(p.a, stream)) {
+            if (p.a) spare.push_back(p.a);
+            if (p.b) spare.push_back(p.b);
+            cudaGetLastError();
+            return;
+        }
+        probes.push_back(p);
+        probe_open = static_cast<int>(probes.size()) - 1;
+        if (config_used == chosen) {
+            ++since_challenge;
+        } else {
+            since_challenge = 0;
+            challenge_pending = true;
+        }
+    }
+    void probe_end(double work, cudaStream_t stream) {
+        if (probe_open < 0) return;
+        probes[probe_open].work = work;
+        cudaEventRecord(probes[probe_open].b, stream);
+        probe_open = -1;
+    }
+    cudaEvent_t take_event() {
+        if (!spare.empty()) {
+            cudaEvent_t e = spare.back();
+            spare.pop_back();
+            return e;
+        }
+        cudaEvent_t e = nullptr;
+        if (cudaEventCreate(&e) != cudaSuccess) {
+            cudaGetLastError();
+            return nullptr;
+        }
+        return e;
+    }
+    // Reads the finished probes in order and applies the switch rule.
+    void poll_probes() {
+        size_t done = 0;
+        for (; done < probes.size() && static_cast<int>(done) != probe_open; ++done) {
+            Probe &p = probes[done];
+            if (cudaEventQuery(p.b) != cudaSuccess) {
+                cudaGetLastError();
+                break;
+            }
+            float ms = 0.f;
+            const bool ok = cudaEventElapsedTime(&ms, p.a, p.b) == cudaSuccess && p.work > 0;
+            cudaGetLastError();
+            spare.push_back(p.a);
+            spare.push_back(p.b);
+            if (!ok) continue;
+            const double v = ms / p.work;
+            if (p.config == chosen) {
+                recent = (recent * recent_n + v) / (recent_n + 1);
+                ++recent_n;
+                continue;
+            }
+            best[p.config] = v;
+            challenge_pending = false;
+            if (recent_n >= 2 && v < recent * (1.0 - kSwitchMargin)) {
+                best[chosen] = recent;
+                chosen = p.config;
+                recent = v;
+                recent_n = 1;
+            } else {
+                if (recent_n > 0) best[chosen] = recent;
+                recent = 0.0;
+                recent_n = 0;
+            }
+        }
+        if (done > 0) {
+            probes.erase(probes.begin(), probes.begin() + done);
+            if (probe_open >= 0) probe_open -= static_cast<int>(done);
+        }
     }
     // Brackets one segment of `work` particle-substeps run under config();
     // only trials are recorded.

@@ -498,7 +498,11 @@ struct TmpmSession {
             // Replay a captured graph for a segment long enough to be worth it,
             // outside per-kernel timing and tuning trials; otherwise launch.
             if (kernel_ms == nullptr && !(tunable && tuner.tuning()) && seg >= kGraphMinSubsteps) {
+                // after the choice, full segments are timed (re-sort included) for the tuner's watch
+                const bool probe = tunable && resort && seg == interval;
+                if (probe) tuner.probe_begin(config, stream);
                 st = run_segment_graph(sp, resort, seg, apply_force);
+                if (probe) tuner.probe_end(static_cast<double>(n_dev) * seg, stream);
             } else {
                 // launch_segment's kernels one by one, timed with `kernel_ms`
                 if (resort) {
@@ -712,6 +716,7 @@ TmpmStatus tmpm_session_create(const TmpmParams *params, const TmpmParticleArray
     s->substep_dt = substep_dt;
     s->substeps = s->options.substeps;
     s->tuner.reset(s->options.launch_shape);
+    s->tuner.watch = true;  // one scene: its best configuration can change as it evolves
     std::string err;
     if (!params_valid(*params)) {
         g_last_error = "invalid MPM input";
@@ -1105,18 +1110,27 @@ TmpmStatus tmpm_bench_substeps(TmpmSession *s, uint32_t steps, double *ms, doubl
     if (st != TMPM_OK) return st;
     if (steps == 0) return s->fail(TMPM_ERR_INVALID_INPUT, "steps must be positive");
     cudaSetDevice(s->device);
-    cudaEvent_t a, b;
+    cudaEvent_t a, b, seg;
     cudaEventCreate(&a);
     cudaEventCreate(&b);
+    cudaEventCreateWithFlags(&seg, cudaEventDisableTiming);
     std::vector<float> acc(10, 0.0f);
     cudaStreamSynchronize(s->stream);
     cudaEventRecord(a, s->stream);
     uint32_t left = steps;
     while (left) {
+        // one submission of at most 64 substeps (the reference's per-submit
+        // maximum) at a time, each waited for, as a caller stepping frame by
+        // frame runs them: the tuner's watch reads each segment's time before
+        // the next segment picks its launch configuration
         uint32_t batch = std::min<uint32_t>(64, left);
         st = s->enqueue(batch, s->substep_dt, true, false, kernel_ms ? &acc : nullptr);
         if (st != TMPM_OK) break;
         left -= batch;
+        if (left) {
+            cudaEventRecord(seg, s->stream);
+            cudaEventSynchronize(seg);
+        }
     }
     cudaEventRecord(b, s->stream);
     cudaEventSynchronize(b);
@@ -1124,6 +1138,7 @@ TmpmStatus tmpm_bench_substeps(TmpmSession *s, uint32_t steps, double *ms, doubl
     cudaEventElapsedTime(&t, a, b);
     cudaEventDestroy(a);
     cudaEventDestroy(b);
+    cudaEventDestroy(seg);
     if (st != TMPM_OK) return st;
     s->pending += steps;
     if (ms) *ms = t;
@@ -1151,14 +1166,12 @@ TmpmStatus tmpm_launch_shape_info(uint32_t shape, uint32_t *threads_per_cta, uin
 
 int32_t tmpm_session_launch_shape(TmpmSession *s, double *ms_per_unit, size_t count) {
     if (!s) return -1;
-    if (s->tuner.tuning()) {
-        cudaSetDevice(s->device);
-        s->tuner.poll();
-    }
+    cudaSetDevice(s->device);
+    if (s->tuner.tuning()) s->tuner.poll();
+    else if (s->tuner.watching()) s->tuner.poll_probes();
     if (ms_per_unit) s->tuner.costs(ms_per_unit, static_cast<uint32_t>(count));
     if (s->has_plastic || s->cpic_active()) return 0;  // variants built for the default shape only
-    if (s->tuner.chosen >= 0 && !s->big_blocks_ok) return s->tuner.config(false, false, !s->obstacles.empty());  // 8^3 without room: best 4^3
-    return s->tuner.chosen;
+    return s->tuner.current(s->big_blocks_ok);  // 8^3 without room: the best 4^3
 }
 
 // ---------------------------------------------------------------- rigid coupling

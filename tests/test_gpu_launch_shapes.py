@@ -88,6 +88,31 @@ def test_tuned_session_settles_and_tracks_the_oracle(dam_break):
     assert_tracks(states[done], s.particles(), pos=4e-5, vel=4e-4, F=4e-4, C=4e-2)
 
 
+def test_session_keeps_timing_and_challenges_after_the_choice(dam_break):
+    """After the choice, a session stepping one 64-substep frame at a time keeps
+    timing its segments and every sixth runs the best other shape, so the
+    reported times move on from the trials' (a challenger's, and the chosen
+    shape's recent mean); the shape in use stays a valid one and the state
+    stays finite through the switches."""
+    sc, _ = dam_break
+    s = Session(sc.params, sc.particles, sc.dt)
+    frames = 0
+    while s.launch_shape()["shape"] is None and frames < 16:
+        s.step(64)
+        frames += 1
+    assert s.launch_shape()["shape"] is not None
+    first = list(s.launch_shape()["ms_per_particle_substep"])
+    for _ in range(12):
+        s.step(64)
+    info = s.launch_shape()
+    costs = info["ms_per_particle_substep"]
+    moved = [k for k, (a, b) in enumerate(zip(first, costs)) if a is not None and b is not None and a != b]
+    assert len(moved) >= 2, (first, costs)
+    assert info["shape"] in SHAPES and costs[info["shape"]] is not None
+    p = s.particles()
+    assert np.isfinite(p.position).all() and np.isfinite(p.velocity).all()
+
+
 def test_batches_under_each_shape_and_tuned_match_the_oracle_per_scene():
     pair = [scenes.batch_scene(21, cells=6), scenes.batch_scene(22, cells=9)]
     steps = (6, 4)
