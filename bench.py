@@ -438,14 +438,15 @@ def run_tessera(args, world, rank, local):
     torch.cuda.synchronize()
     barrier(world)
     session.synchronize()  # validates the device result (raises on any failure flag)
-    shape_end = session.launch_shape()  # the session keeps timing segments and may have switched
     ms_max = allreduce_max(ms, world)
     units = allreduce_sum(float(n) * BATCH * args.steps, world)
     value = units / (ms_max / 1000.0)
 
-    # per-kernel average launch durations (CUDA events on the session stream)
+    # per-kernel average launch durations (CUDA events on the session stream),
+    # one segment under the configuration in use
     _, kms = session.bench_substeps(BATCH, per_kernel=True)
     session.synchronize()
+    shape_end = session.launch_shape()
     g2p2g_ms = float(kms[2])
     peak, peak_kind = measured_peaks()
     # algorithmic bytes of one fused G2P->P2G launch: 248 B per particle (P2G 104 + G2P 48 + 96 write) and
@@ -458,12 +459,18 @@ def run_tessera(args, world, rank, local):
                 "traffic": None, "alg_bytes_per_launch": alg_bytes, "launch_ms": g2p2g_ms,
                 "kernel_ms": {"p2g": float(kms[0]), "grid": float(kms[1]), "g2p2g": g2p2g_ms, "g2p": float(kms[3]),
                               "resort": float(kms[4])}}
+    # DRAM traffic per particle of the fused launch, captured with ncu for a launch
+    # configuration; used when the timed launches ran that configuration
     prof = os.path.join(ROOT, "profiles", "traffic.json")
+    k_end = shape_end["shape"]
+    timed_config = None if k_end is None else "{}x{}/{}^3".format(*shape_end["shapes"][k_end])
+    roofline["launch_config"] = timed_config
     if os.path.exists(prof):
         with open(prof) as f:
             tr = json.load(f)
-        if "g2p2g_bytes_per_particle" in tr:
-            roofline["traffic"] = tr["g2p2g_bytes_per_particle"] * n
+        per = tr.get("g2p2g_bytes_per_particle", {})
+        if timed_config in per:
+            roofline["traffic"] = per[timed_config] * n
             roofline["traffic_source"] = tr.get("source")
 
     # e2e: host arrays -> device -> 64 substeps -> host arrays, through the C ABI
@@ -520,7 +527,7 @@ def run_tessera(args, world, rank, local):
             "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
-            "config": {"workload": "config2-dam-break", "particles_per_gpu": n, "grid": "256^3 virtual, 4^3 blocks",
+            "config": {"workload": "config2-dam-break", "particles_per_gpu": n, "grid": "256^3 virtual, hashed blocks of 4^3 or 8^3 cells (tuned)",
                        "active_grid_nodes": grid_nodes, "dt": sc.dt, "substeps_per_step": BATCH,
                        "l2": "inputs larger than L2 (particle state ~0.4 GB per GPU)",
                        "launch_shape": shape_summary(shape_info),

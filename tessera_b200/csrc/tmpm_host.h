@@ -911,8 +911,9 @@ struct LaunchTuner {
     }
     // Configuration for the next segment.  Without room for 8^3 blocks
     // (`allow_big` false) an 8^3 choice falls back to the best 4^3 one.
-    // `multi` and `obstacles` say which kernel variants the trials run.
-    int config(bool allow_big, bool multi, bool obstacles = false) {
+    // `multi` and `obstacles` say which kernel variants the trials run;
+    // `may_challenge`: the segment will be a full, probed one.
+    int config(bool allow_big, bool multi, bool obstacles = false, bool may_challenge = false) {
         if (candidates == 0 && fixed < 0) {
             candidates = allow_big ? kNumLaunchConfigs : kNumLaunchShapes;
             preload_launch_shapes(multi, obstacles);
@@ -924,7 +925,7 @@ struct LaunchTuner {
         } else if (watching()) {
             poll_probes();
             c = chosen;
-            if (!challenge_pending && recent_n >= 2 && since_challenge >= kChallengeEvery) {
+            if (may_challenge && !challenge_pending && recent_n >= 2 && since_challenge >= kChallengeEvery) {
                 const int r = challenger(allow_big);
                 if (r >= 0) return r;
             }

@@ -487,7 +487,9 @@ struct TmpmSession {
         const bool tunable = !has_plastic && !sp.cpic;
         TmpmStatus st = TMPM_OK;
         for (uint32_t done = 0; done < steps && st == TMPM_OK;) {
-            const int config = tunable ? tuner.config(big_blocks_ok, false, !obstacles.empty()) : 0;
+            // a challenger only where the segment will be a full one replayed from its graph (timed)
+            const bool full = kernel_ms == nullptr && steps - done >= interval && interval >= kGraphMinSubsteps;
+            const int config = tunable ? tuner.config(big_blocks_ok, false, !obstacles.empty(), full) : 0;
             const int shape = config_shape(config), bs = config_block_shift(config);
             sp.shape = shape;
             sp.block_shift = bs;
