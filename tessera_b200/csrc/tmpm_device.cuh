@@ -93,9 +93,8 @@ __device__ __forceinline__ bool regular_corotated(const M3f &F) {
 }
 
 // Corotated Kirchhoff stress 2 mu (F - R) F^T + lambda (J - 1) J I, scaled by
-// snow's hardening factor (material.rs:272-283, 440-455).  Out of line: its
-// polar iteration would otherwise raise register pressure for every particle.
-static __device__ __noinline__ M3f corotated_stress(const DevClass &k, const M3f &F, float J, float plastic_det) {
+// snow's hardening factor (material.rs:272-283, 440-455).
+__device__ __forceinline__ M3f corotated_stress_body(const DevClass &k, const M3f &F, float J, float plastic_det) {
     float factor = 1.0f;
     if (k.kind == kMatSnow) factor = fminf(fmaxf(expf(k.p2 * (1.0f - plastic_det)), 0.01f), 100.0f);
     float lambda = k.p0 * factor, mu = k.p1 * factor;
@@ -108,8 +107,20 @@ static __device__ __noinline__ M3f corotated_stress(const DevClass &k, const M3f
     return s;
 }
 
+// The same out of line.  Which placement holds fewer registers depends on the
+// kernel variant: an out-of-line call takes the class record and F by
+// reference, so they stay in local memory around it; inline, the polar
+// iteration adds to the register peak.  With the obstacle contact (itself an
+// out-of-line call) or plastic state in the kernel, the call spills less; in
+// the lean variants inlining took the fused transfer from 0.499 to 0.451 ms
+// on the dam break.
+static __device__ __noinline__ M3f corotated_stress(const DevClass &k, const M3f &F, float J, float plastic_det) {
+    return corotated_stress_body(k, F, J, plastic_det);
+}
+
 // Kirchhoff stress times -dt V0 4/h^2 (material.rs:233-284; the scaling is
 // world.rs:391 / gpu.wgsl:700).  `plastic_det` feeds snow's hardening factor.
+template <bool INLINE_COROTATED>
 __device__ __forceinline__ M3f scaled_stress(const DevClass &k, const M3f &F, const M3f &Cm, float neg_dt_inv_d,
                                              float plastic_det) {
     float J = det(F);
@@ -134,7 +145,7 @@ __device__ __forceinline__ M3f scaled_stress(const DevClass &k, const M3f &F, co
         s.c1.y += diag;
         s.c2.z += diag;
     } else {  // corotated: elastic, sand, snow (with its hardening factor)
-        s = corotated_stress(k, F, J, plastic_det);
+        s = INLINE_COROTATED ? corotated_stress_body(k, F, J, plastic_det) : corotated_stress(k, F, J, plastic_det);
     }
     return scale(s, neg_dt_inv_d * k.volume);
 }

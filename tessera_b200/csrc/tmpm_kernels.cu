@@ -609,7 +609,7 @@ __global__ void __launch_bounds__(THREADS, MINB)
     V3f mv = mk(0, 0, 0);
     float bound_m = 0.f, bound_p = 0.f;
     if (active) {
-        M3f S = scaled_stress(k, F, Cm, -dt * inv_d, pl[0]);
+        M3f S = scaled_stress<!OBST && !PLASTIC>(k, F, Cm, -dt * inv_d, pl[0]);
         A = add(S, scale(Cm, k.mass));
         mv = v * k.mass;
         // |(m v + A dpos)_i| <= |m v_i| + 1.5 h sum_j |A_ij| and a particle's 27 weights sum to one,
