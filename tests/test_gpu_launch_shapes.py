@@ -16,6 +16,7 @@ import pytest
 
 from oracle import oracle as O
 from tessera_b200 import _native, scenes
+from tessera_b200._abi import Obstacle
 from tessera_b200.batch import Batch
 from tessera_b200.session import Session
 
@@ -53,6 +54,24 @@ def test_every_launch_shape_tracks_the_oracle(dam_break, shape):
     assert_tracks(states[8], s.particles())
     info = s.launch_shape()
     assert info["shape"] == shape and info["shapes"][shape] == _native.launch_shapes()[shape]
+
+
+def test_obstacle_and_obstacle_free_variants_agree(dam_break):
+    """A session with a rigid sphere far outside the scene runs the kernels with
+    the obstacle contact compiled in; without obstacles, the obstacle-free
+    variants. No particle or node comes near the sphere, so both track the
+    oracle and agree with each other to f32 rounding."""
+    sc, states = dam_break
+    runs = []
+    for obstacles in ([], [Obstacle.sphere((50.0, 50.0, 50.0), 0.5)]):
+        for shape in (0, 3):
+            s = Session(sc.params, sc.particles, sc.dt, obstacles=obstacles, launch_shape=shape)
+            s.step(8)
+            runs.append(s.particles())
+            assert_tracks(states[8], runs[-1])
+    for plain, obst in zip(runs[:2], runs[2:]):
+        assert np.abs(plain.position - obst.position).max() < 1e-6
+        assert np.abs(plain.velocity - obst.velocity).max() < 1e-5
 
 
 def test_one_substep_agrees_between_block_edges(dam_break):
