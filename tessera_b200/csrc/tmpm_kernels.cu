@@ -482,6 +482,9 @@ __global__ void __launch_bounds__(THREADS, MINB)
             }
         }
 
+        // the P2G below reuses the block ids of this box (read after its
+        // barriers); published now, the box is dead through the update
+        if (MODE != kModeG2P && threadIdx.x == 0) s_gbox = bx;
         // F is read only now: it is not needed during the gather, whose
         // accumulators and weights are the kernel's peak register demand
         if (valid) {
@@ -586,7 +589,6 @@ __global__ void __launch_bounds__(THREADS, MINB)
             }
         }
         if (MODE == kModeG2P) return;
-        if (threadIdx.x == 0) s_gbox = bx;
     }
 
     // ----------------------------------------------------------------- P2G
