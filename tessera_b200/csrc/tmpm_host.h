@@ -823,6 +823,8 @@ struct LaunchTuner {
     // over when it beat the mean of the chosen configuration's segments since
     // the last challenge by more than kSwitchMargin.  Segments open with a
     // re-sort and a table clear either way, so a switch costs nothing extra.
+    // A segment that first captures its graph is not probed (the capture would
+    // count as device time); a challenge not probed is issued again.
     static constexpr int kChallengeEvery = 6;
     static constexpr double kSwitchMargin = 0.01;
     bool watch = false;

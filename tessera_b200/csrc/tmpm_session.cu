@@ -500,8 +500,11 @@ struct TmpmSession {
             // Replay a captured graph for a segment long enough to be worth it,
             // outside per-kernel timing and tuning trials; otherwise launch.
             if (kernel_ms == nullptr && !(tunable && tuner.tuning()) && seg >= kGraphMinSubsteps) {
-                // after the choice, full segments are timed (re-sort included) for the tuner's watch
-                const bool probe = tunable && resort && seg == interval;
+                // after the choice, full segments are timed (re-sort included) for the
+                // tuner's watch, once their graph exists: a segment that captures its
+                // graph first would count the capture as device time
+                const bool probe = tunable && resort && seg == interval && tuner.watching() &&
+                                   seg_graphs.count(segment_key(sp, cur, resort, seg, apply_force)) > 0;
                 if (probe) tuner.probe_begin(config, stream);
                 st = run_segment_graph(sp, resort, seg, apply_force);
                 if (probe) tuner.probe_end(static_cast<double>(n_dev) * seg, stream);
