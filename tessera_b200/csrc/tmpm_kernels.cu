@@ -486,12 +486,15 @@ __global__ void __launch_bounds__(THREADS, MINB)
         // barriers); published now, the box is dead through the update
         if (MODE != kModeG2P && threadIdx.x == 0) s_gbox = bx;
         // F is read only now: it is not needed during the gather, whose
-        // accumulators and weights are the kernel's peak register demand
+        // accumulators and weights are the kernel's peak register demand.  With
+        // the obstacle contact (an out-of-line call, around which everything
+        // live is saved) an updating particle reads F after the contact.
+        const bool updates = g2p_on && !fixed;
         if (valid) {
-            F = load_m3(P.F, cap, i);
+            if (!OBST || !updates) F = load_m3(P.F, cap, i);
             k = classes[cw & kClassMask];
         }
-        if (g2p_on && !fixed) {
+        if (updates) {
             // Particle update (gpu.wgsl:885-1003; world.rs:443-463).
             if (sp.apply_force) {
                 const size_t w = P.widx[i], fs = P.force_stride;
@@ -528,6 +531,7 @@ __global__ void __launch_bounds__(THREADS, MINB)
                                      (before - vel) * k.mass);
                 }
             }
+            if (OBST) F = load_m3(P.F, cap, i);
             M3f Fn = mul(add(m3_identity(), scale(aff, dt)), F);
             bool plastic_ok = true;
             if (k.kind == kMatFluid) {
