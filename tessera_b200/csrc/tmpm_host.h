@@ -106,7 +106,9 @@ inline void stream_fence() { _mm_sfence(); }
 // took ~0.23 ms).  One job runs at a time: the caller and the workers claim
 // chunk indices from a shared counter, so the caller alone can finish any job;
 // a caller that finds a job running (another thread, or a pass nested inside a
-// chunk) runs its own job on threads of its own instead of waiting.
+// chunk) runs its own job on threads of its own instead of waiting.  A child
+// process forked between passes has no workers and runs each pass on its
+// calling thread alone.
 class HostPool {
   public:
     static HostPool &get() {
