@@ -297,13 +297,17 @@ TmpmStatus tmpm_step_cfl_with_reactions(TmpmSession *session, double dt,
  * session's re-sort uses.  `stream` is a cudaStream_t (NULL =
  * the default stream); the call is asynchronous on it.
  * It allocates nothing: its scratch is a fixed array inside the library
- * (about 4.1 MB, held on every device that loads the library until exit), so
- * `count` is limited to 262,144; larger counts return TMPM_ERR_CAPACITY with
- * the reason in tmpm_last_error().  The first call on a device looks up the
- * scratch address once (set-up), so make that first call before any stream
- * capture.  All calls share the scratch: calls that overlap on the GPU
- * (different streams, or different host threads) race and must be ordered by
- * the caller. */
+ * (4,260,864 bytes, held on every device that loads the library until exit),
+ * so `count` is limited to 262,144; larger counts return TMPM_ERR_CAPACITY
+ * with the reason in tmpm_last_error().  Set-up: a call made outside a stream
+ * capture looks up the scratch address in the current context; a call made
+ * during a capture reuses the address of the last call outside one in the
+ * same context, so make the first call on a device (and the first after a
+ * cudaDeviceReset) before any stream capture.  On entry the call clears any
+ * error an earlier CUDA call left unreported (cudaGetLastError), so that
+ * only its own launches decide its status.  All calls share the scratch:
+ * calls that overlap on the GPU (different streams, or different host
+ * threads) race and must be ordered by the caller. */
 TmpmStatus tmpm_sort_by_block_noalloc(const float *positions, size_t count, size_t stride,
                                       double cell_width, uint32_t *order_out, uint32_t *keys_out,
                                       void *stream);
