@@ -42,6 +42,7 @@ struct AdjParams {
     float gx, gy, gz;
     int wall_mode;
     float bmin[3], bmax[3];
+    int wall_lo[3], wall_hi[3];  // wall nodes by index, as SceneParams (f64 thresholds)
     int lo[3], dim[3];  // node array: cells lo .. lo + dim - 1 per axis
     int n;
     size_t stride;      // row stride of state arrays
@@ -169,8 +170,7 @@ __device__ __forceinline__ float4 node_velocity(const AdjParams &P, int node, fl
     float v[3] = {mp.y / mp.x + P.gx * P.dt, mp.z / mp.x + P.gy * P.dt, mp.w / mp.x + P.gz * P.dt};
     int mask = 0;
     for (int a = 0; a < 3; ++a) {
-        float pos = static_cast<float>(id[a]) * P.h;
-        bool lower = pos <= P.bmin[a] + P.h, upper = pos >= P.bmax[a] - P.h;
+        const bool lower = id[a] <= P.wall_lo[a], upper = id[a] >= P.wall_hi[a];
         if (P.wall_mode == 1) {
             if (lower || upper) mask = 7;
         } else if ((lower && v[a] < 0.0f) || (upper && v[a] > 0.0f)) {
@@ -705,6 +705,8 @@ TmpmStatus tmpm_adjoint_create(const TmpmParams *params, const TmpmParticleArray
     for (int k = 0; k < 3; ++k) {
         P.bmin[k] = static_cast<float>(params->bounds_min[k]);
         P.bmax[k] = static_cast<float>(params->bounds_max[k]);
+        P.wall_lo[k] = wall_index_le(params->bounds_min[k] + h, h);
+        P.wall_hi[k] = wall_index_ge(params->bounds_max[k] - h, h);
         int lo = static_cast<int>(std::floor(P.bmin[k] * P.inv_h - 0.5f)) - 1;
         int hi = static_cast<int>(std::floor(P.bmax[k] * P.inv_h - 0.5f)) + 3;
         P.lo[k] = lo;

@@ -1089,6 +1089,25 @@ inline int class_kind(int material) {
 }
 
 
+// Node indices at the walls, with the f64 arithmetic of apply_grid_boundary
+// (world.rs:561-575: node position i * h against bounds_min + h and
+// bounds_max - h): the largest i with i * h <= bound, and the smallest i with
+// i * h >= bound.  Clamped far beyond the representable cells.
+inline int wall_index_le(double bound, double h) {
+    double q = std::floor(bound / h);
+    long long i = static_cast<long long>(std::min(std::max(q, -1.0e9), 1.0e9));
+    while (static_cast<double>(i + 1) * h <= bound && i < 1000000000LL) ++i;
+    while (static_cast<double>(i) * h > bound && i > -1000000000LL) --i;
+    return static_cast<int>(i);
+}
+inline int wall_index_ge(double bound, double h) {
+    double q = std::ceil(bound / h);
+    long long i = static_cast<long long>(std::min(std::max(q, -1.0e9), 1.0e9));
+    while (static_cast<double>(i - 1) * h >= bound && i > -1000000000LL) --i;
+    while (static_cast<double>(i) * h < bound && i < 1000000000LL) ++i;
+    return static_cast<int>(i);
+}
+
 // Per-scene f32 integration constants (MpmParams + the fixed substep).
 inline SceneParams scene_params(const TmpmParams &params, double dt) {
     SceneParams sc{};
@@ -1110,6 +1129,10 @@ inline SceneParams scene_params(const TmpmParams &params, double dt) {
         float lo = std::floor(sc.bmin[k] * sc.inv_h - 0.5f), hi = std::floor(sc.bmax[k] * sc.inv_h - 0.5f);
         sc.first_base[k] = static_cast<int>(std::max(lo, -1.0e9f)) - 2;
         sc.last_base[k] = static_cast<int>(std::min(hi, 1.0e9f)) + 2;
+        if (params.has_bounds) {
+            sc.wall_lo[k] = wall_index_le(params.bounds_min[k] + params.cell_width, params.cell_width);
+            sc.wall_hi[k] = wall_index_ge(params.bounds_max[k] - params.cell_width, params.cell_width);
+        }
     }
     return sc;
 }

@@ -94,8 +94,14 @@ struct SceneParams {
     int first_base[3];                // escape window of base cells (bounded worlds)
     int live;                         // 0 = removed: dropped by the next re-sort
     int last_base[3], pad;
+    // Wall nodes (bounded worlds): node index i lies within one cell of the
+    // lower wall of axis a when i <= wall_lo[a], of the upper wall when
+    // i >= wall_hi[a].  The host derives both from the f64 comparisons of
+    // apply_grid_boundary (world.rs:561-575), so a node exactly one cell from
+    // a wall is classified as the f64 reference classifies it.
+    int wall_lo[3], wall_hi[3];
 };
-static_assert(sizeof(SceneParams) == 96, "SceneParams layout");
+static_assert(sizeof(SceneParams) == 120, "SceneParams layout");
 
 struct DevObstacle {
     int32_t shape, boundary, cpic_group, plane_offset;
@@ -173,6 +179,11 @@ struct SimParams {
     int shape;            // transfer launch shape (index into kLaunchShapes)
     int block_shift;      // log2 of the grid block edge: kBlockShift (4^3) or kBigBlockShift (8^3)
 };
+// The session's graph cache keys segments by the bytes of a SimParams: neither
+// it nor SceneParams may hold padding, whose contents would be indeterminate.
+static_assert(sizeof(SimParams) == sizeof(SceneParams) + 2 * sizeof(void *) + 10 * sizeof(int),
+              "SimParams must have no padding bytes");
+static_assert(sizeof(SceneParams) == 30 * sizeof(float), "SceneParams must have no padding bytes");
 constexpr int kMaxCpicGroups = 8;
 
 struct ParticleSoA {

@@ -123,12 +123,15 @@ __device__ __forceinline__ void reduce_box(bool valid, const int b[3], uint32_t 
     __syncthreads();
 }
 
-// Box of base cells and colours plus two float sums over the CTA, with one
-// barrier: each warp reduces its lanes and publishes a partial, then every
-// warp combines the partials itself (no second barrier, no shared result).
+// Box of base cells and colours plus the sums and maxima of two non-negative
+// floats over the CTA, with one barrier: each warp reduces its lanes and
+// publishes a partial, then every warp combines the partials itself (no second
+// barrier, no shared result).  The maxima are taken on the float bits, whose
+// integer order is the value order for non-negative floats.
 template <int THREADS, int BS>
 __device__ __forceinline__ void reduce_box_sums(bool valid, const int b[3], uint32_t color, float &sum_a, float &sum_b,
-                                                int (*red)[8], float (*redf)[2], Box &box) {
+                                                float &max_a, float &max_b, int (*red)[8], float (*redf)[4],
+                                                Box &box) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     int r[8];
     for (int a = 0; a < 3; ++a) {
@@ -143,10 +146,14 @@ __device__ __forceinline__ void reduce_box_sums(bool valid, const int b[3], uint
         fa += __shfl_xor_sync(0xffffffffu, fa, off);
         fb += __shfl_xor_sync(0xffffffffu, fb, off);
     }
+    const unsigned ma = __reduce_max_sync(0xffffffffu, __float_as_uint(max_a));
+    const unsigned mb = __reduce_max_sync(0xffffffffu, __float_as_uint(max_b));
     if (lane == 0) {
         for (int a = 0; a < 8; ++a) red[warp][a] = r[a];
         redf[warp][0] = fa;
         redf[warp][1] = fb;
+        redf[warp][2] = __uint_as_float(ma);
+        redf[warp][3] = __uint_as_float(mb);
     }
     __syncthreads();
     constexpr int kWarps = THREADS / 32;
@@ -160,6 +167,8 @@ __device__ __forceinline__ void reduce_box_sums(bool valid, const int b[3], uint
     m[7] = __reduce_max_sync(0xffffffffu, mine ? red[lane][7] : INT_MIN);
     fa = mine ? redf[lane][0] : 0.0f;
     fb = mine ? redf[lane][1] : 0.0f;
+    max_a = __uint_as_float(__reduce_max_sync(0xffffffffu, mine ? __float_as_uint(redf[lane][2]) : 0u));
+    max_b = __uint_as_float(__reduce_max_sync(0xffffffffu, mine ? __float_as_uint(redf[lane][3]) : 0u));
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) {
         fa += __shfl_xor_sync(0xffffffffu, fa, off);
@@ -187,6 +196,13 @@ __device__ __forceinline__ void reduce_box_sums(bool valid, const int b[3], uint
     box.ok = ok ? 1 : 0;
     box.color = static_cast<uint32_t>(m[6]);
 }
+
+// A CTA in which one particle's mass or momentum bound exceeds this share of
+// the CTA's total scatters through the direct path (f32 global atomics per
+// node, each node accurate relative to its own magnitude): its fixed-point
+// scale would be set by that particle alone and would coarsen the quantum of
+// every node its neighbours reach.
+constexpr float kFloatModeShare = 1.0f / 8.0f;
 
 __device__ __forceinline__ void quad_weights(float f, float w[3]) {
     w[0] = 0.5f * (1.5f - f) * (1.5f - f);
@@ -264,7 +280,7 @@ __global__ void __launch_bounds__(THREADS, MINB)
     __shared__ float4 s_tile[kTileNodes];
     float4 *const s_gv = s_tile;
     int (*const s_sc)[kTileNodes] = reinterpret_cast<int (*)[kTileNodes]>(s_tile);
-    __shared__ float s_fred[THREADS / 32][2];
+    __shared__ float s_fred[THREADS / 32][4];
     __shared__ int s_blk[kMaxTileBlocks];
     __shared__ int s_blk2[kMaxTileBlocks];
     __shared__ int s_used[kMaxTileBlocks];
@@ -629,10 +645,12 @@ __global__ void __launch_bounds__(THREADS, MINB)
     }
     // the CTA's box and the sums of the bounds, with one barrier
     if (MODE != kModeP2G && CPIC) ns = particle_namespace(k.color, 1, sp.num_obstacles, obstacles, x);
-    float tot_m = bound_m, tot_p = bound_p;
+    float tot_m = bound_m, tot_p = bound_p, max_m = bound_m, max_p = bound_p;
     Box bx;
-    reduce_box_sums<THREADS, BS>(active, b, ns, tot_m, tot_p, s_red, s_fred, bx);
+    reduce_box_sums<THREADS, BS>(active, b, ns, tot_m, tot_p, max_m, max_p, s_red, s_fred, bx);
     if (MODE == kModeP2G && s_abort) return;
+    // one dominant particle: the whole CTA takes the f32 direct path (CTA-uniform)
+    if (max_m > tot_m * kFloatModeShare || max_p > tot_p * kFloatModeShare) bx.ok = 0;
     if (bx.ok) {
         // every warp has finished its gather (barrier above): the buffer becomes the scatter tile
         for (int t = threadIdx.x; t < bx.nodes; t += THREADS) {
@@ -815,15 +833,16 @@ __global__ void __launch_bounds__(256) k_grid(GridTable g, GridTable nxt, SimPar
         V3f vel = mk(mp.y / mp.x + SCN(gx) * dt, mp.z / mp.x + SCN(gy) * dt, mp.w / mp.x + SCN(gz) * dt);
         V3f pos = mk(static_cast<float>(cx) * h, static_cast<float>(cy) * h, static_cast<float>(cz) * h);
         if (SCN(has_bounds)) {
+            // walls by node index (thresholds from the f64 comparisons, see SceneParams)
+            const int ci[3] = {cx, cy, cz};
             if (SCN(wall_mode) == 1) {
                 bool near = false;
-                for (int a = 0; a < 3; ++a)
-                    near = near || comp(pos, a) <= SCN(bmin[a]) + h || comp(pos, a) >= SCN(bmax[a]) - h;
+                for (int a = 0; a < 3; ++a) near = near || ci[a] <= SCN(wall_lo[a]) || ci[a] >= SCN(wall_hi[a]);
                 if (near) vel = mk(0, 0, 0);
             } else {
                 for (int a = 0; a < 3; ++a) {
-                    float pa = comp(pos, a), va = comp(vel, a);
-                    if ((pa <= SCN(bmin[a]) + h && va < 0.0f) || (pa >= SCN(bmax[a]) - h && va > 0.0f))
+                    const float va = comp(vel, a);
+                    if ((ci[a] <= SCN(wall_lo[a]) && va < 0.0f) || (ci[a] >= SCN(wall_hi[a]) && va > 0.0f))
                         set_comp(vel, a, 0.0f);
                 }
             }

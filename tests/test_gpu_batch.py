@@ -258,3 +258,37 @@ def test_take_returns_what_a_read_returns_and_removes_the_scene():
         assert np.all(arr.velocity[0] == 0.0) and np.all(arr.affine[0] == 0.0)
         assert np.array_equal(arr.position[1], parts.position[1])  # disabled: untouched
         assert np.array_equal(arr.velocity[1], parts.velocity[1])
+
+
+def test_config3_subset_at_size_matches_alone_and_oracle():
+    """Scenes of the 256-scene heterogeneous batch at their real sizes: the
+    largest (262,144 particles on a 128^3 grid, elastic), the largest fluid
+    scene (238,328 particles, 124^3), the smallest (4,096, 32^3) and two
+    mid-sized ones, advanced together as one batch for the workload's 100
+    substeps.  Each scene is compared with the same scene run alone and with
+    the f64 oracle under the relative drift bounds of the configuration-sized
+    parity tests (parity_tol.py): position 1e-3 h, velocity 1e-3 of the largest
+    speed, C 1e-2 of max(|C|, |v| / h), F 1e-4."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    from parity_tol import assert_rel_close
+
+    drift = dict(position=1e-3, velocity=1e-3, affine=1e-2, deformation=1e-4)
+    every = scenes.batch_scenes(256)
+    pick = [49, 174, 6, 0, 1]
+    scs = [every[k] for k in pick]
+    assert scs[0].particles.count == 262144 and scs[0].info["resolution"] == 128
+    assert scs[1].info["material"] == "fluid" and scs[1].particles.count == 238328
+    steps = 100
+    with ThreadPoolExecutor(max_workers=len(scs)) as pool:  # the oracle releases the GIL in its C calls
+        expected = list(pool.map(lambda sc: oracle_run(sc, steps), scs))
+    b = Batch()
+    ids = [b.add_scene(sc.params, sc.particles, sc.dt) for sc in scs]
+    b.run({i: steps for i in ids})
+    for i, k, sc, e in zip(ids, pick, scs, expected):
+        assert b.substeps(i) == steps
+        got = b.particles(i)
+        h = sc.params.cell_width
+        assert_rel_close(e, got, h, drift, f"batch scene {k} vs oracle")
+        assert_rel_close(alone(sc, steps), got, h, drift, f"batch scene {k} vs alone")
+    b.close()
