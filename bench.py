@@ -63,8 +63,8 @@ def parse():
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--batched-scenes", type=int, default=256)
     ap.add_argument("--no-serving", action="store_true")
-    ap.add_argument("--serve-rates", default="200", help="comma-separated arrival rates (requests/s)")
-    ap.add_argument("--serve-requests", type=int, default=12)
+    ap.add_argument("--serve-rates", default="50,200,2000", help="comma-separated arrival rates (requests/s)")
+    ap.add_argument("--serve-requests", type=int, default=100, help="requests per arrival rate")
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--launch-shape", type=int, default=None,
                     help="fix the single-scene launch shape (index of _native.launch_shapes()) instead of tuning it")
@@ -318,7 +318,10 @@ def bench_batched(count: int) -> dict:
 
 def bench_serving(rates, count: int) -> dict:
     """Poisson arrivals of dam-break requests (50-400 substeps) into the
-    continuous-batching server (120 GB budget) and into the one-scene-at-a-time loop."""
+    continuous-batching server (120 GB budget), one run per arrival rate, and
+    the one-scene-at-a-time loop once (every listed rate saturates one GPU, so
+    the plain loop's throughput does not depend on the rate; it runs on the
+    first rate's arrivals)."""
     from tessera_b200 import scenes
     from tessera_b200.batch import Batch
     from tessera_b200.serve import Request, Server, poisson_arrivals, run_plain, summarize
@@ -329,24 +332,38 @@ def bench_serving(rates, count: int) -> dict:
     out = {"workload": "config4-serving", "requests_per_rate": count, "scene": "config2 dam break (4 seeded variants)",
            "particles_per_request": pool[0].particles.count, "substeps": "uniform 50-400 (seeded)",
            "hbm_budget_gb": 120, "chunk_substeps": 32, "unit": METRIC, "rates": []}
-    for rate in rates:
+
+    def requests(rate):
         t = poisson_arrivals(rate, count, seed=int(rate))
-        reqs = [Request(k, float(t[k] - t[0]), pool[k % len(pool)], steps[k]) for k in range(count)]
-        server = Server(batch=Batch(particle_capacity=sum(r.scene.particles.count for r in reqs)), chunk=32,
-                        hbm_budget=120e9)
+        return [Request(k, float(t[k] - t[0]), pool[k % len(pool)], steps[k]) for k in range(count)]
+
+    offered = float(sum(pool[k % len(pool)].particles.count * steps[k] for k in range(count)))
+    for rate in rates:
+        reqs = requests(rate)
+        # rows for the scenes the 120 GB budget can hold at once (the batch grows on demand beyond)
+        cap = min(sum(r.scene.particles.count for r in reqs), 60 * pool[0].particles.count)
+        server = Server(batch=Batch(particle_capacity=cap), chunk=32, hbm_budget=120e9)
         served, span = server.run(reqs)
         s_served = summarize(served, span)
         s_served.update(batches=server.batches, peak_resident=server.peak_resident,
-                        peak_gb=server.peak_bytes / 1e9, launch_shape=shape_summary(server.batch.launch_shape()))
+                        peak_gb=server.peak_bytes / 1e9, launch_shape=shape_summary(server.batch.launch_shape()),
+                        offered_particle_substeps_per_s=offered / max(reqs[-1].arrival, 1e-9))
         tm = dict(server.timing)
         prep = tm.pop("prepare_s")
         tm.update(prepare_mean_s=float(np.mean(prep)) if prep else None, prepare_max_s=max(prep) if prep else None)
         s_served["timing"] = tm
         server.batch.close()
-        plain, span_p = run_plain(reqs)
-        s_plain = summarize(plain, span_p)
-        out["rates"].append({"rate": rate, "served": s_served, "plain": s_plain,
-                             "throughput_ratio": s_served["particle_substeps_per_s"] / s_plain["particle_substeps_per_s"]})
+        out["rates"].append({"rate": rate, "served": s_served})
+    # the plain loop is host-bound at ~0.7 G particle-substeps/s (a session per
+    # request: upload, substeps, readback), so it runs the first half of the
+    # requests; its throughput does not depend on how many it runs
+    plain_n = max(1, count // 2)
+    plain, span_p = run_plain(requests(rates[0])[:plain_n])
+    s_plain = summarize(plain, span_p)
+    s_plain["arrivals"] = f"the first {plain_n} arrivals of the {rates[0]} req/s run"
+    out["plain"] = s_plain
+    for r in out["rates"]:
+        r["throughput_ratio"] = r["served"]["particle_substeps_per_s"] / s_plain["particle_substeps_per_s"]
     return out
 
 

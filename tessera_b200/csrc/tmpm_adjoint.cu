@@ -36,6 +36,10 @@ namespace {
 
 constexpr int kRows = 24;  // x 0-2, v 3-5, C 6-14, F 15-23 (matrices column-major: col * 3 + row)
 constexpr uint32_t kErrGrid = 1u;  // a stencil left the node array
+// Threads per CTA of the particle kernels.  A 64k-particle rollout is ~1.7
+// waves of 256-thread CTAs on 148 SMs (some SMs with two CTAs, some with
+// one); 64-thread CTAs spread the latency-bound particle work evenly.
+constexpr int kParticleThreads = 64;
 
 struct AdjParams {
     float h, inv_h, inv_d, dt;
@@ -128,8 +132,10 @@ __device__ __forceinline__ void lame(float E, float nu, float &lambda, float &mu
 
 // ---------------------------------------------------------------- forward
 
+// Rout (optional): the polar factor R of each particle's F, 9 rows, for the
+// P2G adjoint of the same substep.
 __global__ void k_p2g(AdjParams P, Consts K, const float *__restrict__ S, const float *__restrict__ E,
-                      float4 *grid, uint32_t *err) {
+                      float4 *grid, uint32_t *err, float *__restrict__ Rout) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= P.n) return;
     const size_t st = P.stride;
@@ -138,6 +144,18 @@ __global__ void k_p2g(AdjParams P, Consts K, const float *__restrict__ S, const 
     float lambda, mu;
     lame(E[i], K.nu[i], lambda, mu);
     M3f R = polar_rotation(F);
+    if (Rout) {
+        const M3f &Rs = R;
+        Rout[0 * st + i] = Rs.c0.x;
+        Rout[1 * st + i] = Rs.c0.y;
+        Rout[2 * st + i] = Rs.c0.z;
+        Rout[3 * st + i] = Rs.c1.x;
+        Rout[4 * st + i] = Rs.c1.y;
+        Rout[5 * st + i] = Rs.c1.z;
+        Rout[6 * st + i] = Rs.c2.x;
+        Rout[7 * st + i] = Rs.c2.y;
+        Rout[8 * st + i] = Rs.c2.z;
+    }
     float J = det(F);
     M3f tau = scale(mul_bt(sub(F, R), F), 2.0f * mu);
     float iso = lambda * (J - 1.0f) * J;
@@ -346,7 +364,7 @@ __global__ void k_grid_back(AdjParams P, const float4 *__restrict__ grid, const 
 // state (Ain) and dL/dE accumulated into Eb.
 __global__ void k_p2g_back(AdjParams P, Consts K, const float *__restrict__ S, const float *__restrict__ E,
                            const float4 *__restrict__ gmb, const float *__restrict__ Q, float *__restrict__ Ain,
-                           float *__restrict__ Eb) {
+                           float *__restrict__ Eb, const float *__restrict__ Rin) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= P.n) return;
     const size_t st = P.stride;
@@ -356,7 +374,7 @@ __global__ void k_p2g_back(AdjParams P, Consts K, const float *__restrict__ S, c
     float lambda, mu;
     const float nu = K.nu[i];
     lame(E[i], nu, lambda, mu);
-    M3f R = polar_rotation(F);
+    const M3f R = load_m(Rin, st, 0, i);  // the polar factor the replayed P2G computed
     float J = det(F);
     M3f FmR_FT = mul_bt(sub(F, R), F);
     M3f tau = scale(FmR_FT, 2.0f * mu);
@@ -443,6 +461,11 @@ struct TmpmAdjoint {
     DevBuf<uint8_t> fixed;
     DevBuf<float> ckpt, seg, adj[2], part;
     DevBuf<float4> grid, gv, gvb;
+    // per substep of the segment being replayed: the grid after P2G (mass and
+    // momentum), the node velocities and the particles' polar factors, so the
+    // adjoint sweep reuses them instead of recomputing P2G and the grid update
+    DevBuf<float4> seg_grid, seg_gv;
+    DevBuf<float> seg_R;
     DevBuf<uint32_t> err;
     bool have_forward = false;
     std::string last_error;
@@ -499,19 +522,29 @@ struct TmpmAdjoint {
         const uint32_t segments = (substeps + every - 1) / every;
         for (int sg = static_cast<int>(segments) - 1; sg >= 0; --sg) {
             const uint32_t s0 = sg * every, s1 = std::min(substeps, s0 + every);
-            // replay the segment: seg[j] = state at substep s0 + j
+            // replay the segment: seg[j] = state at substep s0 + j, with the
+            // grid, node velocities and polar factors of each substep kept
             cudaMemcpyAsync(seg.ptr, ckpt.ptr + sg * state_floats(), sizeof(float) * state_floats(),
                             cudaMemcpyDeviceToDevice, stream);
-            for (uint32_t s = s0; s + 1 < s1; ++s)
-                substep(seg.ptr + (s - s0) * state_floats(), seg.ptr + (s - s0 + 1) * state_floats());
+            for (uint32_t s = s0; s < s1; ++s) {
+                const uint32_t j = s - s0;
+                float4 *g = seg_grid.ptr + static_cast<size_t>(j) * nodes, *v = seg_gv.ptr + static_cast<size_t>(j) * nodes;
+                p2g_grid(seg.ptr + j * state_floats(), g, v, seg_R.ptr + static_cast<size_t>(j) * 9 * n);
+                if (s + 1 < s1)
+                    k_g2p<<<blocks_n(), kParticleThreads, 0, stream>>>(P, consts(), seg.ptr + j * state_floats(),
+                                                                       seg.ptr + (j + 1) * state_floats(), v);
+            }
             for (int s = static_cast<int>(s1) - 1; s >= static_cast<int>(s0); --s) {
-                const float *S = seg.ptr + (s - s0) * state_floats();
-                p2g_grid(S);
+                const uint32_t j = s - s0;
+                const float *S = seg.ptr + j * state_floats();
+                const float4 *g = seg_grid.ptr + static_cast<size_t>(j) * nodes, *v = seg_gv.ptr + static_cast<size_t>(j) * nodes;
                 cudaMemsetAsync(gvb.ptr, 0, sizeof(float4) * nodes, stream);
-                k_g2p_back<<<blocks_n(), 256, 0, stream>>>(P, consts(), S, gv.ptr, adj[a].ptr, part.ptr, gvb.ptr);
-                k_grid_back<<<blocks_nodes(), 256, 0, stream>>>(P, grid.ptr, gv.ptr, gvb.ptr, nodes);
-                k_p2g_back<<<blocks_n(), 256, 0, stream>>>(P, consts(), S, E.ptr, gvb.ptr, part.ptr, adj[a ^ 1].ptr,
-                                                           Ebar.ptr);
+                k_g2p_back<<<blocks_n(), kParticleThreads, 0, stream>>>(P, consts(), S, v, adj[a].ptr, part.ptr,
+                                                                        gvb.ptr);
+                k_grid_back<<<blocks_nodes(), 256, 0, stream>>>(P, g, v, gvb.ptr, nodes);
+                k_p2g_back<<<blocks_n(), kParticleThreads, 0, stream>>>(P, consts(), S, E.ptr, gvb.ptr, part.ptr,
+                                                                        adj[a ^ 1].ptr, Ebar.ptr,
+                                                                        seg_R.ptr + static_cast<size_t>(j) * 9 * n);
                 a ^= 1;
             }
         }
@@ -526,18 +559,18 @@ struct TmpmAdjoint {
     }
     Consts consts() const { return Consts{mass.ptr, vol.ptr, radius.ptr, damping.ptr, nu.ptr, fixed.ptr}; }
     size_t state_floats() const { return kRows * n; }
-    int blocks_n() const { return static_cast<int>((n + 255) / 256); }
+    int blocks_n() const { return static_cast<int>((n + kParticleThreads - 1) / kParticleThreads); }
     int blocks_nodes() const { return (nodes + 255) / 256; }
 
-    // P2G + grid of state S into grid / gv.
-    void p2g_grid(const float *S) {
-        cudaMemsetAsync(grid.ptr, 0, sizeof(float4) * nodes, stream);
-        k_p2g<<<blocks_n(), 256, 0, stream>>>(P, consts(), S, E.ptr, grid.ptr, err.ptr);
-        k_grid<<<blocks_nodes(), 256, 0, stream>>>(P, grid.ptr, gv.ptr, nodes);
+    // P2G + grid of state S into g / v (and the polar factors into R when given).
+    void p2g_grid(const float *S, float4 *g, float4 *v, float *R) {
+        cudaMemsetAsync(g, 0, sizeof(float4) * nodes, stream);
+        k_p2g<<<blocks_n(), kParticleThreads, 0, stream>>>(P, consts(), S, E.ptr, g, err.ptr, R);
+        k_grid<<<blocks_nodes(), 256, 0, stream>>>(P, g, v, nodes);
     }
     void substep(const float *S, float *Sn) {
-        p2g_grid(S);
-        k_g2p<<<blocks_n(), 256, 0, stream>>>(P, consts(), S, Sn, gv.ptr);
+        p2g_grid(S, grid.ptr, gv.ptr, nullptr);
+        k_g2p<<<blocks_n(), kParticleThreads, 0, stream>>>(P, consts(), S, Sn, gv.ptr);
     }
 
     TmpmStatus check_err() {
@@ -739,7 +772,9 @@ TmpmStatus tmpm_adjoint_create(const TmpmParams *params, const TmpmParticleArray
         (e = a->nu.alloc(n)) || (e = a->E.alloc(n)) || (e = a->Ebar.alloc(n)) || (e = a->fixed.alloc(n)) ||
         (e = a->ckpt.alloc(segments * sf)) || (e = a->seg.alloc(std::max<size_t>(a->every, 2) * sf)) ||
         (e = a->adj[0].alloc(sf)) || (e = a->adj[1].alloc(sf)) || (e = a->part.alloc(sf)) ||
-        (e = a->grid.alloc(nodes)) || (e = a->gv.alloc(nodes)) || (e = a->gvb.alloc(nodes)) || (e = a->err.alloc(1))) {
+        (e = a->grid.alloc(nodes)) || (e = a->gv.alloc(nodes)) || (e = a->gvb.alloc(nodes)) || (e = a->err.alloc(1)) ||
+        (e = a->seg_grid.alloc(static_cast<size_t>(a->every) * nodes)) ||
+        (e = a->seg_gv.alloc(static_cast<size_t>(a->every) * nodes)) || (e = a->seg_R.alloc(a->every * 9 * n))) {
         g_last_error = std::string("adjoint setup: ") + cudaGetErrorString(e);
         return TMPM_ERR_DEVICE;
     }
