@@ -305,16 +305,25 @@ def binning_reference(position_f32: np.ndarray, cell_width: float):
     return cells, keys, perm
 
 
+def lane_cell(lane):
+    """Cell group of a transfer warp's lane (the device's lane_cell): quarter-warp
+    p = lane // 8 takes a 1 x 2 x 4 slab of the chunk's 2 x 4 x 4 Morton group."""
+    lane = np.asarray(lane)
+    p, q = lane >> 3, lane & 7
+    return (p & 1) * 16 + ((q >> 1) & 1) * 8 + (p >> 1) * 4 + (q >> 2) * 2 + (q & 1)
+
+
 def storage_order(perm: np.ndarray, chunk: int = 256, group: int = 8) -> np.ndarray:
     """Device storage order after a single-scene re-sort: each full chunk of 256
     sorted particles is stored transposed (position kk holds sorted element
-    (kk % 32) * 8 + kk // 32 of its chunk); the last partial chunk is in order."""
+    lane_cell(kk % 32) * 8 + kk // 32 of its chunk); the last partial chunk is in
+    order."""
     perm = np.asarray(perm)
     n = len(perm)
     src = np.arange(n)
     full = (n // chunk) * chunk
     kk = np.arange(full) % chunk
-    src[:full] = (np.arange(full) // chunk) * chunk + (kk % 32) * group + kk // 32
+    src[:full] = (np.arange(full) // chunk) * chunk + lane_cell(kk % 32) * group + kk // 32
     return perm[src]
 
 

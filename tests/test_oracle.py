@@ -551,5 +551,7 @@ def test_binning_reference_is_stable_and_blocks_match_floor_division():
     # storage order: a permutation, transposed within full 256-chunks
     order = O.storage_order(perm)
     assert np.array_equal(np.sort(order), np.sort(perm))
+    assert order[2] == perm[64] and order[8] == perm[128]  # quarter-warps take slabs of the cell group
+    assert sorted(O.lane_cell(np.arange(32))) == list(range(32))
     assert order[1] == perm[8] and order[32] == perm[1] and np.array_equal(order[-(len(perm) % 256):],
                                                                             perm[-(len(perm) % 256):])
