@@ -23,6 +23,8 @@ maximum, gpu.rs:303-322) over the whole scene.
   adjoint  the differentiable rollout (64k-particle corotated block, 256
          substeps, checkpoints every 16): forward and adjoint wall time through
          the C ABI (host arrays in and out).
+  obstacle the benchmark scene with a rigid sphere in the flow: per-launch time
+         of the fused transfer variant that carries the obstacle contact.
 
 `--impl reference` times the reference's CPU path (its C++ restatement in
 oracle/, f64, ordered-map grid) on the host cores for the same workload.
@@ -66,9 +68,10 @@ def parse():
     ap.add_argument("--serve-rates", default="50,200,2000", help="comma-separated arrival rates (requests/s)")
     ap.add_argument("--serve-requests", type=int, default=100, help="requests per arrival rate")
     ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--no-obstacle", action="store_true")
     ap.add_argument("--launch-shape", type=int, default=None,
                     help="fix the single-scene launch shape (index of _native.launch_shapes()) instead of tuning it")
-    ap.add_argument("--only", choices=["batched", "serving", "adjoint"],
+    ap.add_argument("--only", choices=["batched", "serving", "adjoint", "obstacle"],
                     help="run one section alone and print its result (profiling; not the benchmark line)")
     return ap.parse_args()
 
@@ -316,6 +319,46 @@ def bench_batched(count: int) -> dict:
     }
 
 
+def bench_batched_parallel(count: int, world: int, rank: int) -> dict:
+    """The heterogeneous batch split across ranks by scene (no data-path
+    collective): each rank advances the scenes that placement by device
+    footprint assigns to it (largest first onto the least-loaded rank, the same
+    on every rank) in its own multi-scene batch; throughput = all ranks' work
+    over the slowest rank's device time."""
+    import torch
+
+    from tessera_b200 import scenes
+    from tessera_b200.batch import Batch, home_blocks, scene_bytes
+    from tessera_b200.replicas import my_items
+
+    scs = scenes.batch_scenes(count)
+    steps = scs[0].substeps
+    sizes = [scene_bytes(s.particles.count, home_blocks(s.particles.position, s.params.cell_width)) for s in scs]
+    mine = [scs[k] for k in my_items(sizes, world, rank)]
+    b = Batch()
+    ids = [b.add_scene(s.params, s.particles, s.dt) for s in mine]
+    for _ in range(16):  # the launch-shape trials before the timed batches
+        b.run({i: steps for i in ids})
+        if b.launch_shape()["shape"] is not None:
+            break
+    barrier(world)
+    torch.cuda.synchronize()
+    dev = []
+    for _ in range(3):
+        b.run({i: steps for i in ids})
+        dev.append(b.last_ms())
+    fails = sum(b.status(i) != 0 for i in ids)
+    b.close()
+    ms = allreduce_max(float(np.median(dev)), world)
+    work = allreduce_sum(float(sum(s.particles.count for s in mine)) * steps, world)
+    fails = int(allreduce_sum(float(fails), world))
+    return {"workload": "config3-heterogeneous-batch, scene-parallel", "scenes": count, "ranks": world,
+            "placement": "by device footprint, largest first onto the least-loaded rank",
+            "scenes_on_rank0": len(mine), "batched": {"value": work / (ms / 1e3), "ms_per_batch": ms,
+                                                      "failed_scenes": fails}, "unit": METRIC,
+            "timing": "CUDA events around each rank's batch, max over ranks"}
+
+
 def bench_serving(rates, count: int) -> dict:
     """Poisson arrivals of dam-break requests (50-400 substeps) into the
     continuous-batching server (120 GB budget), one run per arrival rate, and
@@ -364,6 +407,36 @@ def bench_serving(rates, count: int) -> dict:
     out["plain"] = s_plain
     for r in out["rates"]:
         r["throughput_ratio"] = r["served"]["particle_substeps_per_s"] / s_plain["particle_substeps_per_s"]
+    return out
+
+
+def bench_obstacle(free_launch_ms: float) -> dict:
+    """The benchmark scene with a rigid sphere just ahead of the column (the
+    fluid reaches it within the first ~400 substeps): per-launch device time of
+    the fused transfer in the variant that carries the obstacle contact, at the
+    64-register (256 x 4) and 80-register (256 x 3) shapes on 8^3 blocks, after
+    the same 18 warm-up segments of 64 substeps, beside the obstacle-free
+    kernel's time from the single-scene section."""
+    from tessera_b200 import scenes
+    from tessera_b200.session import Session
+
+    sc = scenes.dam_break_obstacle()
+    c = np.asarray(sc.obstacles[0].center)
+    r = sc.obstacles[0].dims[0]
+    out = {"workload": "config2 dam break + sphere obstacle", "particles": sc.particles.count,
+           "obstacle": sc.info["obstacle"], "obstacle_free_launch_ms": free_launch_ms, "launch_ms": {}}
+    for cfg, name in ((3, "256x4/8^3"), (5, "256x3/8^3")):
+        s = Session(sc.params, sc.particles, sc.dt, obstacles=sc.obstacles, launch_shape=cfg)
+        for _ in range(18):
+            s.bench_substeps(BATCH)
+        s.synchronize()
+        _, kms = s.bench_substeps(BATCH, per_kernel=True)
+        s.synchronize()
+        out["launch_ms"][name] = float(kms[2])
+        pos = s.read(("position",))["position"]
+        out.setdefault("particles_within_one_cell_of_the_sphere", {})[name] = int(
+            np.count_nonzero(np.linalg.norm(pos - c, axis=1) < r + sc.params.cell_width))
+        s.close()
     return out
 
 
@@ -534,11 +607,16 @@ def run_tessera(args, world, rank, local):
     batched = serving = None
     if rank == 0 and world == 1 and not args.no_batched:
         batched = bench_batched(args.batched_scenes)
+    elif world > 1 and not args.no_batched:  # every rank: its share of the scenes
+        batched = bench_batched_parallel(args.batched_scenes, world, rank)
     if rank == 0 and world == 1 and not args.no_serving:
         serving = bench_serving([float(r) for r in args.serve_rates.split(",") if r], args.serve_requests)
     adjoint = None
     if rank == 0 and world == 1 and not args.no_adjoint:
         adjoint = bench_adjoint()
+    obstacle = None
+    if rank == 0 and world == 1 and not args.no_obstacle:
+        obstacle = bench_obstacle(g2p2g_ms)
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
@@ -558,6 +636,7 @@ def run_tessera(args, world, rank, local):
             "batched": batched,
             "serving": serving,
             "adjoint": adjoint,
+            "obstacle": obstacle,
             "small_configs": small,
         }
         print(json.dumps(line), flush=True)
@@ -570,6 +649,8 @@ def main():
             res = bench_batched(args.batched_scenes)
         elif args.only == "serving":
             res = bench_serving([float(r) for r in args.serve_rates.split(",") if r], args.serve_requests)
+        elif args.only == "obstacle":
+            res = bench_obstacle(float("nan"))
         else:
             res = bench_adjoint()
         print(json.dumps(res), flush=True)

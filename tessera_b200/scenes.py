@@ -90,6 +90,23 @@ def dam_break(seed=2, side=2.2, resolution=256, column=(0.4, 0.8, 1.0), bulk=1e4
                  info=dict(particles=allp.count, fluid=len(fluid), cubes=[c.tolist() for c in cubes], cell_width=h))
 
 
+def dam_break_obstacle(seed=2, scale=1.0, center=(0.40, 0.40, 0.10), radius=0.12, friction=0.3):
+    """Config 2 with a rigid sphere obstacle straddling the column's front face
+    near the floor (the particles it would hold, and those within half a cell
+    of its surface, are left out): the column collapses around and over it,
+    so the particle and grid contact run from the first substep on."""
+    sc = dam_break(seed=seed, scale=scale, name="config2-dam-break-sphere")
+    c = np.asarray(center, dtype=np.float64)
+    c[1] *= scale if scale < 1.0 else 1.0
+    h = sc.params.cell_width
+    keep = np.linalg.norm(sc.particles.position - c, axis=1) > radius + 0.5 * h
+    sc.particles = sc.particles.select(np.nonzero(keep)[0])
+    sc.obstacles = [Obstacle.sphere(tuple(c), radius, friction=friction)]
+    sc.info["obstacle"] = dict(shape="sphere", center=c.tolist(), radius=radius, friction=friction)
+    sc.info["particles"] = sc.particles.count
+    return sc
+
+
 def adjoint_block(seed=5, young=5e3, poisson=0.3, density=1000.0, dt=1e-4, substeps=256, jitter=0.5,
                   cells=20, velocity=None, name="config5-corotated-block"):
     """Config 5: 64k-particle corotated block (20^3 cells at 8 per cell) on a 64^3 grid
