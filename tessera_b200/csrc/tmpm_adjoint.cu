@@ -25,6 +25,7 @@
 // dpos_i^T with s_c, u_c the values at the stencil's centre node, which is the
 // same sum in exact arithmetic.
 
+#include <climits>
 #include <memory>
 
 #include "tmpm_device.cuh"
@@ -36,10 +37,7 @@ namespace {
 
 constexpr int kRows = 24;  // x 0-2, v 3-5, C 6-14, F 15-23 (matrices column-major: col * 3 + row)
 constexpr uint32_t kErrGrid = 1u;  // a stencil left the node array
-// Threads per CTA of the particle kernels.  A 64k-particle rollout is ~1.7
-// waves of 256-thread CTAs on 148 SMs (some SMs with two CTAs, some with
-// one); 64-thread CTAs spread the latency-bound particle work evenly.
-constexpr int kParticleThreads = 64;
+
 
 struct AdjParams {
     float h, inv_h, inv_d, dt;
@@ -125,6 +123,148 @@ __device__ __forceinline__ int node_at(const AdjParams &P, const Stencil &s, int
     return (lx * P.dim[1] + ly) * P.dim[2] + lz;
 }
 
+// ---- box tiles.  A CTA stages the nodes its particles reach (the box of
+// their base cells, 2 cells wider) in shared memory: gathers read the tile
+// instead of 27 global loads per particle, scatters accumulate in it in 32-bit
+// fixed point (one power-of-two scale per quantity from the CTA's bounds, as in
+// the transfer kernels) and flush one float4 atomic per touched node.  A CTA
+// whose box does not fit, leaves the node array, or has one particle that
+// dominates a bound (above 1/8 of the CTA's total) takes the direct path.
+constexpr int kTileThreads = 256;
+constexpr int kAdjTile = 2048;  // nodes (32 KB of float4)
+
+struct TileBox {
+    int lo[3], dim[3], nodes, ok;
+};
+
+// Box of the valid particles' base cells, with the sums and maxima of two
+// non-negative bounds over the CTA; one barrier (every warp combines the
+// per-warp partials itself).
+template <int T>
+__device__ void tile_box(const AdjParams &P, bool valid, const int b[3], float &sa, float &sb, float &ma, float &mb,
+                         int (*red)[6], float (*redf)[4], TileBox &box) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int r[6];
+    for (int a = 0; a < 3; ++a) {
+        r[a] = __reduce_min_sync(0xffffffffu, valid ? b[a] : INT_MAX);
+        r[3 + a] = __reduce_max_sync(0xffffffffu, valid ? b[a] : INT_MIN);
+    }
+    float fa = sa, fb = sb;
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        fa += __shfl_xor_sync(0xffffffffu, fa, off);
+        fb += __shfl_xor_sync(0xffffffffu, fb, off);
+    }
+    const unsigned xa = __reduce_max_sync(0xffffffffu, __float_as_uint(ma));
+    const unsigned xb = __reduce_max_sync(0xffffffffu, __float_as_uint(mb));
+    if (lane == 0) {
+        for (int a = 0; a < 6; ++a) red[warp][a] = r[a];
+        redf[warp][0] = fa;
+        redf[warp][1] = fb;
+        redf[warp][2] = __uint_as_float(xa);
+        redf[warp][3] = __uint_as_float(xb);
+    }
+    __syncthreads();
+    const bool mine = lane < T / 32;
+    int m[6];
+    for (int a = 0; a < 3; ++a) {
+        m[a] = __reduce_min_sync(0xffffffffu, mine ? red[lane][a] : INT_MAX);
+        m[3 + a] = __reduce_max_sync(0xffffffffu, mine ? red[lane][3 + a] : INT_MIN);
+    }
+    fa = mine ? redf[lane][0] : 0.0f;
+    fb = mine ? redf[lane][1] : 0.0f;
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        fa += __shfl_xor_sync(0xffffffffu, fa, off);
+        fb += __shfl_xor_sync(0xffffffffu, fb, off);
+    }
+    sa = fa;
+    sb = fb;
+    ma = __uint_as_float(__reduce_max_sync(0xffffffffu, mine ? __float_as_uint(redf[lane][2]) : 0u));
+    mb = __uint_as_float(__reduce_max_sync(0xffffffffu, mine ? __float_as_uint(redf[lane][3]) : 0u));
+    bool ok = m[0] <= m[3];
+    int nodes = 1;
+    for (int a = 0; a < 3 && ok; ++a) {
+        box.lo[a] = m[a];
+        box.dim[a] = m[3 + a] - m[a] + 3;
+        ok = box.dim[a] <= 64 && box.lo[a] >= P.lo[a] && box.lo[a] + box.dim[a] <= P.lo[a] + P.dim[a];
+        nodes *= box.dim[a];
+    }
+    box.nodes = nodes;
+    box.ok = ok && nodes <= kAdjTile;
+}
+
+// The box's nodes of the dense array `src` into the tile (16-byte cp.async copies), then a barrier.
+template <int T>
+__device__ void fill_tile(const AdjParams &P, const TileBox &box, const float4 *src, float4 *tile) {
+    for (int t = threadIdx.x; t < box.nodes; t += T) {
+        const int tz = t % box.dim[2], q = t / box.dim[2];
+        const int ty = q % box.dim[1], tx = q / box.dim[1];
+        const int id = ((box.lo[0] + tx - P.lo[0]) * P.dim[1] + (box.lo[1] + ty - P.lo[1])) * P.dim[2] +
+                       (box.lo[2] + tz - P.lo[2]);
+        const unsigned dst = static_cast<unsigned>(__cvta_generic_to_shared(tile + t));
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src + id) : "memory");
+    }
+    asm volatile("cp.async.wait_all;" ::: "memory");
+    __syncthreads();
+}
+
+// Where a particle's 27 nodes are read: the CTA's tile (t0 = the particle's
+// base node in it) or, without one, the dense array.
+struct TileRef {
+    const float4 *tile;
+    int t0, d1, d2;
+};
+__device__ __forceinline__ TileRef tile_ref(const TileBox &box, const Stencil &s, const float4 *tile) {
+    TileRef r;
+    r.tile = box.ok ? tile : nullptr;
+    r.d1 = box.dim[1];
+    r.d2 = box.dim[2];
+    r.t0 = ((s.b[0] - box.lo[0]) * box.dim[1] + (s.b[1] - box.lo[1])) * box.dim[2] + (s.b[2] - box.lo[2]);
+    return r;
+}
+// TILE: read the CTA's tile (every node of a valid particle is in it);
+// otherwise the dense array, where a node outside it reads as absent.
+template <bool TILE>
+__device__ __forceinline__ bool node_value(const AdjParams &P, const Stencil &s, const float4 *glob, const TileRef &tr,
+                                           int a, int b, int c, float4 &g) {
+    if (TILE) {
+        g = tr.tile[tr.t0 + (a * tr.d1 + b) * tr.d2 + c];
+        return true;
+    }
+    const int id = node_at(P, s, a, b, c);
+    if (id < 0) return false;
+    g = glob[id];
+    return true;
+}
+
+// Largest power of two s with total * s <= 2^30 (exponent clamped to the normal range).
+__device__ __forceinline__ float pow2_scale30(float total) {
+    float e = floorf(30.0f - log2f(fmaxf(total, 1e-30f)));
+    e = fminf(fmaxf(e, -120.0f), 120.0f);
+    return exp2f(e);
+}
+
+// The tile's fixed-point sums (component-major, `comps` of 4) added to the
+// dense array: one float4 atomic per node with a non-zero sum.
+template <int T>
+__device__ void flush_tile(const AdjParams &P, const TileBox &box, int (*sc)[kAdjTile], int comps, float inv0,
+                           float inv1, float4 *dst) {
+    for (int t = threadIdx.x; t < box.nodes; t += T) {
+        const int v0 = sc[0][t], v1 = sc[1][t], v2 = sc[2][t], v3 = comps > 3 ? sc[3][t] : 0;
+        if ((v0 | v1 | v2 | v3) == 0) continue;
+        const int tz = t % box.dim[2], q = t / box.dim[2];
+        const int ty = q % box.dim[1], tx = q / box.dim[1];
+        const int id = ((box.lo[0] + tx - P.lo[0]) * P.dim[1] + (box.lo[1] + ty - P.lo[1])) * P.dim[2] +
+                       (box.lo[2] + tz - P.lo[2]);
+        const float4 val = comps > 3 ? make_float4(v0 * inv0, v1 * inv1, v2 * inv1, v3 * inv1)
+                                     : make_float4(v0 * inv0, v1 * inv0, v2 * inv0, 0.0f);
+        red_add_v4(dst + id, val);
+    }
+}
+
+__device__ __forceinline__ unsigned fx_round(float v) { return static_cast<unsigned>(__float2int_rn(v)); }
+
 __device__ __forceinline__ void lame(float E, float nu, float &lambda, float &mu) {
     lambda = E * nu / ((1.0f + nu) * (1.0f - 2.0f * nu));
     mu = E / (2.0f * (1.0f + nu));
@@ -134,17 +274,22 @@ __device__ __forceinline__ void lame(float E, float nu, float &lambda, float &mu
 
 // Rout (optional): the polar factor R of each particle's F, 9 rows, for the
 // P2G adjoint of the same substep.
-__global__ void k_p2g(AdjParams P, Consts K, const float *__restrict__ S, const float *__restrict__ E,
-                      float4 *grid, uint32_t *err, float *__restrict__ Rout) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= P.n) return;
+__global__ void __launch_bounds__(kTileThreads) k_p2g(AdjParams P, Consts K, const float *__restrict__ S,
+                                                      const float *__restrict__ E, float4 *grid, uint32_t *err,
+                                                      float *__restrict__ Rout) {
+    __shared__ float4 s_tile[kAdjTile];
+    __shared__ int s_red[kTileThreads / 32][6];
+    __shared__ float s_redf[kTileThreads / 32][4];
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool valid = i < P.n;
+    const int ic = valid ? i : 0;
     const size_t st = P.stride;
-    V3f x = load_v(S, st, 0, i), v = load_v(S, st, 3, i);
-    M3f C = load_m(S, st, 6, i), F = load_m(S, st, 15, i);
+    V3f x = load_v(S, st, 0, ic), v = load_v(S, st, 3, ic);
+    M3f C = load_m(S, st, 6, ic), F = load_m(S, st, 15, ic);
     float lambda, mu;
-    lame(E[i], K.nu[i], lambda, mu);
+    lame(E[ic], K.nu[ic], lambda, mu);
     M3f R = polar_rotation(F);
-    if (Rout) {
+    if (Rout && valid) {
         const M3f &Rs = R;
         Rout[0 * st + i] = Rs.c0.x;
         Rout[1 * st + i] = Rs.c0.y;
@@ -162,23 +307,64 @@ __global__ void k_p2g(AdjParams P, Consts K, const float *__restrict__ S, const 
     tau.c0.x += iso;
     tau.c1.y += iso;
     tau.c2.z += iso;
-    const float m = K.mass[i];
-    M3f A = add(scale(tau, -P.dt * K.vol[i] * P.inv_d), scale(C, m));
+    const float m = K.mass[ic];
+    M3f A = add(scale(tau, -P.dt * K.vol[ic] * P.inv_d), scale(C, m));
     Stencil s;
     stencil(x, P.inv_h, s);
-    for (int a = 0; a < 3; ++a)
-        for (int b = 0; b < 3; ++b)
-            for (int c = 0; c < 3; ++c) {
-                int id = node_at(P, s, a, b, c);
-                if (id < 0) {
-                    atomicOr(err, kErrGrid);
-                    continue;
+    // node sums are bounded by the CTA's sums of m and |m v| + 1.5 h sum |A| (weights sum to one)
+    float bm = 0.0f, bp = 0.0f;
+    if (valid) {
+        const V3f mv = v * m;
+        bm = m;
+        bp = fmaxf(fmaxf(fabsf(mv.x) + 1.5f * P.h * (fabsf(A.c0.x) + fabsf(A.c1.x) + fabsf(A.c2.x)),
+                         fabsf(mv.y) + 1.5f * P.h * (fabsf(A.c0.y) + fabsf(A.c1.y) + fabsf(A.c2.y))),
+                   fabsf(mv.z) + 1.5f * P.h * (fabsf(A.c0.z) + fabsf(A.c1.z) + fabsf(A.c2.z)));
+        if (!(bp < 1e30f)) bp = 1e30f;
+    }
+    float sum_m = bm, sum_p = bp, max_m = bm, max_p = bp;
+    TileBox box;
+    tile_box<kTileThreads>(P, valid, s.b, sum_m, sum_p, max_m, max_p, s_red, s_redf, box);
+    if (!box.ok || max_m > 0.125f * sum_m || max_p > 0.125f * sum_p) {  // direct path (CTA-uniform)
+        if (!valid) return;
+        for (int a = 0; a < 3; ++a)
+            for (int b = 0; b < 3; ++b)
+                for (int c = 0; c < 3; ++c) {
+                    int id = node_at(P, s, a, b, c);
+                    if (id < 0) {
+                        atomicOr(err, kErrGrid);
+                        continue;
+                    }
+                    float w = s.w[0][a] * s.w[1][b] * s.w[2][c];
+                    V3f dpos = mk((a - s.fx[0]) * P.h, (b - s.fx[1]) * P.h, (c - s.fx[2]) * P.h);
+                    V3f mom = v * m + mul(A, dpos);
+                    red_add_v4(grid + id, make_float4(w * m, w * mom.x, w * mom.y, w * mom.z));
                 }
-                float w = s.w[0][a] * s.w[1][b] * s.w[2][c];
-                V3f dpos = mk((a - s.fx[0]) * P.h, (b - s.fx[1]) * P.h, (c - s.fx[2]) * P.h);
-                V3f mom = v * m + mul(A, dpos);
-                red_add_v4(grid + id, make_float4(w * m, w * mom.x, w * mom.y, w * mom.z));
-            }
+        return;
+    }
+    int (*sc)[kAdjTile] = reinterpret_cast<int (*)[kAdjTile]>(s_tile);
+    for (int t = threadIdx.x; t < box.nodes; t += kTileThreads) sc[0][t] = sc[1][t] = sc[2][t] = sc[3][t] = 0;
+    __syncthreads();
+    const float sm = pow2_scale30(sum_m), sp = pow2_scale30(sum_p);
+    if (valid) {
+        const TileRef tr = tile_ref(box, s, s_tile);
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+#pragma unroll
+            for (int b = 0; b < 3; ++b)
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+                    const int t = tr.t0 + (a * tr.d1 + b) * tr.d2 + c;
+                    float w = s.w[0][a] * s.w[1][b] * s.w[2][c];
+                    V3f dpos = mk((a - s.fx[0]) * P.h, (b - s.fx[1]) * P.h, (c - s.fx[2]) * P.h);
+                    V3f mom = (v * m + mul(A, dpos)) * (w * sp);
+                    atomicAdd(reinterpret_cast<unsigned *>(&sc[0][t]), fx_round(w * m * sm));
+                    atomicAdd(reinterpret_cast<unsigned *>(&sc[1][t]), fx_round(mom.x));
+                    atomicAdd(reinterpret_cast<unsigned *>(&sc[2][t]), fx_round(mom.y));
+                    atomicAdd(reinterpret_cast<unsigned *>(&sc[3][t]), fx_round(mom.z));
+                }
+    }
+    __syncthreads();
+    flush_tile<kTileThreads>(P, box, sc, 4, 1.0f / sm, 1.0f / sp, grid);
 }
 
 // Node velocity with the wall rule; w = bitmask of the components the walls zeroed.
@@ -208,29 +394,49 @@ __global__ void k_grid(AdjParams P, const float4 *__restrict__ grid, float4 *gv,
 }
 
 // Gather of one particle: velocity, affine matrix (4/h^2 sum w v dpos^T).
-__device__ __forceinline__ void gather(const AdjParams &P, const Stencil &s, const float4 *gv, V3f &vel, M3f &aff) {
+// The 27 nodes' loads are independent: unrolled, they are issued together.
+template <bool TILE>
+__device__ __forceinline__ void gather_nodes(const AdjParams &P, const Stencil &s, const float4 *gv, const TileRef &tr,
+                                             V3f &vel, M3f &aff) {
     vel = mk(0, 0, 0);
     aff = m3_zero();
+#pragma unroll
     for (int a = 0; a < 3; ++a)
+#pragma unroll
         for (int b = 0; b < 3; ++b)
+#pragma unroll
             for (int c = 0; c < 3; ++c) {
-                int id = node_at(P, s, a, b, c);
-                if (id < 0) continue;
+                float4 g;
+                if (!node_value<TILE>(P, s, gv, tr, a, b, c, g)) continue;
                 float w = s.w[0][a] * s.w[1][b] * s.w[2][c];
-                float4 g = gv[id];
                 V3f nv = mk(g.x, g.y, g.z);
                 V3f dpos = mk((a - s.fx[0]) * P.h, (b - s.fx[1]) * P.h, (c - s.fx[2]) * P.h);
                 vel = vel + nv * w;
                 aff = add(aff, scale(outer(nv, dpos), w * P.inv_d));
             }
 }
+__device__ __forceinline__ void gather(const AdjParams &P, const Stencil &s, const float4 *gv, const TileRef &tr,
+                                       V3f &vel, M3f &aff) {
+    if (tr.tile) gather_nodes<true>(P, s, gv, tr, vel, aff);
+    else gather_nodes<false>(P, s, gv, tr, vel, aff);
+}
 
-__global__ void k_g2p(AdjParams P, Consts K, const float *__restrict__ S, float *__restrict__ Sn,
-                      const float4 *__restrict__ gv) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= P.n) return;
+__global__ void __launch_bounds__(kTileThreads) k_g2p(AdjParams P, Consts K, const float *__restrict__ S,
+                                                      float *__restrict__ Sn, const float4 *__restrict__ gv) {
+    __shared__ float4 s_tile[kAdjTile];
+    __shared__ int s_red[kTileThreads / 32][6];
+    __shared__ float s_redf[kTileThreads / 32][4];
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool valid = i < P.n;
     const size_t st = P.stride;
-    V3f x = load_v(S, st, 0, i);
+    V3f x = load_v(S, st, 0, valid ? i : 0);
+    Stencil s;
+    stencil(x, P.inv_h, s);
+    float z0 = 0.f, z1 = 0.f, z2 = 0.f, z3 = 0.f;
+    TileBox box;
+    tile_box<kTileThreads>(P, valid, s.b, z0, z1, z2, z3, s_red, s_redf, box);
+    if (box.ok) fill_tile<kTileThreads>(P, box, gv, s_tile);
+    if (!valid) return;
     M3f F = load_m(S, st, 15, i);
     if (K.fixed[i]) {
         store_v(Sn, st, 0, i, x);
@@ -239,11 +445,9 @@ __global__ void k_g2p(AdjParams P, Consts K, const float *__restrict__ S, float 
         store_m(Sn, st, 15, i, F);
         return;
     }
-    Stencil s;
-    stencil(x, P.inv_h, s);
     V3f vel;
     M3f aff;
-    gather(P, s, gv, vel, aff);
+    gather(P, s, gv, tile_ref(box, s, s_tile), vel, aff);
     vel = vel * expf(-K.damping[i] * P.dt);
     V3f pos = x + vel * P.dt;
     M3f Fn = mul(add(m3_identity(), scale(aff, P.dt)), F);
@@ -270,60 +474,28 @@ __global__ void k_g2p(AdjParams P, Consts K, const float *__restrict__ S, float 
 // G2P adjoint.  In: the substep's input state S, node velocities gv, the
 // adjoint Ab of the substep's output state.  Out: partial adjoints of x and F
 // (rows 0-2 and 15-23 of Q) and the node-velocity adjoint gvb (atomics).
-__global__ void k_g2p_back(AdjParams P, Consts K, const float *__restrict__ S, const float4 *__restrict__ gv,
-                           const float *__restrict__ Ab, float *__restrict__ Q, float4 *gvb) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= P.n) return;
-    const size_t st = P.stride;
-    V3f x = load_v(S, st, 0, i);
-    M3f F = load_m(S, st, 15, i);
-    V3f xb_o = load_v(Ab, st, 0, i), vb_o = load_v(Ab, st, 3, i);
-    M3f Cb_o = load_m(Ab, st, 6, i), Fb_o = load_m(Ab, st, 15, i);
-    if (K.fixed[i]) {  // x and F pass through; v and C are reset
-        store_v(Q, st, 0, i, xb_o);
-        store_m(Q, st, 15, i, Fb_o);
-        return;
-    }
-    Stencil s;
-    stencil(x, P.inv_h, s);
-    V3f vel;
-    M3f aff;
-    gather(P, s, gv, vel, aff);
-    const float ed = expf(-K.damping[i] * P.dt);
-    V3f veld = vel * ed;
-    V3f pos = x + veld * P.dt;
-    const float r = K.radius[i];
-    V3f xb = xb_o, velb = vb_o;
-    for (int a = 0; a < 3; ++a) {
-        float lower = P.bmin[a] + r, upper = P.bmax[a] - r;
-        float pa = comp(pos, a), va = comp(veld, a);
-        if (pa < lower) {
-            set_comp(xb, a, 0.0f);
-            if (!(va > 0.0f)) set_comp(velb, a, 0.0f);
-        } else if (pa > upper) {
-            set_comp(xb, a, 0.0f);
-            if (!(va < 0.0f)) set_comp(velb, a, 0.0f);
-        }
-    }
-    velb = (velb + xb * P.dt) * ed;                       // pos = x + dt v_damped
-    M3f Cb = add(Cb_o, scale(mul_bt(Fb_o, F), P.dt));     // Fn = (I + dt C) F
-    M3f Fb = mul(transpose(add(m3_identity(), scale(aff, P.dt))), Fb_o);
-    V3f xbar = xb;
+// The position adjoint's node sum of the G2P adjoint (unrolled: the 27 node
+// loads are independent).
+template <bool TILE>
+__device__ __forceinline__ void xbar_nodes(const AdjParams &P, const Stencil &s, const float4 *gv, const TileRef &tr,
+                                           V3f velb, const M3f &Cb, V3f &xbar) {
     const M3f CbT = transpose(Cb);
     V3f nv_c = mk(0, 0, 0);
     {
-        int idc = node_at(P, s, 1, 1, 1);
-        if (idc >= 0) nv_c = mk(gv[idc].x, gv[idc].y, gv[idc].z);
+        float4 g;
+        if (node_value<TILE>(P, s, gv, tr, 1, 1, 1, g)) nv_c = mk(g.x, g.y, g.z);
     }
+#pragma unroll
     for (int a = 0; a < 3; ++a)
+#pragma unroll
         for (int b = 0; b < 3; ++b)
+#pragma unroll
             for (int c = 0; c < 3; ++c) {
-                int id = node_at(P, s, a, b, c);
-                if (id < 0) continue;
+                float4 g;
+                if (!node_value<TILE>(P, s, gv, tr, a, b, c, g)) continue;
                 float w = s.w[0][a] * s.w[1][b] * s.w[2][c];
                 V3f dw = mk(s.dw[0][a] * s.w[1][b] * s.w[2][c], s.w[0][a] * s.dw[1][b] * s.w[2][c],
                             s.w[0][a] * s.w[1][b] * s.dw[2][c]) * P.inv_h;
-                float4 g = gv[id];
                 V3f nv = mk(g.x, g.y, g.z);
                 V3f dnv = nv - nv_c;
                 V3f dpos = mk((a - s.fx[0]) * P.h, (b - s.fx[1]) * P.h, (c - s.fx[2]) * P.h);
@@ -331,11 +503,146 @@ __global__ void k_g2p_back(AdjParams P, Consts K, const float *__restrict__ S, c
                 // grad w (v_i . velb + v_i . C_b dpos_i) - w C_b^T v_i with v_i -> v_i - v_c (file header)
                 float gs = dot(dnv, velb) + P.inv_d * dot(dnv, Cd);
                 xbar = xbar + dw * gs - mul(CbT, dnv) * (P.inv_d * w);
-                V3f gb = velb * w + Cd * (P.inv_d * w);
-                red_add_v4(gvb + id, make_float4(gb.x, gb.y, gb.z, 0.0f));
             }
-    store_v(Q, st, 0, i, xbar);
-    store_m(Q, st, 15, i, Fb);
+}
+
+// The P2G adjoint's node sums: velocity and affine adjoints, position adjoint.
+template <bool TILE>
+__device__ __forceinline__ void p2g_back_nodes(const AdjParams &P, const Stencil &s, const float4 *gmb,
+                                               const TileRef &tr, float m, V3f v, const M3f &A, V3f &vbar,
+                                               M3f &Abar, V3f &xbar) {
+    const M3f AT = transpose(A);
+    float4 gc = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (!node_value<TILE>(P, s, gmb, tr, 1, 1, 1, gc)) gc = make_float4(0.f, 0.f, 0.f, 0.f);
+    const V3f pb_c = mk(gc.y, gc.z, gc.w);
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int b = 0; b < 3; ++b)
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                float4 g;
+                if (!node_value<TILE>(P, s, gmb, tr, a, b, c, g)) continue;
+                float w = s.w[0][a] * s.w[1][b] * s.w[2][c];
+                V3f dw = mk(s.dw[0][a] * s.w[1][b] * s.w[2][c], s.w[0][a] * s.dw[1][b] * s.w[2][c],
+                            s.w[0][a] * s.w[1][b] * s.dw[2][c]) * P.inv_h;
+                V3f pb = mk(g.y, g.z, g.w);
+                V3f dpb = pb - pb_c;
+                V3f dpos = mk((a - s.fx[0]) * P.h, (b - s.fx[1]) * P.h, (c - s.fx[2]) * P.h);
+                // grad w (m m_b + p_b . (m v + A dpos)) - w A^T p_b with m_b, p_b -> minus their centre values
+                vbar = vbar + pb * (w * m);
+                Abar = add(Abar, scale(outer(dpb, dpos), w));
+                xbar = xbar + dw * (m * (g.x - gc.x) + m * dot(v, dpb) + dot(dpb, mul(A, dpos))) - mul(AT, dpb) * w;
+            }
+}
+
+__global__ void __launch_bounds__(kTileThreads) k_g2p_back(AdjParams P, Consts K, const float *__restrict__ S,
+                                                           const float4 *__restrict__ gv, const float *__restrict__ Ab,
+                                                           float *__restrict__ Q, float4 *gvb) {
+    __shared__ float4 s_tile[kAdjTile];
+    __shared__ int s_red[kTileThreads / 32][6];
+    __shared__ float s_redf[kTileThreads / 32][4];
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool valid = i < P.n;
+    const int ic = valid ? i : 0;
+    const bool active = valid && !K.fixed[ic];
+    const size_t st = P.stride;
+    V3f x = load_v(S, st, 0, ic);
+    Stencil s;
+    stencil(x, P.inv_h, s);
+    float z0 = 0.f, z1 = 0.f, z2 = 0.f, z3 = 0.f;
+    TileBox box;
+    tile_box<kTileThreads>(P, valid, s.b, z0, z1, z2, z3, s_red, s_redf, box);
+    if (box.ok) fill_tile<kTileThreads>(P, box, gv, s_tile);
+    const TileRef tr = tile_ref(box, s, s_tile);
+    V3f velb = mk(0, 0, 0);
+    M3f Cb = m3_zero();
+    float bg = 0.0f;  // bound of the particle's velocity-adjoint contributions
+    if (valid) {
+        M3f F = load_m(S, st, 15, i);
+        V3f xb_o = load_v(Ab, st, 0, i), vb_o = load_v(Ab, st, 3, i);
+        M3f Cb_o = load_m(Ab, st, 6, i), Fb_o = load_m(Ab, st, 15, i);
+        if (!active) {  // x and F pass through; v and C are reset
+            store_v(Q, st, 0, i, xb_o);
+            store_m(Q, st, 15, i, Fb_o);
+        } else {
+            V3f vel;
+            M3f aff;
+            gather(P, s, gv, tr, vel, aff);
+            const float ed = expf(-K.damping[i] * P.dt);
+            V3f veld = vel * ed;
+            V3f pos = x + veld * P.dt;
+            const float r = K.radius[i];
+            V3f xb = xb_o;
+            velb = vb_o;
+            for (int a = 0; a < 3; ++a) {
+                float lower = P.bmin[a] + r, upper = P.bmax[a] - r;
+                float pa = comp(pos, a), va = comp(veld, a);
+                if (pa < lower) {
+                    set_comp(xb, a, 0.0f);
+                    if (!(va > 0.0f)) set_comp(velb, a, 0.0f);
+                } else if (pa > upper) {
+                    set_comp(xb, a, 0.0f);
+                    if (!(va < 0.0f)) set_comp(velb, a, 0.0f);
+                }
+            }
+            velb = (velb + xb * P.dt) * ed;                       // pos = x + dt v_damped
+            Cb = add(Cb_o, scale(mul_bt(Fb_o, F), P.dt));         // Fn = (I + dt C) F
+            M3f Fb = mul(transpose(add(m3_identity(), scale(aff, P.dt))), Fb_o);
+            V3f xbar = xb;
+            if (tr.tile) xbar_nodes<true>(P, s, gv, tr, velb, Cb, xbar);
+            else xbar_nodes<false>(P, s, gv, tr, velb, Cb, xbar);
+            store_v(Q, st, 0, i, xbar);
+            store_m(Q, st, 15, i, Fb);
+            // |gb_k| <= w (|velb_k| + 4/h^2 * 1.5 h sum_j |Cb_kj|), and the weights sum to one
+            const float q = P.inv_d * 1.5f * P.h;
+            bg = fmaxf(fmaxf(fabsf(velb.x) + q * (fabsf(Cb.c0.x) + fabsf(Cb.c1.x) + fabsf(Cb.c2.x)),
+                             fabsf(velb.y) + q * (fabsf(Cb.c0.y) + fabsf(Cb.c1.y) + fabsf(Cb.c2.y))),
+                       fabsf(velb.z) + q * (fabsf(Cb.c0.z) + fabsf(Cb.c1.z) + fabsf(Cb.c2.z)));
+            if (!(bg < 1e30f)) bg = 1e30f;
+        }
+    }
+    // the velocity-adjoint scatter; the reduction's barrier also ends every read of the gv tile
+    float sum_g = bg, sum_0 = 0.0f, max_g = bg, max_0 = 0.0f;
+    TileBox box2;
+    tile_box<kTileThreads>(P, active, s.b, sum_g, sum_0, max_g, max_0, s_red, s_redf, box2);
+    const bool tiled = box.ok && !(max_g > 0.125f * sum_g);
+    if (!tiled) {
+        if (!active) return;
+        for (int a = 0; a < 3; ++a)
+            for (int b = 0; b < 3; ++b)
+                for (int c = 0; c < 3; ++c) {
+                    int id = node_at(P, s, a, b, c);
+                    if (id < 0) continue;
+                    float w = s.w[0][a] * s.w[1][b] * s.w[2][c];
+                    V3f dpos = mk((a - s.fx[0]) * P.h, (b - s.fx[1]) * P.h, (c - s.fx[2]) * P.h);
+                    V3f gb = velb * w + mul(Cb, dpos) * (P.inv_d * w);
+                    red_add_v4(gvb + id, make_float4(gb.x, gb.y, gb.z, 0.0f));
+                }
+        return;
+    }
+    int (*sc)[kAdjTile] = reinterpret_cast<int (*)[kAdjTile]>(s_tile);
+    for (int t = threadIdx.x; t < box.nodes; t += kTileThreads) sc[0][t] = sc[1][t] = sc[2][t] = 0;
+    __syncthreads();
+    const float sg = pow2_scale30(sum_g);
+    if (active) {
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+#pragma unroll
+            for (int b = 0; b < 3; ++b)
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+                    const int t = tr.t0 + (a * tr.d1 + b) * tr.d2 + c;
+                    float w = s.w[0][a] * s.w[1][b] * s.w[2][c];
+                    V3f dpos = mk((a - s.fx[0]) * P.h, (b - s.fx[1]) * P.h, (c - s.fx[2]) * P.h);
+                    V3f gb = (velb + mul(Cb, dpos) * P.inv_d) * (w * sg);
+                    atomicAdd(reinterpret_cast<unsigned *>(&sc[0][t]), fx_round(gb.x));
+                    atomicAdd(reinterpret_cast<unsigned *>(&sc[1][t]), fx_round(gb.y));
+                    atomicAdd(reinterpret_cast<unsigned *>(&sc[2][t]), fx_round(gb.z));
+                }
+    }
+    __syncthreads();
+    flush_tile<kTileThreads>(P, box, sc, 3, 1.0f / sg, 1.0f / sg, gvb);
 }
 
 // Grid adjoint: node velocity v = p / m + g dt (walls zero some components).
@@ -362,13 +669,26 @@ __global__ void k_grid_back(AdjParams P, const float4 *__restrict__ grid, const 
 // P2G adjoint.  In: the substep's input state S, node (m_bar, p_bar), partial
 // adjoints Q from the G2P adjoint.  Out: the adjoint of the substep's input
 // state (Ain) and dL/dE accumulated into Eb.
-__global__ void k_p2g_back(AdjParams P, Consts K, const float *__restrict__ S, const float *__restrict__ E,
-                           const float4 *__restrict__ gmb, const float *__restrict__ Q, float *__restrict__ Ain,
-                           float *__restrict__ Eb, const float *__restrict__ Rin) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= P.n) return;
+__global__ void __launch_bounds__(kTileThreads) k_p2g_back(AdjParams P, Consts K, const float *__restrict__ S,
+                                                           const float *__restrict__ E, const float4 *__restrict__ gmb,
+                                                           const float *__restrict__ Q, float *__restrict__ Ain,
+                                                           float *__restrict__ Eb, const float *__restrict__ Rin) {
+    __shared__ float4 s_tile[kAdjTile];
+    __shared__ int s_red[kTileThreads / 32][6];
+    __shared__ float s_redf[kTileThreads / 32][4];
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool valid = i < P.n;
     const size_t st = P.stride;
-    V3f x = load_v(S, st, 0, i), v = load_v(S, st, 3, i);
+    const V3f x = load_v(S, st, 0, valid ? i : 0);
+    Stencil s;
+    stencil(x, P.inv_h, s);
+    float z0 = 0.f, z1 = 0.f, z2 = 0.f, z3 = 0.f;
+    TileBox box;
+    tile_box<kTileThreads>(P, valid, s.b, z0, z1, z2, z3, s_red, s_redf, box);
+    if (box.ok) fill_tile<kTileThreads>(P, box, gmb, s_tile);
+    if (!valid) return;
+    const TileRef tr = tile_ref(box, s, s_tile);
+    V3f v = load_v(S, st, 3, i);
     M3f C = load_m(S, st, 6, i), F = load_m(S, st, 15, i);
     const float m = K.mass[i];
     float lambda, mu;
@@ -384,36 +704,12 @@ __global__ void k_p2g_back(AdjParams P, Consts K, const float *__restrict__ S, c
     tau.c2.z += iso;
     const float sc = -P.dt * K.vol[i] * P.inv_d;
     M3f A = add(scale(tau, sc), scale(C, m));
-    const M3f AT = transpose(A);
-    Stencil s;
-    stencil(x, P.inv_h, s);
     V3f xbar = load_v(Q, st, 0, i);
     M3f Fbar = load_m(Q, st, 15, i);
     V3f vbar = mk(0, 0, 0);
     M3f Abar = m3_zero();
-    float4 gc = make_float4(0.f, 0.f, 0.f, 0.f);
-    {
-        int idc = node_at(P, s, 1, 1, 1);
-        if (idc >= 0) gc = gmb[idc];
-    }
-    const V3f pb_c = mk(gc.y, gc.z, gc.w);
-    for (int a = 0; a < 3; ++a)
-        for (int b = 0; b < 3; ++b)
-            for (int c = 0; c < 3; ++c) {
-                int id = node_at(P, s, a, b, c);
-                if (id < 0) continue;
-                float w = s.w[0][a] * s.w[1][b] * s.w[2][c];
-                V3f dw = mk(s.dw[0][a] * s.w[1][b] * s.w[2][c], s.w[0][a] * s.dw[1][b] * s.w[2][c],
-                            s.w[0][a] * s.w[1][b] * s.dw[2][c]) * P.inv_h;
-                float4 g = gmb[id];
-                V3f pb = mk(g.y, g.z, g.w);
-                V3f dpb = pb - pb_c;
-                V3f dpos = mk((a - s.fx[0]) * P.h, (b - s.fx[1]) * P.h, (c - s.fx[2]) * P.h);
-                // grad w (m m_b + p_b . (m v + A dpos)) - w A^T p_b with m_b, p_b -> minus their centre values
-                vbar = vbar + pb * (w * m);
-                Abar = add(Abar, scale(outer(dpb, dpos), w));
-                xbar = xbar + dw * (m * (g.x - gc.x) + m * dot(v, dpb) + dot(dpb, mul(A, dpos))) - mul(AT, dpb) * w;
-            }
+    if (tr.tile) p2g_back_nodes<true>(P, s, gmb, tr, m, v, A, vbar, Abar, xbar);
+    else p2g_back_nodes<false>(P, s, gmb, tr, m, v, A, vbar, Abar, xbar);
     M3f Cbar = scale(Abar, m);
     M3f taub = scale(Abar, sc);
     float trt = trace(taub);
@@ -531,7 +827,7 @@ struct TmpmAdjoint {
                 float4 *g = seg_grid.ptr + static_cast<size_t>(j) * nodes, *v = seg_gv.ptr + static_cast<size_t>(j) * nodes;
                 p2g_grid(seg.ptr + j * state_floats(), g, v, seg_R.ptr + static_cast<size_t>(j) * 9 * n);
                 if (s + 1 < s1)
-                    k_g2p<<<blocks_n(), kParticleThreads, 0, stream>>>(P, consts(), seg.ptr + j * state_floats(),
+                    k_g2p<<<blocks_n(), kTileThreads, 0, stream>>>(P, consts(), seg.ptr + j * state_floats(),
                                                                        seg.ptr + (j + 1) * state_floats(), v);
             }
             for (int s = static_cast<int>(s1) - 1; s >= static_cast<int>(s0); --s) {
@@ -539,10 +835,10 @@ struct TmpmAdjoint {
                 const float *S = seg.ptr + j * state_floats();
                 const float4 *g = seg_grid.ptr + static_cast<size_t>(j) * nodes, *v = seg_gv.ptr + static_cast<size_t>(j) * nodes;
                 cudaMemsetAsync(gvb.ptr, 0, sizeof(float4) * nodes, stream);
-                k_g2p_back<<<blocks_n(), kParticleThreads, 0, stream>>>(P, consts(), S, v, adj[a].ptr, part.ptr,
+                k_g2p_back<<<blocks_n(), kTileThreads, 0, stream>>>(P, consts(), S, v, adj[a].ptr, part.ptr,
                                                                         gvb.ptr);
                 k_grid_back<<<blocks_nodes(), 256, 0, stream>>>(P, g, v, gvb.ptr, nodes);
-                k_p2g_back<<<blocks_n(), kParticleThreads, 0, stream>>>(P, consts(), S, E.ptr, gvb.ptr, part.ptr,
+                k_p2g_back<<<blocks_n(), kTileThreads, 0, stream>>>(P, consts(), S, E.ptr, gvb.ptr, part.ptr,
                                                                         adj[a ^ 1].ptr, Ebar.ptr,
                                                                         seg_R.ptr + static_cast<size_t>(j) * 9 * n);
                 a ^= 1;
@@ -559,18 +855,18 @@ struct TmpmAdjoint {
     }
     Consts consts() const { return Consts{mass.ptr, vol.ptr, radius.ptr, damping.ptr, nu.ptr, fixed.ptr}; }
     size_t state_floats() const { return kRows * n; }
-    int blocks_n() const { return static_cast<int>((n + kParticleThreads - 1) / kParticleThreads); }
+    int blocks_n() const { return static_cast<int>((n + kTileThreads - 1) / kTileThreads); }
     int blocks_nodes() const { return (nodes + 255) / 256; }
 
     // P2G + grid of state S into g / v (and the polar factors into R when given).
     void p2g_grid(const float *S, float4 *g, float4 *v, float *R) {
         cudaMemsetAsync(g, 0, sizeof(float4) * nodes, stream);
-        k_p2g<<<blocks_n(), kParticleThreads, 0, stream>>>(P, consts(), S, E.ptr, g, err.ptr, R);
+        k_p2g<<<blocks_n(), kTileThreads, 0, stream>>>(P, consts(), S, E.ptr, g, err.ptr, R);
         k_grid<<<blocks_nodes(), 256, 0, stream>>>(P, g, v, nodes);
     }
     void substep(const float *S, float *Sn) {
         p2g_grid(S, grid.ptr, gv.ptr, nullptr);
-        k_g2p<<<blocks_n(), kParticleThreads, 0, stream>>>(P, consts(), S, Sn, gv.ptr);
+        k_g2p<<<blocks_n(), kTileThreads, 0, stream>>>(P, consts(), S, Sn, gv.ptr);
     }
 
     TmpmStatus check_err() {

@@ -823,6 +823,7 @@ __global__ void __launch_bounds__(THREADS, MINB)
             if ((m | px | py | pz) == 0) continue;  // also every padding entry
             int tx, ty, tz;
             split_n(t, tx, ty, tz);
+            if (ty >= bx.dim[1] || tz >= bx.dim[2]) continue;  // padding (zero by construction; never flushed)
             int cx = bx.lo[0] + tx, cy = bx.lo[1] + ty, cz = bx.lo[2] + tz;
             int id = s_blk2[tile_block_index<BS>(bx, cx, cy, cz)];
             if (id < 0) continue;
