@@ -755,27 +755,37 @@ struct TmpmAdjoint {
     int nodes = 0;
     DevBuf<float> mass, vol, radius, damping, nu, E, Ebar;
     DevBuf<uint8_t> fixed;
-    DevBuf<float> ckpt, seg, adj[2], part;
+    DevBuf<float> ckpt, adj[2], part;
     DevBuf<float4> grid, gv, gvb;
-    // per substep of the segment being replayed: the grid after P2G (mass and
+    // Two buffer sets for replayed segments (segment sg uses set sg & 1): per
+    // substep of the segment, its state, the grid after P2G (mass and
     // momentum), the node velocities and the particles' polar factors, so the
-    // adjoint sweep reuses them instead of recomputing P2G and the grid update
-    DevBuf<float4> seg_grid, seg_gv;
-    DevBuf<float> seg_R;
+    // adjoint sweep reuses them instead of recomputing P2G and the grid
+    // update.  The forward ping-pongs between the first two states of set 0.
+    DevBuf<float> seg[2];
+    DevBuf<float4> seg_grid[2], seg_gv[2];
+    DevBuf<float> seg_R[2];
     DevBuf<uint32_t> err;
     bool have_forward = false;
     std::string last_error;
     // The forward and adjoint sweeps (fixed launches over fixed buffers) are
     // captured as CUDA graphs on first use and replayed afterwards.
     cudaGraphExec_t fwd_exec = nullptr, bwd_exec = nullptr;
+    // The adjoint sweep replays segment sg - 1 on `side` while `stream` runs the
+    // adjoint of segment sg: at the sizes this rollout is built for, each
+    // kernel fills less than one wave of the GPU, so the two overlap.
+    cudaStream_t side = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_replayed = nullptr, ev_swept = nullptr;
 
     ~TmpmAdjoint() {
-        if (stream) {
-            cudaStreamSynchronize(stream);
-            cudaStreamDestroy(stream);
-        }
+        if (stream) cudaStreamSynchronize(stream);
+        if (side) cudaStreamSynchronize(side);
         if (fwd_exec) cudaGraphExecDestroy(fwd_exec);
         if (bwd_exec) cudaGraphExecDestroy(bwd_exec);
+        for (cudaEvent_t ev : {ev_fork, ev_replayed, ev_swept})
+            if (ev) cudaEventDestroy(ev);
+        if (side) cudaStreamDestroy(side);
+        if (stream) cudaStreamDestroy(stream);
     }
 
     // Capture `launch` (stream work only) into *exec once, then launch it.
@@ -797,10 +807,10 @@ struct TmpmAdjoint {
         return cudaGraphLaunch(*exec, stream);
     }
 
-    // The forward sweep: `substeps` substeps from seg[0] ping-ponging with
-    // seg[1], a checkpoint every `every`.
+    // The forward sweep: `substeps` substeps from seg[0] (its first state)
+    // ping-ponging with its second state, a checkpoint every `every`.
     void forward_sweep() {
-        float *cur = seg.ptr, *nxt = seg.ptr + state_floats();
+        float *cur = seg[0].ptr, *nxt = seg[0].ptr + state_floats();
         for (uint32_t s = 0; s < substeps; ++s) {
             if (s % every == 0)
                 cudaMemcpyAsync(ckpt.ptr + (s / every) * state_floats(), cur, sizeof(float) * state_floats(),
@@ -810,40 +820,67 @@ struct TmpmAdjoint {
         }
     }
 
+    // Replay segment sg from its checkpoint into buffer set sg & 1 on stream st:
+    // per substep j its state, grid, node velocities and polar factors.
+    void replay_segment(int sg, cudaStream_t st) {
+        const int set = sg & 1;
+        const uint32_t s0 = sg * every, s1 = std::min(substeps, s0 + every);
+        float *S = seg[set].ptr;
+        cudaMemcpyAsync(S, ckpt.ptr + sg * state_floats(), sizeof(float) * state_floats(), cudaMemcpyDeviceToDevice,
+                        st);
+        for (uint32_t s = s0; s < s1; ++s) {
+            const uint32_t j = s - s0;
+            float4 *g = seg_grid[set].ptr + static_cast<size_t>(j) * nodes;
+            float4 *v = seg_gv[set].ptr + static_cast<size_t>(j) * nodes;
+            p2g_grid(S + j * state_floats(), g, v, seg_R[set].ptr + static_cast<size_t>(j) * 9 * n, st);
+            if (s + 1 < s1)
+                k_g2p<<<blocks_n(), kTileThreads, 0, st>>>(P, consts(), S + j * state_floats(),
+                                                           S + (j + 1) * state_floats(), v);
+        }
+    }
+
+    // The adjoint of segment sg (replayed into set sg & 1), substep by substep
+    // from its last; `a` is the adj buffer holding the adjoint of its final state.
+    void sweep_segment(int sg, int &a) {
+        const int set = sg & 1;
+        const uint32_t s0 = sg * every, s1 = std::min(substeps, s0 + every);
+        for (int s = static_cast<int>(s1) - 1; s >= static_cast<int>(s0); --s) {
+            const uint32_t j = s - s0;
+            const float *S = seg[set].ptr + j * state_floats();
+            const float4 *g = seg_grid[set].ptr + static_cast<size_t>(j) * nodes;
+            const float4 *v = seg_gv[set].ptr + static_cast<size_t>(j) * nodes;
+            cudaMemsetAsync(gvb.ptr, 0, sizeof(float4) * nodes, stream);
+            k_g2p_back<<<blocks_n(), kTileThreads, 0, stream>>>(P, consts(), S, v, adj[a].ptr, part.ptr, gvb.ptr);
+            k_grid_back<<<blocks_nodes(), 256, 0, stream>>>(P, g, v, gvb.ptr, nodes);
+            k_p2g_back<<<blocks_n(), kTileThreads, 0, stream>>>(P, consts(), S, E.ptr, gvb.ptr, part.ptr, adj[a ^ 1].ptr,
+                                                                Ebar.ptr, seg_R[set].ptr + static_cast<size_t>(j) * 9 * n);
+            a ^= 1;
+        }
+    }
+
     // The adjoint sweep from adj[0] (the loss gradient of the final state),
     // segment by segment from the last checkpoint back; the initial-state
-    // adjoint ends in adj[substeps & 1].
+    // adjoint ends in adj[substeps & 1].  Segment sg - 1 is replayed on `side`
+    // while `stream` sweeps segment sg; the replay into a set waits for the
+    // sweep that last read it (segment sg + 1), and each sweep for its replay.
     void backward_sweep() {
         int a = 0;
-        const uint32_t segments = (substeps + every - 1) / every;
-        for (int sg = static_cast<int>(segments) - 1; sg >= 0; --sg) {
-            const uint32_t s0 = sg * every, s1 = std::min(substeps, s0 + every);
-            // replay the segment: seg[j] = state at substep s0 + j, with the
-            // grid, node velocities and polar factors of each substep kept
-            cudaMemcpyAsync(seg.ptr, ckpt.ptr + sg * state_floats(), sizeof(float) * state_floats(),
-                            cudaMemcpyDeviceToDevice, stream);
-            for (uint32_t s = s0; s < s1; ++s) {
-                const uint32_t j = s - s0;
-                float4 *g = seg_grid.ptr + static_cast<size_t>(j) * nodes, *v = seg_gv.ptr + static_cast<size_t>(j) * nodes;
-                p2g_grid(seg.ptr + j * state_floats(), g, v, seg_R.ptr + static_cast<size_t>(j) * 9 * n);
-                if (s + 1 < s1)
-                    k_g2p<<<blocks_n(), kTileThreads, 0, stream>>>(P, consts(), seg.ptr + j * state_floats(),
-                                                                       seg.ptr + (j + 1) * state_floats(), v);
+        const int segments = static_cast<int>((substeps + every - 1) / every);
+        cudaEventRecord(ev_fork, stream);
+        cudaStreamWaitEvent(side, ev_fork, 0);
+        replay_segment(segments - 1, side);
+        cudaEventRecord(ev_replayed, side);
+        for (int sg = segments - 1; sg >= 0; --sg) {
+            cudaStreamWaitEvent(stream, ev_replayed, 0);
+            if (sg >= 1) {
+                if (sg + 1 < segments) cudaStreamWaitEvent(side, ev_swept, 0);
+                replay_segment(sg - 1, side);
+                cudaEventRecord(ev_replayed, side);
             }
-            for (int s = static_cast<int>(s1) - 1; s >= static_cast<int>(s0); --s) {
-                const uint32_t j = s - s0;
-                const float *S = seg.ptr + j * state_floats();
-                const float4 *g = seg_grid.ptr + static_cast<size_t>(j) * nodes, *v = seg_gv.ptr + static_cast<size_t>(j) * nodes;
-                cudaMemsetAsync(gvb.ptr, 0, sizeof(float4) * nodes, stream);
-                k_g2p_back<<<blocks_n(), kTileThreads, 0, stream>>>(P, consts(), S, v, adj[a].ptr, part.ptr,
-                                                                        gvb.ptr);
-                k_grid_back<<<blocks_nodes(), 256, 0, stream>>>(P, g, v, gvb.ptr, nodes);
-                k_p2g_back<<<blocks_n(), kTileThreads, 0, stream>>>(P, consts(), S, E.ptr, gvb.ptr, part.ptr,
-                                                                        adj[a ^ 1].ptr, Ebar.ptr,
-                                                                        seg_R.ptr + static_cast<size_t>(j) * 9 * n);
-                a ^= 1;
-            }
+            sweep_segment(sg, a);
+            cudaEventRecord(ev_swept, stream);
         }
+        // every replay on `side` ends before a sweep that `stream` waits for
     }
     TmpmStatus fail(TmpmStatus st, const std::string &msg) {
         last_error = msg;
@@ -859,13 +896,13 @@ struct TmpmAdjoint {
     int blocks_nodes() const { return (nodes + 255) / 256; }
 
     // P2G + grid of state S into g / v (and the polar factors into R when given).
-    void p2g_grid(const float *S, float4 *g, float4 *v, float *R) {
-        cudaMemsetAsync(g, 0, sizeof(float4) * nodes, stream);
-        k_p2g<<<blocks_n(), kTileThreads, 0, stream>>>(P, consts(), S, E.ptr, g, err.ptr, R);
-        k_grid<<<blocks_nodes(), 256, 0, stream>>>(P, g, v, nodes);
+    void p2g_grid(const float *S, float4 *g, float4 *v, float *R, cudaStream_t st) {
+        cudaMemsetAsync(g, 0, sizeof(float4) * nodes, st);
+        k_p2g<<<blocks_n(), kTileThreads, 0, st>>>(P, consts(), S, E.ptr, g, err.ptr, R);
+        k_grid<<<blocks_nodes(), 256, 0, st>>>(P, g, v, nodes);
     }
     void substep(const float *S, float *Sn) {
-        p2g_grid(S, grid.ptr, gv.ptr, nullptr);
+        p2g_grid(S, grid.ptr, gv.ptr, nullptr, stream);
         k_g2p<<<blocks_n(), kTileThreads, 0, stream>>>(P, consts(), S, Sn, gv.ptr);
     }
 
@@ -906,13 +943,13 @@ struct TmpmAdjoint {
         }
         cudaError_t e;
         if ((e = cudaMemcpyAsync(E.ptr, Ef.data(), sizeof(float) * n, cudaMemcpyHostToDevice, stream)) ||
-            (e = cudaMemcpyAsync(seg.ptr, S0.data(), sizeof(float) * state_floats(), cudaMemcpyHostToDevice, stream)) ||
+            (e = cudaMemcpyAsync(seg[0].ptr, S0.data(), sizeof(float) * state_floats(), cudaMemcpyHostToDevice, stream)) ||
             (e = cudaMemsetAsync(err.ptr, 0, sizeof(uint32_t), stream)))
             return cuda_fail(e, "adjoint upload");
-        // seg holds two ping-pong states during the forward; the final state is
-        // in the first of them after an even number of substeps
+        // seg[0] holds two ping-pong states during the forward; the final state
+        // is in the first of them after an even number of substeps
         if ((e = replay(&fwd_exec, [&]() { forward_sweep(); }))) return cuda_fail(e, "adjoint forward");
-        const float *cur = (substeps % 2 == 0) ? seg.ptr : seg.ptr + state_floats();
+        const float *cur = (substeps % 2 == 0) ? seg[0].ptr : seg[0].ptr + state_floats();
         std::vector<float> out(6 * n);
         if ((e = cudaMemcpyAsync(out.data(), cur, sizeof(float) * 6 * n, cudaMemcpyDeviceToHost, stream)) ||
             (e = cudaStreamSynchronize(stream)))
@@ -1064,16 +1101,26 @@ TmpmStatus tmpm_adjoint_create(const TmpmParams *params, const TmpmParticleArray
     const uint32_t segments = (substeps + a->every - 1) / a->every;
     const size_t sf = kRows * n;
     if ((e = cudaSetDevice(device)) || (e = cudaStreamCreateWithFlags(&a->stream, cudaStreamNonBlocking)) ||
+        (e = cudaStreamCreateWithFlags(&a->side, cudaStreamNonBlocking)) ||
+        (e = cudaEventCreateWithFlags(&a->ev_fork, cudaEventDisableTiming)) ||
+        (e = cudaEventCreateWithFlags(&a->ev_replayed, cudaEventDisableTiming)) ||
+        (e = cudaEventCreateWithFlags(&a->ev_swept, cudaEventDisableTiming)) ||
         (e = a->mass.alloc(n)) || (e = a->vol.alloc(n)) || (e = a->radius.alloc(n)) || (e = a->damping.alloc(n)) ||
         (e = a->nu.alloc(n)) || (e = a->E.alloc(n)) || (e = a->Ebar.alloc(n)) || (e = a->fixed.alloc(n)) ||
-        (e = a->ckpt.alloc(segments * sf)) || (e = a->seg.alloc(std::max<size_t>(a->every, 2) * sf)) ||
-        (e = a->adj[0].alloc(sf)) || (e = a->adj[1].alloc(sf)) || (e = a->part.alloc(sf)) ||
-        (e = a->grid.alloc(nodes)) || (e = a->gv.alloc(nodes)) || (e = a->gvb.alloc(nodes)) || (e = a->err.alloc(1)) ||
-        (e = a->seg_grid.alloc(static_cast<size_t>(a->every) * nodes)) ||
-        (e = a->seg_gv.alloc(static_cast<size_t>(a->every) * nodes)) || (e = a->seg_R.alloc(a->every * 9 * n))) {
+        (e = a->ckpt.alloc(segments * sf)) || (e = a->adj[0].alloc(sf)) || (e = a->adj[1].alloc(sf)) ||
+        (e = a->part.alloc(sf)) || (e = a->grid.alloc(nodes)) || (e = a->gv.alloc(nodes)) ||
+        (e = a->gvb.alloc(nodes)) || (e = a->err.alloc(1))) {
         g_last_error = std::string("adjoint setup: ") + cudaGetErrorString(e);
         return TMPM_ERR_DEVICE;
     }
+    for (int set = 0; set < 2; ++set)
+        if ((e = a->seg[set].alloc(std::max<size_t>(a->every, 2) * sf)) ||
+            (e = a->seg_grid[set].alloc(static_cast<size_t>(a->every) * nodes)) ||
+            (e = a->seg_gv[set].alloc(static_cast<size_t>(a->every) * nodes)) ||
+            (e = a->seg_R[set].alloc(a->every * 9 * n))) {
+            g_last_error = std::string("adjoint setup: ") + cudaGetErrorString(e);
+            return TMPM_ERR_DEVICE;
+        }
     cudaMemcpyAsync(a->mass.ptr, m.data(), sizeof(float) * n, cudaMemcpyHostToDevice, a->stream);
     cudaMemcpyAsync(a->vol.ptr, v.data(), sizeof(float) * n, cudaMemcpyHostToDevice, a->stream);
     cudaMemcpyAsync(a->radius.ptr, r.data(), sizeof(float) * n, cudaMemcpyHostToDevice, a->stream);

@@ -26,7 +26,11 @@ namespace tmpm {
 
 namespace {
 
-constexpr int kTileMaxDim = 16;     // box edge in cells
+// Box edge in cells: only bounds the arithmetic (a padded entry count far
+// inside int range); the entry and block counts decide whether a box fits.
+// An elongated box (a chunk that wraps from one row of blocks to the next
+// in storage order) fits when its volume does.
+constexpr int kTileMaxDim = 64;
 // Box nodes a CTA of `threads` particles stages: 8 per particle (2048 nodes,
 // one 32 KB shared buffer, for 256), used as the gather tile and then as the
 // scatter tile.
