@@ -543,7 +543,8 @@ def run_tessera(args, world, rank, local):
     # 32 B per active node (P2G write 16 + G2P read 16); the grid update's 32 B/node is the other kernel
     alg_bytes = 248.0 * n + 32.0 * grid_nodes
     achieved = alg_bytes / (g2p2g_ms / 1000.0) / 1e9
-    roofline = {"kernel": "k_transfer<G2P2G> (fused G2P of step n + P2G of step n+1)", "bound": "hbm",
+    roofline = {"kernel": "fused G2P of step n + P2G of step n+1: k_transfer_fast with k_transfer_deferred beside and "
+                          "after it, timed together", "bound": "hbm",
                 "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind,
                 "traffic": None, "alg_bytes_per_launch": alg_bytes, "launch_ms": g2p2g_ms,

@@ -168,6 +168,9 @@ struct SimParams {
     SceneParams s0;             // the scene of a single-scene session (kernel parameter, constant bank)
     const SceneParams *scenes;  // multi-scene batch: device scene table, indexed by namespace >> kSceneShift
     uint32_t *scene_status;     // multi-scene batch: per-scene resident failure flags
+    // One scene: the fused transfer's deferred-chunk lists (layout at
+    // DeferLists); null: every transfer takes the general kernel.
+    uint32_t *defer;
     int multi;                  // 1 = multi-scene batch (per-particle scene lookup and step gating)
     int step_index;             // substep completed by this launch's G2P (-1 for the opening P2G)
     int num_obstacles;
@@ -178,11 +181,20 @@ struct SimParams {
     int cpic;             // CPIC on: grid namespace = colour << 8 | side mask of the CPIC groups (< 8)
     int shape;            // transfer launch shape (index into kLaunchShapes)
     int block_shift;      // log2 of the grid block edge: kBlockShift (4^3) or kBigBlockShift (8^3)
+    int defer_cap;        // entries per deferred-chunk list (transfer chunks of the smallest CTA)
+    int pad_;
 };
 // The session's graph cache keys segments by the bytes of a SimParams: neither
 // it nor SceneParams may hold padding, whose contents would be indeterminate.
-static_assert(sizeof(SimParams) == sizeof(SceneParams) + 2 * sizeof(void *) + 10 * sizeof(int),
+static_assert(sizeof(SimParams) == sizeof(SceneParams) + 3 * sizeof(void *) + 12 * sizeof(int),
               "SimParams must have no padding bytes");
+
+// Deferred-chunk lists of the fast fused transfer, in one device buffer of
+// kDeferHeader + 4 * cap words: counts [0] P2G-only, [1] whole chunk,
+// [2 + p] no record for a launch of step parity p; then the lists in that
+// order (cap entries each).
+constexpr int kDeferHeader = 8;
+inline size_t defer_words(size_t cap) { return kDeferHeader + 4 * cap; }
 static_assert(sizeof(SceneParams) == 30 * sizeof(float), "SceneParams must have no padding bytes");
 constexpr int kMaxCpicGroups = 8;
 
@@ -209,12 +221,24 @@ struct SortBuffers {
 
 enum TransferMode { kModeP2G = 0, kModeG2P2G = 1, kModeG2P = 2 };
 
+// A second stream and two events, for launches that fork work off `stream`
+// and join it back (the fused transfer's deferred chunks).
+struct ForkJoin {
+    cudaStream_t side;
+    cudaEvent_t fork, join;
+};
+
 // Launchers (tmpm_kernels.cu).  All run on `stream`.
 // `cur` and `next` share one hash table (block ids are stable within a batch)
 // and differ in their node pools; `cache` holds kCacheStride ints per CTA.
+// With `fj`, sp.defer set and one scene without CPIC, the fused transfer
+// (kModeG2P2G) runs as the fast kernel beside the chunks without a record
+// (on fj->side) and then the chunks the fast kernel deferred; the grid update
+// before it must carry the same step_index.
 void launch_transfer(int mode, const ParticleSoA &P, int n, const DevClass *classes, const GridTable &cur,
                      const GridTable &next, const SimParams &sp, const DevObstacle *obstacles,
-                     const float *planes, double *reactions, uint32_t *status, int *cache, cudaStream_t stream);
+                     const float *planes, double *reactions, uint32_t *status, int *cache, cudaStream_t stream,
+                     const ForkJoin *fj = nullptr);
 // Grid update of `g`'s pool; also zeroes the same blocks in `next`'s pool.
 void launch_grid_update(const GridTable &g, const GridTable &next, const SimParams &sp,
                         const DevObstacle *obstacles, const float *planes, double *reactions,

@@ -16,6 +16,10 @@
 // accumulates step-(n+1) mass and momentum with shared atomics and is flushed
 // to the block pool with one float4 atomic per touched node.  Chunks whose box
 // is too large (scattered particles) fall back to per-node global access.
+//
+// In a session the fused transfer of one scene runs as k_transfer_fast (the
+// common path only) with k_transfer_deferred beside and after it for the
+// chunks the common path does not cover (see transfer_chunk).
 
 #include <climits>
 
@@ -306,34 +310,99 @@ __device__ __forceinline__ float pow2_scale(float total) {
 // (80 registers: 172 bytes of spill stores against 28 without it), which cost
 // the obstacle-free dam break ~10 % of its fused transfer time.
 enum Variant { kPlain = 0, kMulti = 1, kCpic = 2, kPlainObst = 3 };
-template <int MODE, bool PLASTIC, int VARIANT, int THREADS, int MINB, int BS>
-__global__ void __launch_bounds__(THREADS, MINB)
-    k_transfer(ParticleSoA P, int n, const DevClass *__restrict__ classes, GridTable cur, GridTable next,
-               SimParams sp, const DevObstacle *__restrict__ obstacles, const float *__restrict__ planes,
-               double *reactions, uint32_t *status, int *__restrict__ cache) {
+constexpr bool has_obstacles(int variant) { return variant == kCpic || variant == kPlainObst; }
+
+// Shared memory of a transfer CTA, as pointers to its arrays.  One buffer
+// holds the G2P gather tile (float4 per node) and then the P2G scatter tile
+// (4 fixed-point ints per node, component-major).
+template <int THREADS, bool OBST>
+struct TransferSmem {
+    float4 *tile;
+    float (*fred)[4];
+    int *blk;
+    int *blk2;
+    int *used;
+    int (*red)[8];
+    Box *box;
+    Box *gbox;  // the G2P box, whose block ids the P2G reuses (shared: not held in registers)
+    int *abort;
+    float (*park)[THREADS];  // the affine matrix across the obstacle contact
+};
+// The arrays, one set per kernel for each (THREADS, OBST): the deferred
+// kernel's P2G-only and whole-chunk passes share them.
+template <int THREADS, bool OBST>
+__device__ __forceinline__ TransferSmem<THREADS, OBST> transfer_smem() {
+    __shared__ float4 tile[tile_nodes(THREADS)];
+    __shared__ float fred[THREADS / 32][4];
+    __shared__ int blk[kMaxTileBlocks];
+    __shared__ int blk2[kMaxTileBlocks];
+    __shared__ int used[kMaxTileBlocks];
+    __shared__ int red[THREADS / 32][8];
+    __shared__ Box box;
+    __shared__ Box gbox;
+    __shared__ int abort_flag;
+    __shared__ float park[OBST ? 9 : 1][THREADS];
+    return TransferSmem<THREADS, OBST>{tile, fred, blk, blk2, used, red, &box, &gbox, &abort_flag, park};
+}
+
+// Deferred-chunk lists (layout at DeferLists): 0 = P2G only, 1 = whole
+// chunk, 2 + p = no record for a launch of step parity p.
+__device__ __forceinline__ void defer_push(const SimParams &sp, int list, int chunk) {
+    const uint32_t slot = atomicAdd(sp.defer + list, 1u);
+    if (slot < static_cast<uint32_t>(sp.defer_cap))
+        sp.defer[kDeferHeader + static_cast<size_t>(list) * sp.defer_cap + slot] = static_cast<uint32_t>(chunk);
+}
+// The tag of the per-CTA records that the P2G of a launch with this step
+// index writes (1 or 2); a G2P accepts the tag of its own step index.  The
+// general chunks of a fused transfer run beside the fast kernel and write
+// their records meanwhile: the tag keeps the fast kernel from reading them
+// as records of its own step.
+__device__ __forceinline__ int record_tag(int step_index) { return 1 + (step_index & 1); }
+
+#define TMPM_TRANSFER_PARAMS                                                                                 \
+    ParticleSoA P, int n, const DevClass *__restrict__ classes, GridTable cur, GridTable next, SimParams sp, \
+        const DevObstacle *__restrict__ obstacles, const float *__restrict__ planes, double *reactions,      \
+        uint32_t *status, int *__restrict__ cache
+#define TMPM_TRANSFER_ARGS P, n, classes, cur, next, sp, obstacles, planes, reactions, status, cache
+
+// One chunk of THREADS consecutive particles in storage order, by one CTA.
+//
+// FAST (the fused G2P2G of one scene without CPIC) compiles only the common
+// path: the G2P box and block ids from the chunk's record, the gather from
+// the tile and the fixed-point scatter tile.  A chunk without a record of
+// this step is skipped (it is on the no-record list, which
+// k_transfer_deferred runs beside the fast kernel); a chunk whose particles
+// left the recorded box is deferred whole before any write; a chunk whose
+// P2G box does not fit or has a dominant particle stores its particles'
+// velocity and affine matrix and defers its P2G.  Without the fallback code
+// (box reduction and hash lookups for the G2P, per-node global gathers and
+// scatters) the fast kernel keeps the common path's values in registers: at
+// 64 registers 24 / 28 bytes of spill stores / loads against 52 / 84 with the
+// fallbacks compiled in.
+template <int MODE, bool PLASTIC, int VARIANT, int THREADS, int BS, bool FAST>
+__device__ __forceinline__ void transfer_chunk(TMPM_TRANSFER_PARAMS, const int chunk) {
     constexpr bool MULTI = VARIANT == kMulti;
     constexpr bool CPIC = VARIANT == kCpic;
-    constexpr bool OBST = VARIANT == kCpic || VARIANT == kPlainObst;
-    // One buffer holds the G2P gather tile (float4 per node) and then the P2G
-    // scatter tile (4 fixed-point ints per node, component-major).
+    constexpr bool OBST = has_obstacles(VARIANT);
+    static_assert(!FAST || (MODE == kModeG2P2G && !MULTI && !CPIC), "the fast path is the fused transfer of one scene");
     constexpr int kTileNodes = tile_nodes(THREADS);
-    __shared__ float4 s_tile[kTileNodes];
-    float4 *const s_gv = s_tile;
-    int (*const s_sc)[kTileNodes] = reinterpret_cast<int (*)[kTileNodes]>(s_tile);
-    __shared__ float s_fred[THREADS / 32][4];
-    __shared__ int s_blk[kMaxTileBlocks];
-    __shared__ int s_blk2[kMaxTileBlocks];
-    __shared__ int s_used[kMaxTileBlocks];
-    __shared__ int s_red[THREADS / 32][8];
-    __shared__ Box s_box;
-    __shared__ Box s_gbox;  // the G2P box, whose block ids the P2G reuses (shared: not held in registers)
-    __shared__ int s_abort;
-    __shared__ float s_park[OBST ? 9 : 1][THREADS];  // the affine matrix across the obstacle contact
+    const TransferSmem<THREADS, OBST> S = transfer_smem<THREADS, OBST>();
+    float4 *const s_gv = S.tile;
+    int (*const s_sc)[kTileNodes] = reinterpret_cast<int (*)[kTileNodes]>(S.tile);
+    float (*const s_fred)[4] = S.fred;
+    int *const s_blk = S.blk;
+    int *const s_blk2 = S.blk2;
+    int *const s_used = S.used;
+    int (*const s_red)[8] = S.red;
+    Box &s_box = *S.box;
+    Box &s_gbox = *S.gbox;
+    int &s_abort = *S.abort;
+    float (*const s_park)[THREADS] = S.park;
 
     const size_t cap = P.cap;
-    const int i = blockIdx.x * THREADS + threadIdx.x;
+    const int i = chunk * THREADS + static_cast<int>(threadIdx.x);
     const bool valid = i < n;
-    int *const cc = cache + static_cast<size_t>(blockIdx.x) * kCacheStride;
+    int *const cc = cache + static_cast<size_t>(chunk) * kCacheStride;
 
     if (threadIdx.x == 0) s_abort = (*reinterpret_cast<volatile uint32_t *>(status) & kFatal) != 0;
     if (MODE != kModeG2P) {
@@ -397,9 +466,12 @@ __global__ void __launch_bounds__(THREADS, MINB)
         // very positions (ids are stable within a batch), so normally no box
         // reduction and no hash lookup is needed.  A record that does not
         // cover every particle sends the CTA through the general path.
-        bool use_cache = cc[0] == 1;
+        bool use_cache = cc[0] == record_tag(sp.step_index);
+        if constexpr (FAST) {
+            if (!use_cache) return;  // on the no-record list (CTA-uniform)
+        }
         Box bx;
-        for (int attempt = 0; attempt < 2; ++attempt) {
+        for (int attempt = 0; attempt < (FAST ? 1 : 2); ++attempt) {
             if (use_cache) {
                 bx.lo[0] = cc[8];
                 bx.lo[1] = cc[9];
@@ -418,7 +490,7 @@ __global__ void __launch_bounds__(THREADS, MINB)
                 bx.nbt = cc[15];
                 bx.ok = 1;
                 tile_strides(bx.dim[1], bx.dim[2], bx.s1, bx.s2);
-            } else {
+            } else if constexpr (!FAST) {
                 reduce_box<THREADS, BS>(g2p_on, b, ns, s_red, s_box);
                 bx = s_box;
                 if (bx.ok) {
@@ -457,6 +529,10 @@ __global__ void __launch_bounds__(THREADS, MINB)
             }
             bad = __syncthreads_or(bad) != 0;
             if (!bad) break;
+            if constexpr (FAST) {  // a particle left the recorded box: the whole chunk, nothing written yet
+                if (threadIdx.x == 0) defer_push(sp, 1, chunk);
+                return;
+            }
             use_cache = false;
         }
         if (s_abort) return;
@@ -476,7 +552,7 @@ __global__ void __launch_bounds__(THREADS, MINB)
                 dys[a] = (a - fx.y) * h * inv_d;
                 dzs[a] = (a - fx.z) * h * inv_d;
             }
-            if (bx.ok) {
+            if (FAST || bx.ok) {
                 const int ox = b[0] - bx.lo[0], oy = b[1] - bx.lo[1], oz = b[2] - bx.lo[2];
                 // Paired f32 arithmetic (Blackwell FFMA2): accumulators
                 // p0..p2 = (vel, C column 0) and q0..q2 = (C column 1, C column 2)
@@ -714,6 +790,20 @@ __global__ void __launch_bounds__(THREADS, MINB)
     if (MODE == kModeP2G && s_abort) return;
     // one dominant particle: the whole CTA takes the f32 direct path (CTA-uniform)
     if (max_m > tot_m * kFloatModeShare || max_p > tot_p * kFloatModeShare) bx.ok = 0;
+    if constexpr (FAST) {
+        if (!bx.ok) {
+            // the P2G-only pass reads velocity and affine matrix from the
+            // particle arrays (position, F and plastic state are stored)
+            if (p2g_on) {
+                P.v[i] = v.x;
+                P.v[cap + i] = v.y;
+                P.v[2 * cap + i] = v.z;
+                store_m3(P.C, cap, i, Cm);
+            }
+            if (threadIdx.x == 0) defer_push(sp, 0, chunk);
+            return;
+        }
+    }
     if (bx.ok) {
         // every warp has finished its gather (barrier above): the buffer becomes the scatter tile
         for (int t = threadIdx.x; t < bx.nodes; t += THREADS) {
@@ -802,7 +892,7 @@ __global__ void __launch_bounds__(THREADS, MINB)
             cc[kCacheHeader + t] = id;
         }
         if (threadIdx.x == 0) {
-            cc[0] = 1;
+            cc[0] = record_tag(sp.step_index + 1);
             cc[1] = bx.blo[0];
             cc[2] = bx.blo[1];
             cc[3] = bx.blo[2];
@@ -836,7 +926,10 @@ __global__ void __launch_bounds__(THREADS, MINB)
                                   static_cast<float>(py) * inv_sp, static_cast<float>(pz) * inv_sp));
         }
     } else {
-        if (threadIdx.x == 0) cc[0] = 0;
+        if (threadIdx.x == 0) {
+            cc[0] = 0;
+            if (!MULTI && sp.defer) defer_push(sp, 2 + ((sp.step_index + 1) & 1), chunk);
+        }
         if (active) {
             unsigned long long last_key = kEmptyKey;
             int last_id = -1;
@@ -862,6 +955,54 @@ __global__ void __launch_bounds__(THREADS, MINB)
 #undef SCN
 }
 
+// The general transfer: every chunk, one CTA each.
+template <int MODE, bool PLASTIC, int VARIANT, int THREADS, int MINB, int BS>
+__global__ void __launch_bounds__(THREADS, MINB) k_transfer(TMPM_TRANSFER_PARAMS) {
+    transfer_chunk<MODE, PLASTIC, VARIANT, THREADS, BS, false>(TMPM_TRANSFER_ARGS, blockIdx.x);
+}
+
+// The fast fused transfer: every chunk with a record of this step.
+template <bool PLASTIC, int VARIANT, int THREADS, int MINB, int BS>
+__global__ void __launch_bounds__(THREADS, MINB) k_transfer_fast(TMPM_TRANSFER_PARAMS) {
+    transfer_chunk<kModeG2P2G, PLASTIC, VARIANT, THREADS, BS, true>(TMPM_TRANSFER_ARGS, blockIdx.x);
+}
+
+// The deferred chunks of a fast fused transfer through the general path, a
+// grid-stride loop of CTAs over a list.  PRE: the chunks without a record of
+// this step (written by the previous launch's general P2Gs), run beside the
+// fast kernel; otherwise the chunks the fast kernel deferred: P2G only, then
+// whole chunks.  The register bound is the general kernel's: a CTA of this
+// kernel running beside the fast kernel then takes one CTA slot of an SM, not
+// the whole register file.
+template <bool PRE, bool PLASTIC, int VARIANT, int THREADS, int BS>
+__global__ void __launch_bounds__(THREADS, THREADS == 256 ? TMPM_TRANSFER_MIN_BLOCKS : 8)
+    k_transfer_deferred(TMPM_TRANSFER_PARAMS) {
+    const uint32_t cap = static_cast<uint32_t>(sp.defer_cap);
+    const uint32_t *const lists = sp.defer + kDeferHeader;
+    if (PRE) {
+        const int list = 2 + (sp.step_index & 1);
+        const uint32_t count = min(sp.defer[list], cap);
+        for (uint32_t e = blockIdx.x; e < count; e += gridDim.x) {
+            __syncthreads();  // the previous chunk's last reads of shared memory
+            transfer_chunk<kModeG2P2G, PLASTIC, VARIANT, THREADS, BS, false>(
+                TMPM_TRANSFER_ARGS, static_cast<int>(lists[list * cap + e]));
+        }
+    } else {
+        const uint32_t np = min(sp.defer[0], cap), nw = min(sp.defer[1], cap);
+        for (uint32_t e = blockIdx.x; e < np + nw; e += gridDim.x) {
+            __syncthreads();
+            if (e < np)
+                transfer_chunk<kModeP2G, PLASTIC, VARIANT, THREADS, BS, false>(TMPM_TRANSFER_ARGS,
+                                                                               static_cast<int>(lists[e]));
+            else
+                transfer_chunk<kModeG2P2G, PLASTIC, VARIANT, THREADS, BS, false>(
+                    TMPM_TRANSFER_ARGS, static_cast<int>(lists[cap + (e - np)]));
+        }
+    }
+}
+#undef TMPM_TRANSFER_ARGS
+#undef TMPM_TRANSFER_PARAMS
+
 // Grid update over all allocated blocks; also zeroes those blocks in the other pool.
 // MULTI: each block takes its scene's parameters from the scene table
 // (scene = block namespace >> kSceneShift).  Blocks have edge 2^BS cells.
@@ -871,6 +1012,12 @@ __global__ void __launch_bounds__(256) k_grid(GridTable g, GridTable nxt, SimPar
                                                const DevObstacle *__restrict__ obstacles,
                                                const float *__restrict__ planes, double *reactions, uint32_t *status) {
     __shared__ int s_abort;
+    // empty the deferred-chunk lists that the next transfer (step_index) fills
+    if (!MULTI && sp.defer && blockIdx.x == 0 && threadIdx.x == 0) {
+        sp.defer[0] = 0;
+        sp.defer[1] = 0;
+        sp.defer[2 + ((sp.step_index + 1) & 1)] = 0;
+    }
     if (threadIdx.x == 0) s_abort = (*reinterpret_cast<volatile uint32_t *>(status) & kFatal) != 0;
     __syncthreads();
     if (s_abort) return;
@@ -1080,10 +1227,60 @@ int device_sm_count() {
     return sms;
 }
 
+namespace {
+// The fused transfer of one scene as three kernels: the no-record chunks on
+// fj.side beside the fast kernel on `stream`, then (after both) the chunks
+// the fast kernel deferred.  The deferred kernels run one CTA per SM over
+// their lists; an empty list costs one short launch.
+void launch_fused(const ParticleSoA &P, int n, const DevClass *classes, const GridTable &cur, const GridTable &next,
+                  const SimParams &sp, const DevObstacle *obstacles, const float *planes, double *reactions,
+                  uint32_t *status, int *cache, cudaStream_t stream, const ForkJoin &fj) {
+    const bool pl = sp.has_plastic != 0;
+    const bool obst = sp.num_obstacles > 0;
+    const int shape = pl ? 0 : sp.shape;
+    const bool big = !pl && sp.block_shift == kBigBlockShift;
+    const int sms = device_sm_count();
+#define TMPM_FUSED(PL, V, T, B, BS)                                                                                \
+    do {                                                                                                           \
+        cudaEventRecord(fj.fork, stream);                                                                          \
+        cudaStreamWaitEvent(fj.side, fj.fork, 0);                                                                  \
+        k_transfer_deferred<true, PL, V, T, BS><<<sms, T, 0, fj.side>>>(P, n, classes, cur, next, sp, obstacles,   \
+                                                                        planes, reactions, status, cache);         \
+        cudaEventRecord(fj.join, fj.side);                                                                         \
+        k_transfer_fast<PL, V, T, B, BS><<<dim3((n + (T) - 1) / (T)), T, 0, stream>>>(                             \
+            P, n, classes, cur, next, sp, obstacles, planes, reactions, status, cache);                            \
+        cudaStreamWaitEvent(stream, fj.join, 0);                                                                   \
+        k_transfer_deferred<false, PL, V, T, BS><<<sms, T, 0, stream>>>(P, n, classes, cur, next, sp, obstacles,   \
+                                                                        planes, reactions, status, cache);         \
+    } while (0)
+#define TMPM_FUSED_SHAPES_BS(V, BS)                                    \
+    do {                                                               \
+        if (shape == 1) TMPM_FUSED(false, V, 128, 8, BS);              \
+        else if (shape == 2) TMPM_FUSED(false, V, 256, 3, BS);         \
+        else TMPM_FUSED(false, V, 256, TMPM_TRANSFER_MIN_BLOCKS, BS);  \
+    } while (0)
+#define TMPM_FUSED_SHAPES(V)                                   \
+    do {                                                       \
+        if (big) TMPM_FUSED_SHAPES_BS(V, kBigBlockShift);      \
+        else TMPM_FUSED_SHAPES_BS(V, kBlockShift);             \
+    } while (0)
+    if (pl) TMPM_FUSED(true, kPlainObst, 256, TMPM_TRANSFER_MIN_BLOCKS, kBlockShift);
+    else if (obst) TMPM_FUSED_SHAPES(kPlainObst);
+    else TMPM_FUSED_SHAPES(kPlain);
+#undef TMPM_FUSED_SHAPES
+#undef TMPM_FUSED_SHAPES_BS
+#undef TMPM_FUSED
+}
+}  // namespace
+
 void launch_transfer(int mode, const ParticleSoA &P, int n, const DevClass *classes, const GridTable &cur,
                      const GridTable &next, const SimParams &sp, const DevObstacle *obstacles, const float *planes,
-                     double *reactions, uint32_t *status, int *cache, cudaStream_t stream) {
+                     double *reactions, uint32_t *status, int *cache, cudaStream_t stream, const ForkJoin *fj) {
     if (n <= 0) return;
+    if (mode == kModeG2P2G && fj && sp.defer && !sp.multi && !sp.cpic) {
+        launch_fused(P, n, classes, cur, next, sp, obstacles, planes, reactions, status, cache, stream, *fj);
+        return;
+    }
     // Launch shapes other than the default exist for the variants the tuner
     // picks among (no plastic state; one scene or a batch).  Plastic state and
     // CPIC run with the obstacle contact compiled in, with or without obstacles.
@@ -1154,8 +1351,20 @@ void touch_transfer() {
     cudaFuncAttributes a;
     cudaFuncGetAttributes(&a, k_transfer<M, false, V, T, B, BS>);
 }
+template <int V, int T, int B, int BS>
+void touch_fused() {
+    if constexpr (V == kPlain || V == kPlainObst) {
+        cudaFuncAttributes a;
+        cudaFuncGetAttributes(&a, k_transfer_fast<false, V, T, B, BS>);
+        cudaFuncGetAttributes(&a, k_transfer_deferred<true, false, V, T, BS>);
+        cudaFuncGetAttributes(&a, k_transfer_deferred<false, false, V, T, BS>);
+    }
+}
 template <int V, int BS>
 void touch_shapes() {
+    touch_fused<V, 256, TMPM_TRANSFER_MIN_BLOCKS, BS>();
+    touch_fused<V, 128, 8, BS>();
+    touch_fused<V, 256, 3, BS>();
     touch_transfer<kModeP2G, V, 256, TMPM_TRANSFER_MIN_BLOCKS, BS>();
     touch_transfer<kModeG2P2G, V, 256, TMPM_TRANSFER_MIN_BLOCKS, BS>();
     touch_transfer<kModeG2P, V, 256, TMPM_TRANSFER_MIN_BLOCKS, BS>();

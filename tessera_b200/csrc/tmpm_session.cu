@@ -70,6 +70,8 @@ struct TmpmSession {
     DevBuf<DevRigidMap> rigid_maps;
     size_t rigid_body_count = 0, rigid_map_count = 0;
     DevBuf<int> cta_cache;  // kCacheStride ints per transfer CTA
+    DevBuf<uint32_t> defer;  // the fused transfer's deferred-chunk lists (defer_words of the chunk count)
+    ForkJoin fj{};           // second stream and events of the fused transfer
     DevBuf<uint32_t> sort_keys[2], sort_vals[2], sort_hist, sort_totals;
     PinnedBuf staging;         // readback
     DevBuf<float> unsorted;    // readback rows in world order
@@ -91,8 +93,12 @@ struct TmpmSession {
         if (stream) {
             cudaStreamSynchronize(stream);
         }
+        if (fj.side) cudaStreamSynchronize(fj.side);
         drop_graphs();
         if (done) cudaEventDestroy(done);
+        if (fj.fork) cudaEventDestroy(fj.fork);
+        if (fj.join) cudaEventDestroy(fj.join);
+        if (fj.side) cudaStreamDestroy(fj.side);
         for (cudaEvent_t &ev : read_events)
             if (ev) cudaEventDestroy(ev);
         if (stream) cudaStreamDestroy(stream);
@@ -274,6 +280,8 @@ struct TmpmSession {
         size_t ctas = (cap + kMinTransferThreads - 1) / kMinTransferThreads;
         if (cta_cache.count < ctas * kCacheStride)
             if ((e = cta_cache.alloc(ctas * kCacheStride))) return cuda_fail(e, "cudaMalloc cache");
+        if (defer.count < defer_words(ctas))
+            if ((e = defer.alloc(defer_words(ctas)))) return cuda_fail(e, "cudaMalloc deferred lists");
         if (force.count < 3 * std::max<size_t>(world.n, 1)) {
             if ((e = force.alloc(3 * std::max<size_t>(world.n, 1)))) return cuda_fail(e, "cudaMalloc forces");
             cudaMemsetAsync(force.ptr, 0, sizeof(float) * force.count, stream);
@@ -389,17 +397,36 @@ struct TmpmSession {
         grid_views(g, bs);
         const ParticleSoA P = pbuf[rows].view(force.ptr, std::max<size_t>(world.n, 1));
         launch_clear_table(g[0], g[1], bs, stream);
-        launch_transfer(kModeP2G, P, n_dev, classes.ptr, g[1], g[0], sp, dev_obstacles.ptr, dev_planes.ptr,
+        const SimParams sp0 = substep_params(sp, -1, false);
+        open_defer_lists(sp0);
+        launch_transfer(kModeP2G, P, n_dev, classes.ptr, g[1], g[0], sp0, dev_obstacles.ptr, dev_planes.ptr,
                         reactions.ptr, status.ptr, cta_cache.ptr, stream);
         for (uint32_t k = 0; k < seg; ++k) {
             const GridTable &gc = g[k & 1], &gn = g[(k + 1) & 1];
-            launch_grid_update(gc, gn, sp, dev_obstacles.ptr, dev_planes.ptr, reactions.ptr, status.ptr, stream);
-            SimParams spk = sp;
-            spk.apply_force = (apply_force && k == 0) ? 1 : 0;
+            const SimParams spk = substep_params(sp, static_cast<int>(k), apply_force && k == 0);
+            launch_grid_update(gc, gn, spk, dev_obstacles.ptr, dev_planes.ptr, reactions.ptr, status.ptr, stream);
             launch_transfer(k + 1 == seg ? kModeG2P : kModeG2P2G, P, n_dev, classes.ptr, gc, gn, spk,
-                            dev_obstacles.ptr, dev_planes.ptr, reactions.ptr, status.ptr, cta_cache.ptr, stream);
+                            dev_obstacles.ptr, dev_planes.ptr, reactions.ptr, status.ptr, cta_cache.ptr, stream, &fj);
             if (apply_force && k == 0) cudaMemsetAsync(force.ptr, 0, sizeof(float) * force.count, stream);
         }
+    }
+
+    // The parameters of one launch of a segment: the substep it completes
+    // (-1: the opening P2G), which tags the per-CTA records and picks the
+    // deferred-chunk lists, and the one-shot forces.
+    SimParams substep_params(const SimParams &sp, int step_index, bool apply_force) const {
+        SimParams spk = sp;
+        spk.step_index = step_index;
+        spk.apply_force = apply_force ? 1 : 0;
+        spk.defer = defer.ptr;
+        spk.defer_cap = static_cast<int>(defer.count >= static_cast<size_t>(kDeferHeader)
+                                             ? (defer.count - kDeferHeader) / 4
+                                             : 0);
+        return spk;
+    }
+    // Empty the deferred-chunk list counts before a segment's opening P2G.
+    void open_defer_lists(const SimParams &sp0) {
+        if (sp0.defer) cudaMemsetAsync(sp0.defer, 0, sizeof(uint32_t) * kDeferHeader, stream);
     }
 
     // Everything launch_segment's kernels bake in, as a byte string.
@@ -409,8 +436,8 @@ struct TmpmSession {
             ParticleSoA rows[2];
             GridTable g[2];
             SortBuffers sb;
-            const void *ptr[7];
-            size_t force_count, n_world;
+            const void *ptr[8];
+            size_t force_count, n_world, defer_count;
             int64_t from, resort, seg, n_dev, apply_force;
         } k;
         std::memset(&k, 0, sizeof k);
@@ -418,10 +445,11 @@ struct TmpmSession {
         for (int b = 0; b < 2; ++b) k.rows[b] = pbuf[b].view(force.ptr, std::max<size_t>(world.n, 1));
         grid_views(k.g, sp.block_shift);
         k.sb = sort_buffers();
-        const void *ptrs[7] = {classes.ptr, dev_obstacles.ptr, dev_planes.ptr, reactions.ptr, status.ptr,
-                               cta_cache.ptr, force.ptr};
-        for (int i = 0; i < 7; ++i) k.ptr[i] = ptrs[i];
+        const void *ptrs[8] = {classes.ptr, dev_obstacles.ptr, dev_planes.ptr, reactions.ptr, status.ptr,
+                               cta_cache.ptr, force.ptr, defer.ptr};
+        for (int i = 0; i < 8; ++i) k.ptr[i] = ptrs[i];
         k.force_count = force.count;
+        k.defer_count = defer.count;
         k.n_world = world.n;
         k.from = from;
         k.resort = resort;
@@ -524,22 +552,23 @@ struct TmpmSession {
                 const ParticleSoA P = pbuf[resort ? cur ^ 1 : cur].view(force.ptr, std::max<size_t>(world.n, 1));
                 tick(0);
                 launch_clear_table(g[0], g[1], bs, stream);
-                launch_transfer(kModeP2G, P, n_dev, classes.ptr, g[1], g[0], sp, dev_obstacles.ptr, dev_planes.ptr,
+                const SimParams sp0 = substep_params(sp, -1, false);
+                open_defer_lists(sp0);
+                launch_transfer(kModeP2G, P, n_dev, classes.ptr, g[1], g[0], sp0, dev_obstacles.ptr, dev_planes.ptr,
                                 reactions.ptr, status.ptr, cta_cache.ptr, stream);
                 tock(0);
                 for (uint32_t k = 0; k < seg; ++k) {
                     const GridTable &gc = g[k & 1], &gn = g[(k + 1) & 1];
+                    const SimParams spk = substep_params(sp, static_cast<int>(k), apply_force && k == 0);
                     tick(0);
-                    launch_grid_update(gc, gn, sp, dev_obstacles.ptr, dev_planes.ptr, reactions.ptr, status.ptr,
+                    launch_grid_update(gc, gn, spk, dev_obstacles.ptr, dev_planes.ptr, reactions.ptr, status.ptr,
                                        stream);
                     tock(1);
-                    SimParams spk = sp;
-                    spk.apply_force = (apply_force && k == 0) ? 1 : 0;
                     const bool last = k + 1 == seg;
                     tick(0);
                     launch_transfer(last ? kModeG2P : kModeG2P2G, P, n_dev, classes.ptr, gc, gn, spk,
                                     dev_obstacles.ptr, dev_planes.ptr, reactions.ptr, status.ptr, cta_cache.ptr,
-                                    stream);
+                                    stream, &fj);
                     tock(last ? 3 : 2);
                     if (apply_force && k == 0) cudaMemsetAsync(force.ptr, 0, sizeof(float) * force.count, stream);
                 }
@@ -755,7 +784,10 @@ TmpmStatus tmpm_session_create(const TmpmParams *params, const TmpmParticleArray
         return TMPM_ERR_DEVICE;
     }
     if ((e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking)) ||
-        (e = cudaEventCreateWithFlags(&s->done, cudaEventDisableTiming))) {
+        (e = cudaEventCreateWithFlags(&s->done, cudaEventDisableTiming)) ||
+        (e = cudaStreamCreateWithFlags(&s->fj.side, cudaStreamNonBlocking)) ||
+        (e = cudaEventCreateWithFlags(&s->fj.fork, cudaEventDisableTiming)) ||
+        (e = cudaEventCreateWithFlags(&s->fj.join, cudaEventDisableTiming))) {
         g_last_error = std::string("stream setup: ") + cudaGetErrorString(e);
         return TMPM_ERR_DEVICE;
     }
