@@ -50,7 +50,14 @@ sys.path.insert(0, ROOT)
 BATCH = 64
 # re-sort per batch: bin keys, 4 radix passes (27-bit keys) x (hist, scan, scatter), gather
 RESORT_LAUNCHES = 1 + 4 * 3 + 1
+# kernels of one 64-substep segment: re-sort, table clear, opening P2G, then per
+# substep the grid update and the fused transfer (k_transfer_fast with the two
+# k_transfer_deferred launches beside and after it), the last substep's
+# transfer a single G2P launch
+SEGMENT_LAUNCHES = RESORT_LAUNCHES + 2 + 4 * (BATCH - 1) + 2
 METRIC = "particle-substeps/s"
+# the fields a substep changes (--save-state / --load-state)
+STATE_FIELDS = ("position", "velocity", "deformation", "affine", "plastic")
 
 
 def parse():
@@ -73,6 +80,11 @@ def parse():
                     help="fix the single-scene launch shape (index of _native.launch_shapes()) instead of tuning it")
     ap.add_argument("--only", choices=["batched", "serving", "adjoint", "obstacle"],
                     help="run one section alone and print its result (profiling; not the benchmark line)")
+    ap.add_argument("--save-state", default=None,
+                    help="after the single-scene timing, save the evolved particle state (.npz) for --load-state")
+    ap.add_argument("--load-state", default=None,
+                    help="start the single scene from a state saved by --save-state (profiling the evolved scene "
+                         "with few launches before the captured one; not the benchmark line)")
     return ap.parse_args()
 
 
@@ -503,6 +515,10 @@ def run_tessera(args, world, rank, local):
 
     torch.cuda.set_device(local)
     sc = scenes.dam_break(seed=2 + rank, scale=args.scale)
+    if args.load_state:  # the evolved dynamic fields over the same seeded scene
+        with np.load(args.load_state) as st:
+            for f in STATE_FIELDS:
+                getattr(sc.particles, f)[...] = st[f]
     n = sc.particles.count
     session = Session(sc.params, sc.particles, sc.dt, device=local, launch_shape=args.launch_shape)
     # active grid nodes G (nodes with mass after P2G) for the algorithmic bytes
@@ -537,6 +553,9 @@ def run_tessera(args, world, rank, local):
     _, kms = session.bench_substeps(BATCH, per_kernel=True)
     session.synchronize()
     shape_end = session.launch_shape()
+    if args.save_state:  # f32 is exact: the device state is f32
+        st = session.particles()
+        np.savez(args.save_state, **{f: getattr(st, f).astype(np.float32) for f in STATE_FIELDS})
     g2p2g_ms = float(kms[2])
     peak, peak_kind = measured_peaks()
     # algorithmic bytes of one fused G2P->P2G launch: 248 B per particle (P2G 104 + G2P 48 + 96 write) and
@@ -629,7 +648,7 @@ def run_tessera(args, world, rank, local):
                        "launch_shape": shape_summary(shape_info),
                        "launch_shape_after_timing": shape_summary(shape_end),
                        "parallelism": f"replicas x{world}"},
-            "gpu_launches": (2 * BATCH + 2 + RESORT_LAUNCHES) * args.steps,
+            "gpu_launches": SEGMENT_LAUNCHES * args.steps,
             "roofline": roofline,
             "cpu_baseline": cpu,
             "e2e": e2e,

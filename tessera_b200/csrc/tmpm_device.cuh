@@ -518,6 +518,16 @@ __device__ __forceinline__ bool obstacle_may_contact(const DevObstacle &o, V3f p
     return true;
 }
 
+// Whether a point may lie within `r` of an obstacle's surface: its local
+// coordinates within r of the box that holds the surface (DevObstacle::reach).
+// Inline and call-free; false guarantees obstacle_surface(o, p) >= r, so the
+// particle has no contact with this obstacle.
+__device__ __forceinline__ bool obstacle_near(const DevObstacle &o, V3f p, float r) {
+    const V3f l = qrot_inv(o.q, p - mk(o.center[0], o.center[1], o.center[2]));
+    return fabsf(l.x) <= o.reach[0] + r && fabsf(l.y) <= o.reach[1] + r && l.z <= o.reach[2] + r &&
+           (o.reach[3] != 0.0f || l.z >= -o.reach[2] - r);
+}
+
 // RigidObstacle::contact_velocity (obstacle.rs:501-540).
 __device__ __forceinline__ V3f contact_velocity(const DevObstacle &o, V3f point, V3f vel, V3f n) {
     V3f surface = mk(o.lin[0], o.lin[1], o.lin[2]) +

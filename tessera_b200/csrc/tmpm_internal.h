@@ -112,6 +112,12 @@ struct DevObstacle {
     float ang[4];
     float dims[4];
     float verts[12];    // a, b, c (xyz + pad)
+    // Local-frame box that holds the whole surface: |x| <= reach[0],
+    // |y| <= reach[1], |z| <= reach[2]; reach[3] = 1 drops the lower z bound
+    // (the ground, a half-space below its plane).  A point whose local
+    // coordinates lie farther than a particle radius outside it cannot touch
+    // the obstacle (obstacle_near).
+    float reach[4];
 };
 
 // Rigid body of the two-way coupling (the reference's RigidState layout,

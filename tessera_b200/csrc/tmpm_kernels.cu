@@ -384,9 +384,13 @@ __device__ __forceinline__ void transfer_chunk(TMPM_TRANSFER_PARAMS, const int c
     constexpr bool MULTI = VARIANT == kMulti;
     constexpr bool CPIC = VARIANT == kCpic;
     constexpr bool OBST = has_obstacles(VARIANT);
+    // The obstacle contact is compiled into the general path only: the fast
+    // path tests each particle against the obstacles' reach (inline, no call)
+    // and defers a chunk that may touch one.
+    constexpr bool CONTACT = OBST && !FAST;
     static_assert(!FAST || (MODE == kModeG2P2G && !MULTI && !CPIC), "the fast path is the fused transfer of one scene");
     constexpr int kTileNodes = tile_nodes(THREADS);
-    const TransferSmem<THREADS, OBST> S = transfer_smem<THREADS, OBST>();
+    const TransferSmem<THREADS, CONTACT> S = transfer_smem<THREADS, CONTACT>();
     float4 *const s_gv = S.tile;
     int (*const s_sc)[kTileNodes] = reinterpret_cast<int (*)[kTileNodes]>(S.tile);
     float (*const s_fred)[4] = S.fred;
@@ -626,9 +630,10 @@ __device__ __forceinline__ void transfer_chunk(TMPM_TRANSFER_PARAMS, const int c
         // live is saved) an updating particle reads F after the contact.
         const bool updates = g2p_on && !fixed;
         if (valid) {
-            if (!OBST || !updates) F = load_m3(P.F, cap, i);
+            if (!CONTACT || !updates) F = load_m3(P.F, cap, i);
             k = classes[cw & kClassMask];
         }
+        V3f pos = x;
         if (updates) {
             // Particle update (gpu.wgsl:885-1003; world.rs:443-463).
             if (sp.apply_force) {
@@ -637,7 +642,7 @@ __device__ __forceinline__ void transfer_chunk(TMPM_TRANSFER_PARAMS, const int c
                 vel = vel + mk(f.x / k.mass, f.y / k.mass, f.z / k.mass) * dt;  // force / mass * dt (gpu.wgsl:885)
             }
             vel = vel * expf(-k.damping * dt);
-            V3f pos = x + vel * dt;
+            pos = x + vel * dt;
             const float radius = k.radius;
             if (SCN(has_bounds)) {
                 for (int a = 0; a < 3; ++a) {
@@ -652,7 +657,7 @@ __device__ __forceinline__ void transfer_chunk(TMPM_TRANSFER_PARAMS, const int c
                     }
                 }
             }
-            if (OBST) {
+            if constexpr (CONTACT) {
                 // The surface function is an out-of-line call, around which
                 // every live value is saved: the affine matrix waits in shared
                 // memory and the class record is dropped (reloaded below), so
@@ -686,7 +691,26 @@ __device__ __forceinline__ void transfer_chunk(TMPM_TRANSFER_PARAMS, const int c
                 aff.c2 = mk(s_park[6][threadIdx.x], s_park[7][threadIdx.x], s_park[8][threadIdx.x]);
                 k = classes[cw & kClassMask];
             }
-            if (OBST) F = load_m3(P.F, cap, i);
+        }
+        if constexpr (OBST && FAST) {
+            // A chunk in which some particle may touch an obstacle runs whole
+            // through the general path, which has the contact: deferred here,
+            // before this kernel writes anything or flags a failure for it.
+            // The reach test is conservative (f32 rounding margins in the
+            // reach and 5 % of a cell here), so a chunk that stays has no
+            // contact, exactly as the general path would find.
+            bool near = false;
+            if (updates) {
+                const float r = k.radius * 1.0001f + 0.05f * h;
+                for (int oi = 0; oi < sp.num_obstacles; ++oi) near = near || obstacle_near(obstacles[oi], pos, r);
+            }
+            if (__syncthreads_or(near)) {
+                if (threadIdx.x == 0) defer_push(sp, 1, chunk);
+                return;
+            }
+        }
+        if (updates) {
+            if (CONTACT) F = load_m3(P.F, cap, i);
             M3f Fn = mul(add(m3_identity(), scale(aff, dt)), F);
             bool plastic_ok = true;
             if (k.kind == kMatFluid) {
@@ -770,7 +794,7 @@ __device__ __forceinline__ void transfer_chunk(TMPM_TRANSFER_PARAMS, const int c
     V3f mv = mk(0, 0, 0);
     float bound_m = 0.f, bound_p = 0.f;
     if (active) {
-        M3f S = scaled_stress<!OBST && !PLASTIC>(k, F, Cm, -dt * inv_d, pl[0]);
+        M3f S = scaled_stress<!CONTACT && !PLASTIC>(k, F, Cm, -dt * inv_d, pl[0]);
         A = add(S, scale(Cm, k.mass));
         mv = v * k.mass;
         // |(m v + A dpos)_i| <= |m v_i| + 1.5 h sum_j |A_ij| and a particle's 27 weights sum to one,

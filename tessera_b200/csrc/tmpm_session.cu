@@ -31,6 +31,42 @@ using namespace tmpm;
 
 void tmpm::set_last_error(const std::string &msg) { g_last_error = msg; }
 
+namespace {
+// The local-frame box that holds an obstacle's surface (DevObstacle::reach),
+// from the shape definitions of obstacle.rs:372-472, widened by 1e-4 of
+// itself against the f32 rounding of the device's distance evaluations.
+void obstacle_reach(const TmpmObstacle &o, DevObstacle &d) {
+    const double *dm = o.dims;
+    double r[3] = {0.0, 0.0, 0.0};
+    double ground = 0.0;
+    switch (o.shape) {
+    case TMPM_SHAPE_SPHERE:
+        r[0] = r[1] = r[2] = dm[0];
+        break;
+    case TMPM_SHAPE_BOX:
+        r[0] = dm[0], r[1] = dm[1], r[2] = dm[2];
+        break;
+    case TMPM_SHAPE_CAPSULE:  // segment of half height dm[0] along z, radius dm[1]
+        r[0] = r[1] = dm[1];
+        r[2] = dm[0] + dm[1];
+        break;
+    case TMPM_SHAPE_CYLINDER:  // half height dm[0] along z, radius dm[1]
+    case TMPM_SHAPE_CONE:      // base radius dm[1] at z = -dm[0], apex at z = dm[0]
+        r[0] = r[1] = dm[1];
+        r[2] = dm[0];
+        break;
+    case TMPM_SHAPE_GROUND:  // the plane z = 0 over |x| <= dm[0], |y| <= dm[1], solid below
+        r[0] = dm[0], r[1] = dm[1];
+        ground = 1.0;
+        break;
+    default:  // triangle prism, convex: the bounding radius
+        r[0] = r[1] = r[2] = static_cast<double>(d.center[3]);
+    }
+    for (int k = 0; k < 3; ++k) d.reach[k] = static_cast<float>(r[k] * (1.0 + 1e-4));
+    d.reach[3] = static_cast<float>(ground);
+}
+}  // namespace
+
 // Segments of at least this many substeps are captured and replayed as CUDA
 // graphs (shorter ones, e.g. the single substeps of tmpm_step_cfl, are
 // launched: a capture costs more than it saves when not repeated).
@@ -266,6 +302,7 @@ struct TmpmSession {
                 }
                 ok = ok && f32_ok(o.bound_radius * (1.0 + 1e-5), d.center[3]);
             }
+            obstacle_reach(o, d);
             if (!ok) return fail(TMPM_ERR_INVALID_INPUT, "obstacle not representable in f32");
             dobs.push_back(d);
         }
