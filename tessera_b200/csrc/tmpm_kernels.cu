@@ -296,6 +296,35 @@ __device__ __forceinline__ float pow2_scale(float total) {
     return exp2f(e);
 }
 
+// The blocks a particle's 3 x 3 x 3 stencil reaches from base cell b: at most
+// two per axis, slot (qx << 2) | (qy << 1) | qz for block (b >> BS) + q.  Each
+// thread looks up (or, INSERT, finds or inserts) the distinct ones and stores
+// the ids at ids[slot * THREADS], the unreached slots -1.
+template <int THREADS, int BS, bool INSERT>
+__device__ __forceinline__ void stencil_blocks(const GridTable &g, const int b[3], uint32_t ns, int *ids,
+                                               uint32_t *status) {
+    const int g0 = b[0] >> BS, g1 = b[1] >> BS, g2 = b[2] >> BS;
+    const int e0 = ((b[0] + 2) >> BS) - g0, e1 = ((b[1] + 2) >> BS) - g1, e2 = ((b[2] + 2) >> BS) - g2;
+    for (int q = 0; q < 8; ++q) {
+        const int qx = q >> 2, qy = (q >> 1) & 1, qz = q & 1;
+        int id = -1;
+        if (qx <= e0 && qy <= e1 && qz <= e2) {
+            const unsigned long long key = block_key(g0 + qx, g1 + qy, g2 + qz, ns);
+            if constexpr (INSERT)
+                id = find_or_insert_block(g, key, make_int4(g0 + qx, g1 + qy, g2 + qz, static_cast<int>(ns)), status);
+            else
+                id = lookup_block(g, key);
+        }
+        ids[q * THREADS] = id;
+    }
+}
+// The slot (stencil_blocks) of the block holding cell (cx, cy, cz) of the
+// stencil based at b.
+template <int BS>
+__device__ __forceinline__ int stencil_block_slot(const int b[3], int cx, int cy, int cz) {
+    return (((cx >> BS) - (b[0] >> BS)) << 2) | (((cy >> BS) - (b[1] >> BS)) << 1) | ((cz >> BS) - (b[2] >> BS));
+}
+
 // PLASTIC selects the variant that carries plastic state (snow, sand, NH sand);
 // scenes without plastic materials run the leaner variant.  VARIANT selects
 // kPlain (one scene without obstacles, parameters from the kernel parameters),
@@ -596,21 +625,22 @@ __device__ __forceinline__ void transfer_chunk(TMPM_TRANSFER_PARAMS, const int c
                 aff.c1 = mk(q0.x, q1.x, q2.x);
                 aff.c2 = mk(q0.y, q1.y, q2.y);
             } else {
-                unsigned long long last_key = kEmptyKey;
-                int last_id = -1;
+                // Per-node global gather.  The stencil's blocks are looked up
+                // first (the tile is unused on this path and holds each
+                // thread's ids), so no node load waits on a lookup.
+                int *const ids = reinterpret_cast<int *>(s_gv) + threadIdx.x;
+                stencil_blocks<THREADS, BS, false>(cur, b, ns, ids, status);
+#pragma unroll
                 for (int a = 0; a < 3; ++a)
+#pragma unroll
                     for (int c = 0; c < 3; ++c)
+#pragma unroll
                         for (int e = 0; e < 3; ++e) {
-                            int cx = b[0] + a, cy = b[1] + c, cz = b[2] + e;
-                            unsigned long long key =
-                                block_key(cx >> BS, cy >> BS, cz >> BS, ns);
-                            if (key != last_key) {
-                                last_key = key;
-                                last_id = lookup_block(cur, key);
-                            }
+                            const int cx = b[0] + a, cy = b[1] + c, cz = b[2] + e;
+                            const int id = ids[stencil_block_slot<BS>(b, cx, cy, cz) * THREADS];
                             float4 val = make_float4(0.f, 0.f, 0.f, 0.f);
-                            if (last_id >= 0)
-                                val = __ldcg(cur.pool + static_cast<size_t>(last_id) * (1 << (3 * BS)) + node_local<BS>(cx, cy, cz));
+                            if (id >= 0)
+                                val = __ldcg(cur.pool + static_cast<size_t>(id) * (1 << (3 * BS)) + node_local<BS>(cx, cy, cz));
                             const float w = wx[a] * wy[c] * wz[e];
                             const V3f nv = mk(val.x, val.y, val.z);
                             vel = vel + nv * w;
@@ -955,23 +985,24 @@ __device__ __forceinline__ void transfer_chunk(TMPM_TRANSFER_PARAMS, const int c
             if (!MULTI && sp.defer) defer_push(sp, 2 + ((sp.step_index + 1) & 1), chunk);
         }
         if (active) {
-            unsigned long long last_key = kEmptyKey;
-            int last_id = -1;
+            // Per-node global scatter, the stencil's blocks found or inserted
+            // first (the tile is unused on this path: every warp is past its
+            // gather, the barrier of the box reduction orders it).
+            int *const ids = reinterpret_cast<int *>(s_gv) + threadIdx.x;
+            stencil_blocks<THREADS, BS, true>(next, b, ns, ids, status);
+#pragma unroll
             for (int a = 0; a < 3; ++a)
+#pragma unroll
                 for (int c = 0; c < 3; ++c)
+#pragma unroll
                     for (int e = 0; e < 3; ++e) {
-                        int cx = b[0] + a, cy = b[1] + c, cz = b[2] + e;
-                        int gx = cx >> BS, gy = cy >> BS, gz = cz >> BS;
-                        unsigned long long key = block_key(gx, gy, gz, ns);
-                        if (key != last_key) {
-                            last_key = key;
-                            last_id = find_or_insert_block(next, key, make_int4(gx, gy, gz, static_cast<int>(ns)), status);
-                        }
-                        if (last_id < 0) continue;
+                        const int cx = b[0] + a, cy = b[1] + c, cz = b[2] + e;
+                        const int id = ids[stencil_block_slot<BS>(b, cx, cy, cz) * THREADS];
+                        if (id < 0) continue;
                         float w = wx[a] * wy[c] * wz[e];
                         V3f dpos = mk((a - fx.x) * h, (c - fx.y) * h, (e - fx.z) * h);
                         V3f mom = (mv + mul(A, dpos)) * w;
-                        atomicAdd(next.pool + static_cast<size_t>(last_id) * (1 << (3 * BS)) + node_local<BS>(cx, cy, cz),
+                        atomicAdd(next.pool + static_cast<size_t>(id) * (1 << (3 * BS)) + node_local<BS>(cx, cy, cz),
                                   make_float4(w * k.mass, mom.x, mom.y, mom.z));
                     }
         }

@@ -567,11 +567,19 @@ struct TmpmSession {
             if (kernel_ms == nullptr && !(tunable && tuner.tuning()) && seg >= kGraphMinSubsteps) {
                 // after the choice, full segments are timed (re-sort included) for the
                 // tuner's watch, once their graph exists: a segment that captures its
-                // graph first would count the capture as device time
-                const bool probe = tunable && resort && seg == interval && tuner.watching() &&
-                                   seg_graphs.count(segment_key(sp, cur, resort, seg, apply_force)) > 0;
+                // graph first would count the capture as device time.  A
+                // challenger without a graph runs its kernels directly (probed:
+                // the launches stay ahead of the device, so its device time is
+                // the replay's) and gets no graph unless it takes over, so a
+                // challenge never pays a capture.
+                const bool cached = seg_graphs.count(segment_key(sp, cur, resort, seg, apply_force)) > 0;
+                const bool challenge = tunable && tuner.watching() && config != tuner.current(big_blocks_ok);
+                const bool probe = tunable && resort && seg == interval && tuner.watching() && (cached || challenge);
                 if (probe) tuner.probe_begin(config, stream);
-                st = run_segment_graph(sp, resort, seg, apply_force);
+                if (challenge && !cached)
+                    launch_segment(sp, cur, resort, seg, apply_force);
+                else
+                    st = run_segment_graph(sp, resort, seg, apply_force);
                 if (probe) tuner.probe_end(static_cast<double>(n_dev) * seg, stream);
             } else {
                 // launch_segment's kernels one by one, timed with `kernel_ms`
