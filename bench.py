@@ -476,9 +476,32 @@ def bench_adjoint() -> dict:
     sim.close()
     work = float(n) * sc.substeps
     f, b = float(np.median(fw)), float(np.median(bw))
+    # the dense node array of the rollout: cells floor(bound / h - 0.5) - 1 .. + 3 per axis
+    h = sc.params.cell_width
+    dims = [int(np.floor(np.float32(sc.params.bounds_max[k]) * np.float32(1.0 / h) - np.float32(0.5))) + 3 -
+            (int(np.floor(np.float32(sc.params.bounds_min[k]) * np.float32(1.0 / h) - np.float32(0.5))) - 1) + 1
+            for k in range(3)]
+    nodes = int(np.prod(dims))
+    peak, peak_kind = measured_peaks()
+
+    def roof(bytes_particle, bytes_node, seconds):
+        alg = (bytes_particle * n + bytes_node * nodes) * sc.substeps
+        gbs = alg / seconds / 1e9
+        return {"bound": "latency (every kernel is one partial wave of CTAs at 64k particles)",
+                "alg_bytes_per_particle_substep": bytes_particle, "alg_bytes_per_node_substep": bytes_node,
+                "nodes": nodes, "achieved": gbs, "peak": peak, "unit": "GB/s", "frac": gbs / peak,
+                "peak_source": peak_kind}
+
+    # algorithmic bytes per substep: forward P2G (state 96 + E 4 in, node 16 out), grid (32 per node),
+    # G2P (state 96 in and out, node 16 in), node clear (16), checkpoint copies (12 per particle);
+    # backward replay as the forward plus the polar factors (36), and the adjoint: G2P adjoint (state 96,
+    # state adjoint 96, partials 48 out; node velocity 16 in, node adjoint 16 out, cleared 16), grid
+    # adjoint (48 in, 16 out per node), P2G adjoint (state 96, E 4, partials 48, polar 36 in; node 16 in;
+    # state adjoint 96 and E adjoint 4 out)
+    roofline = {"forward": roof(304, 80, f), "backward": roof(852, 208, b)}
     return {"workload": "config5-differentiable", "particles": n, "substeps": sc.substeps, "checkpoint_every": 16,
             "forward_s": f, "backward_s": b, "forward": work / f, "backward": work / b,
-            "forward_plus_backward": work / (f + b), "unit": METRIC,
+            "forward_plus_backward": work / (f + b), "unit": METRIC, "roofline": roofline,
             "timing": "wall clock through the C ABI (host f64 arrays in and out, synchronous calls)",
             "parity": "gradients vs central differences of the oracle: tests/test_gpu_adjoint.py"}
 
