@@ -170,6 +170,8 @@ struct TmpmBatch {
     DevBuf<uint32_t> status, scene_status;
     DevBuf<SceneParams> dscenes;
     DevBuf<int> cta_cache;
+    DevBuf<uint32_t> defer;  // the fused transfer's deferred-chunk lists (defer_words of the chunk count)
+    ForkJoin fj{};           // second stream and events of the fused transfer
     DevBuf<uint32_t> sort_keys[2], sort_vals[2], sort_hist, sort_totals;
     PinnedBuf table_staging;
     std::vector<std::unique_ptr<TmpmPreparedScene>> in_flight_uploads;  // kept until the copies complete
@@ -228,6 +230,10 @@ struct TmpmBatch {
         if (t_begin) cudaEventDestroy(t_begin);
         if (t_end) cudaEventDestroy(t_end);
         if (read_stream) cudaStreamDestroy(read_stream);
+        if (fj.side) cudaStreamSynchronize(fj.side);
+        if (fj.fork) cudaEventDestroy(fj.fork);
+        if (fj.join) cudaEventDestroy(fj.join);
+        if (fj.side) cudaStreamDestroy(fj.side);
         if (stream) cudaStreamDestroy(stream);
     }
 
@@ -327,6 +333,10 @@ struct TmpmBatch {
         const size_t ctas = (cap + kMinTransferThreads - 1) / kMinTransferThreads;
         if (cta_cache.count < ctas * kCacheStride) {
             if ((e = cta_cache.alloc(ctas * kCacheStride))) return cuda_fail(e, "cudaMalloc cache");
+            ++epoch;
+        }
+        if (defer.count < defer_words(ctas)) {
+            if ((e = defer.alloc(defer_words(ctas)))) return cuda_fail(e, "cudaMalloc deferred lists");
             ++epoch;
         }
         if (sort_keys[0].count < cap) {
@@ -624,6 +634,13 @@ struct TmpmBatch {
         g[1].pool = grids[1].pool.ptr;
         const int n = static_cast<int>(n_live);
         launch_clear_table(g[0], g[1], bs, stream);
+        // the fused transfer's deferred-chunk lists (as in a session): emptied
+        // before the opening P2G, then by each grid update for its transfer
+        sp.defer = defer.ptr;
+        sp.defer_cap = static_cast<int>(defer.count >= static_cast<size_t>(kDeferHeader)
+                                            ? (defer.count - kDeferHeader) / 4
+                                            : 0);
+        if (sp.defer) cudaMemsetAsync(sp.defer, 0, sizeof(uint32_t) * kDeferHeader, stream);
         SimParams sp0 = sp;
         sp0.step_index = -1;
         launch_transfer(kModeP2G, dst, n, dclasses.ptr, g[1], g[0], sp0, nullptr, nullptr, nullptr, status.ptr,
@@ -634,7 +651,7 @@ struct TmpmBatch {
             spk.step_index = static_cast<int>(s);
             launch_grid_update(gc, gn, spk, nullptr, nullptr, nullptr, status.ptr, stream);
             launch_transfer(s + 1 == steps ? kModeG2P : kModeG2P2G, dst, n, dclasses.ptr, gc, gn, spk, nullptr,
-                            nullptr, nullptr, status.ptr, cta_cache.ptr, stream);
+                            nullptr, nullptr, status.ptr, cta_cache.ptr, stream, &fj);
         }
     }
 
@@ -1032,7 +1049,8 @@ struct TmpmBatch {
         for (int g = 0; g < 2; ++g)
             b += grids[g].pool_nodes * 16 + static_cast<size_t>(grids[g].max_blocks) * 16 +
                  static_cast<size_t>(grids[g].capacity) * 12;
-        b += cta_cache.count * 4 + dclasses.count * sizeof(DevClass) + kMaxScenes * (sizeof(SceneParams) + 4);
+        b += (cta_cache.count + defer.count) * 4 + dclasses.count * sizeof(DevClass) +
+             kMaxScenes * (sizeof(SceneParams) + 4);
         b += read_unsorted.count * 4;
         return b;
     }
@@ -1093,6 +1111,9 @@ TmpmStatus tmpm_batch_create(const TmpmBatchOptions *options, TmpmBatch **out) {
         (e = cudaStreamCreateWithFlags(&b->upload_stream, cudaStreamNonBlocking)) ||
         (e = cudaEventCreateWithFlags(&b->upload_done, cudaEventDisableTiming)) ||
         (e = cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming)) || (e = cudaEventCreate(&b->t_begin)) ||
+        (e = cudaStreamCreateWithFlags(&b->fj.side, cudaStreamNonBlocking)) ||
+        (e = cudaEventCreateWithFlags(&b->fj.fork, cudaEventDisableTiming)) ||
+        (e = cudaEventCreateWithFlags(&b->fj.join, cudaEventDisableTiming)) ||
         (e = cudaEventCreate(&b->t_end)) || (e = b->status.alloc(1)) || (e = b->scene_status.alloc(kMaxScenes)) ||
         (e = b->dscenes.alloc(kMaxScenes))) {
         g_last_error = std::string("batch setup: ") + cudaGetErrorString(e);

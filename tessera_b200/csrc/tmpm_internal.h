@@ -237,7 +237,8 @@ struct ForkJoin {
 // Launchers (tmpm_kernels.cu).  All run on `stream`.
 // `cur` and `next` share one hash table (block ids are stable within a batch)
 // and differ in their node pools; `cache` holds kCacheStride ints per CTA.
-// With `fj`, sp.defer set and one scene without CPIC, the fused transfer
+// With `fj`, sp.defer set and no CPIC (and, in a multi-scene batch, no
+// plastic state), the fused transfer
 // (kModeG2P2G) runs as the fast kernel beside the chunks without a record
 // (on fj->side) and then the chunks the fast kernel deferred; the grid update
 // before it must carry the same step_index.

@@ -224,7 +224,7 @@ __device__ __forceinline__ void reduce_box_sums(bool valid, const int b[3], uint
     sum_a = fa;
     sum_b = fb;
     bool ok = m[0] <= m[3] && m[6] == m[7];
-    int nodes = 1, nbt = 1;
+    int nodes = m[0] <= m[3] ? 1 : 0, nbt = 1;  // nodes 0: no valid particle
     for (int a = 0; a < 3 && ok; ++a)
         if (static_cast<long long>(m[3 + a]) - m[a] + 3 > kTileMaxDim) ok = false;
     if (ok) {
@@ -422,7 +422,7 @@ __device__ __forceinline__ void transfer_chunk(TMPM_TRANSFER_PARAMS, const int c
     // path tests each particle against the obstacles' reach (inline, no call)
     // and defers a chunk that may touch one.
     constexpr bool CONTACT = OBST && !FAST;
-    static_assert(!FAST || (MODE == kModeG2P2G && !MULTI && !CPIC), "the fast path is the fused transfer of one scene");
+    static_assert(!FAST || (MODE == kModeG2P2G && !CPIC), "the fast path is the fused transfer without CPIC");
     constexpr int kTileNodes = tile_nodes(THREADS);
     const TransferSmem<THREADS, CONTACT> S = transfer_smem<THREADS, CONTACT>();
     float4 *const s_gv = S.tile;
@@ -851,6 +851,12 @@ __device__ __forceinline__ void transfer_chunk(TMPM_TRANSFER_PARAMS, const int c
     if (max_m > tot_m * kFloatModeShare || max_p > tot_p * kFloatModeShare) bx.ok = 0;
     if constexpr (FAST) {
         if (!bx.ok) {
+            // A chunk with nothing to scatter (every particle's scene is past
+            // its last substep of the batch) needs no P2G and no record.
+            if (bx.nodes == 0) {
+                if (threadIdx.x == 0) cc[0] = 0;
+                return;
+            }
             // the P2G-only pass reads velocity and affine matrix from the
             // particle arrays (position, F and plastic state are stored)
             if (p2g_on) {
@@ -987,7 +993,7 @@ __device__ __forceinline__ void transfer_chunk(TMPM_TRANSFER_PARAMS, const int c
     } else {
         if (threadIdx.x == 0) {
             cc[0] = 0;
-            if (!MULTI && sp.defer) defer_push(sp, 2 + ((sp.step_index + 1) & 1), chunk);
+            if (sp.defer) defer_push(sp, 2 + ((sp.step_index + 1) & 1), chunk);
         }
         if (active) {
             // Per-node global scatter, the stencil's blocks found or inserted
@@ -1073,7 +1079,7 @@ __global__ void __launch_bounds__(256) k_grid(GridTable g, GridTable nxt, SimPar
                                                const float *__restrict__ planes, double *reactions, uint32_t *status) {
     __shared__ int s_abort;
     // empty the deferred-chunk lists that the next transfer (step_index) fills
-    if (!MULTI && sp.defer && blockIdx.x == 0 && threadIdx.x == 0) {
+    if (sp.defer && blockIdx.x == 0 && threadIdx.x == 0) {
         sp.defer[0] = 0;
         sp.defer[1] = 0;
         sp.defer[2 + ((sp.step_index + 1) & 1)] = 0;
@@ -1324,7 +1330,8 @@ void launch_fused(const ParticleSoA &P, int n, const DevClass *classes, const Gr
         if (big) TMPM_FUSED_SHAPES_BS(V, kBigBlockShift);      \
         else TMPM_FUSED_SHAPES_BS(V, kBlockShift);             \
     } while (0)
-    if (pl) TMPM_FUSED(true, kPlainObst, 256, TMPM_TRANSFER_MIN_BLOCKS, kBlockShift);
+    if (sp.multi) TMPM_FUSED_SHAPES(kMulti);
+    else if (pl) TMPM_FUSED(true, kPlainObst, 256, TMPM_TRANSFER_MIN_BLOCKS, kBlockShift);
     else if (obst) TMPM_FUSED_SHAPES(kPlainObst);
     else TMPM_FUSED_SHAPES(kPlain);
 #undef TMPM_FUSED_SHAPES
@@ -1337,7 +1344,7 @@ void launch_transfer(int mode, const ParticleSoA &P, int n, const DevClass *clas
                      const GridTable &next, const SimParams &sp, const DevObstacle *obstacles, const float *planes,
                      double *reactions, uint32_t *status, int *cache, cudaStream_t stream, const ForkJoin *fj) {
     if (n <= 0) return;
-    if (mode == kModeG2P2G && fj && sp.defer && !sp.multi && !sp.cpic) {
+    if (mode == kModeG2P2G && fj && sp.defer && !sp.cpic && !(sp.multi && sp.has_plastic)) {
         launch_fused(P, n, classes, cur, next, sp, obstacles, planes, reactions, status, cache, stream, *fj);
         return;
     }
@@ -1413,7 +1420,7 @@ void touch_transfer() {
 }
 template <int V, int T, int B, int BS>
 void touch_fused() {
-    if constexpr (V == kPlain || V == kPlainObst) {
+    if constexpr (V == kPlain || V == kPlainObst || V == kMulti) {
         cudaFuncAttributes a;
         cudaFuncGetAttributes(&a, k_transfer_fast<false, V, T, B, BS>);
         cudaFuncGetAttributes(&a, k_transfer_deferred<true, false, V, T, BS>);
